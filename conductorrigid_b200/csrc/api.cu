@@ -1,0 +1,428 @@
+// api.cu -- the C ABI declared in include/conductor_rigid.h.
+//
+// The handle plays the part of the reference's ConductorRigid ForceCompute
+// (ConductorRigid.h:21-112): it owns the derived parameters, tables, mesh, FFT plans,
+// per-solve geometry and the Krylov workspace; the caller owns the particle arrays.
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "cr_internal.cuh"
+
+namespace cr {
+
+int fail(cr_handle *h, int status, const std::string &msg) {
+    if (h) h->last_error = msg;
+    return status;
+}
+
+int check_cuda(cr_handle *h, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return CR_OK;
+    cudaGetLastError();
+    const int st = e == cudaErrorMemoryAllocation ? CR_OUT_OF_MEMORY : CR_CUDA_ERROR;
+    return fail(h, st, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int check_cufft(cr_handle *h, cufftResult r, const char *what) {
+    if (r == CUFFT_SUCCESS) return CR_OK;
+    return fail(h, r == CUFFT_ALLOC_FAILED ? CR_OUT_OF_MEMORY : CR_CUDA_ERROR,
+                std::string(what) + ": cuFFT error " + std::to_string((int)r));
+}
+
+namespace {
+
+void free_all(cr_handle *h) {
+    mesh_free(h->m64);
+    mesh_free(h->m32);
+    geometry_free(h);
+    krylov_free(h);
+    dfree(&h->d_body);
+    dfree(&h->d_rigid);
+    dfree(&h->d_Q);
+    dfree(&h->d_bsize);
+    dfree(&h->d_body_start);
+    dfree(&h->d_body_members);
+    dfree(&h->d_bpos);
+    dfree(&h->d_tmp_n);
+    dfree(&h->d_tmp_n2);
+    dfree(&h->d_force);
+    dfree(&h->d_io_pos);
+    dfree(&h->d_io_bpos);
+    dfree(&h->d_io_q);
+    dfree(&h->d_io_phi);
+    dfree(&h->d_io_force);
+}
+
+int derive(cr_handle *h, const cr_params *p, const double L[3]) {
+    cr_derived d;
+    const int st = cr_derive_params(p, L, &d);
+    if (st == CR_GRID_TOO_LARGE) return fail(h, st, "requested number of Fourier nodes exceeds maximum of 4096");
+    if (st != CR_OK) return fail(h, st, "invalid parameters (xi, errortol, box, or rcut above half the box)");
+    h->user = *p;
+    h->d = d;
+    for (int k = 0; k < 3; ++k) {
+        h->L[k] = L[k];
+        h->field[k] = p->field[k];
+    }
+    const int nt = d.n_table + 1;
+    h->h_phiq.assign(2 * (size_t)nt, 0.0);
+    h->h_gradphiq.assign(2 * (size_t)nt, 0.0);
+    cr_build_tables(&d, p->xi, h->h_phiq.data(), h->h_gradphiq.data());
+    // tiles of 8^3 nodes (fewer along short dimensions)
+    h->tile = 8;
+    h->ntiles = 1;
+    for (int k = 0; k < 3; ++k) {
+        h->ntiles_dim[k] = (d.grid[k] + h->tile - 1) / h->tile;
+        h->ntiles *= h->ntiles_dim[k];
+    }
+    return CR_OK;
+}
+
+// Allocate every device structure for the current parameters and topology size.
+int realize(cr_handle *h) {
+    CR_TRY(mesh_init(h, h->m64));
+    CR_TRY(mesh_init(h, h->m32));
+    CR_TRY(geometry_alloc(h));
+    CR_TRY(krylov_alloc(h));
+    CR_TRY(dalloc(h, &h->d_bpos, (size_t)std::max(h->B, 1)));
+    CR_TRY(dalloc(h, &h->d_tmp_n, (size_t)(h->N + h->B)));
+    CR_TRY(dalloc(h, &h->d_tmp_n2, (size_t)(h->N + h->B)));
+    CR_TRY(dalloc(h, &h->d_force, 3 * (size_t)h->N));
+    CR_CUDA(h, cudaMemset(h->d_bpos, 0, sizeof(double4) * std::max(h->B, 1)));
+    return CR_OK;
+}
+
+int need_ready(cr_handle *h) {
+    if (!h) return CR_BAD_PARAM;
+    if (!h->have_topology) return fail(h, CR_NOT_READY, "topology not set");
+    return CR_OK;
+}
+
+int need_geometry(cr_handle *h) {
+    CR_TRY(need_ready(h));
+    if (!h->geo.valid) return fail(h, CR_NOT_READY, "positions not set");
+    return CR_OK;
+}
+
+bool finite_params(const cr_params *p) {
+    if (!std::isfinite(p->xi) || !std::isfinite(p->errortol) || !std::isfinite(p->rcut) ||
+        !std::isfinite(p->gmres_tol))
+        return false;
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(p->field[k])) return false;
+    return true;
+}
+
+template <typename R> int wave_out(cr_handle *h, MeshBuffers<R> &m, const double *d_q, double *d_phi) {
+    CR_TRY(cast_charges(h, m, d_q));
+    CR_TRY(wave_potential(h, m));
+    CR_TRY(cast_to_double(h, m.phi, d_phi, h->N));
+    return CR_OK;
+}
+
+}  // namespace
+}  // namespace cr
+
+using namespace cr;
+
+extern "C" {
+
+int cr_abi_version(void) { return CR_ABI_VERSION; }
+
+const char *cr_status_string(int s) {
+    switch (s) {
+        case CR_OK: return "ok";
+        case CR_NOT_CONVERGED: return "not converged";
+        case CR_BAD_PARAM: return "bad parameter";
+        case CR_CUDA_ERROR: return "CUDA error";
+        case CR_TIMEOUT: return "timeout";
+        case CR_OUT_OF_MEMORY: return "out of memory";
+        case CR_GRID_TOO_LARGE: return "grid too large";
+        case CR_NOT_READY: return "not ready";
+        case CR_NUMERICAL: return "non-finite value";
+        default: return "unknown status";
+    }
+}
+
+const char *cr_last_error(const cr_handle *h) { return h ? h->last_error.c_str() : "null handle"; }
+
+int cr_create(const cr_params *p, const double L[3], cr_handle **out) {
+    if (!p || !L || !out) return CR_BAD_PARAM;
+    *out = nullptr;
+    if (!finite_params(p)) return CR_BAD_PARAM;
+    cr_handle *h = new cr_handle();
+    const int st = derive(h, p, L);
+    if (st != CR_OK) {
+        delete h;
+        return st;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        delete h;
+        return CR_CUDA_ERROR;
+    }
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+    *out = h;
+    return CR_OK;
+}
+
+int cr_destroy(cr_handle *h) {
+    if (!h) return CR_BAD_PARAM;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    else cudaDeviceSynchronize();
+    free_all(h);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    delete h;
+    return CR_OK;
+}
+
+int cr_get_derived(const cr_handle *h, cr_derived *out) {
+    if (!h || !out) return CR_BAD_PARAM;
+    *out = h->d;
+    return CR_OK;
+}
+
+int cr_set_field(cr_handle *h, const double field[3]) {
+    if (!h || !field) return CR_BAD_PARAM;
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(field[k])) return fail(h, CR_BAD_PARAM, "non-finite field");
+    for (int k = 0; k < 3; ++k) {
+        h->field[k] = field[k];
+        h->user.field[k] = field[k];
+    }
+    return CR_OK;
+}
+
+int cr_set_params(cr_handle *h, const cr_params *p, const double L[3]) {
+    if (!h || !p || !L) return CR_BAD_PARAM;
+    if (!finite_params(p)) return fail(h, CR_BAD_PARAM, "non-finite parameter");
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    CR_TRY(derive(h, p, L));
+    h->geo.valid = false;
+    if (h->have_topology) {
+        mesh_free(h->m64);
+        mesh_free(h->m32);
+        geometry_free(h);
+        krylov_free(h);
+        CR_TRY(realize(h));
+    }
+    return CR_OK;
+}
+
+int cr_set_stream(cr_handle *h, void *stream) {
+    if (!h) return CR_BAD_PARAM;
+    h->stream = (cudaStream_t)stream;
+    return CR_OK;
+}
+
+int cr_set_topology(cr_handle *h, int n_beads, const uint32_t *body, int n_bodies, const uint8_t *rigid,
+                    const double *body_charge) {
+    if (!h || n_beads < 0 || n_bodies < 0) return CR_BAD_PARAM;
+    if (n_beads > 0 && (!body || n_bodies == 0)) return fail(h, CR_BAD_PARAM, "missing body list");
+    if (n_bodies > 0 && (!rigid || !body_charge)) return fail(h, CR_BAD_PARAM, "missing body arrays");
+    std::vector<int> size(n_bodies, 0);
+    for (int i = 0; i < n_beads; ++i) {
+        if (body[i] >= (uint32_t)n_bodies) return fail(h, CR_BAD_PARAM, "body tag out of range");
+        size[body[i]]++;
+    }
+    for (int b = 0; b < n_bodies; ++b) {
+        if (size[b] == 0) return fail(h, CR_BAD_PARAM, "body without beads");
+        if (!rigid[b] && size[b] != 1) return fail(h, CR_BAD_PARAM, "a free bead body must hold exactly one bead");
+        if (!std::isfinite(body_charge[b])) return fail(h, CR_BAD_PARAM, "non-finite body charge");
+    }
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    h->have_topology = false;
+    h->N = n_beads;
+    h->B = n_bodies;
+    CR_TRY(dalloc(h, &h->d_body, (size_t)std::max(n_beads, 1)));
+    CR_TRY(dalloc(h, &h->d_rigid, (size_t)std::max(n_bodies, 1)));
+    CR_TRY(dalloc(h, &h->d_Q, (size_t)std::max(n_bodies, 1)));
+    CR_TRY(dalloc(h, &h->d_bsize, (size_t)std::max(n_bodies, 1)));
+    CR_TRY(dalloc(h, &h->d_body_start, (size_t)n_bodies + 1));
+    CR_TRY(dalloc(h, &h->d_body_members, (size_t)std::max(n_beads, 1)));
+    if (n_beads) CR_CUDA(h, cudaMemcpy(h->d_body, body, n_beads * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (n_bodies) {
+        CR_CUDA(h, cudaMemcpy(h->d_rigid, rigid, n_bodies, cudaMemcpyHostToDevice));
+        CR_CUDA(h, cudaMemcpy(h->d_Q, body_charge, n_bodies * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    CR_TRY(realize(h));
+    if (n_beads) CR_TRY(topology_build(h));
+    h->have_topology = true;
+    return CR_OK;
+}
+
+int cr_set_positions(cr_handle *h, const double *d_pos, const double *d_body_pos) {
+    CR_TRY(need_ready(h));
+    if (!d_pos && h->N > 0) return fail(h, CR_BAD_PARAM, "null positions");
+    CR_TRY(geometry_update(h, d_pos, d_body_pos));
+    return CR_OK;
+}
+
+int cr_apply_operator(cr_handle *h, const double *d_x, double *d_y, int precision) {
+    CR_TRY(need_geometry(h));
+    if (h->N == 0) return CR_OK;
+    if (!d_x || !d_y) return fail(h, CR_BAD_PARAM, "null vector");
+    CR_TRY(apply_operator(h, d_x, d_y, precision));
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_apply_operator");
+}
+
+int cr_precondition(cr_handle *h, const double *d_x, double *d_y) {
+    CR_TRY(need_ready(h));
+    if (h->N == 0) return CR_OK;
+    if (!d_x || !d_y) return fail(h, CR_BAD_PARAM, "null vector");
+    CR_TRY(precondition(h, d_x, d_y));
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_precondition");
+}
+
+int cr_objective(cr_handle *h, double *d_rhs) {
+    CR_TRY(need_geometry(h));
+    if (h->N == 0) return CR_OK;
+    if (!d_rhs) return fail(h, CR_BAD_PARAM, "null vector");
+    CR_TRY(objective(h, d_rhs));
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_objective");
+}
+
+int cr_wave_potential(cr_handle *h, const double *d_q, double *d_phi, int precision) {
+    CR_TRY(need_geometry(h));
+    if (h->N == 0) return CR_OK;
+    if (!d_q || !d_phi) return fail(h, CR_BAD_PARAM, "null vector");
+    if (precision == CR_FP64) CR_TRY(wave_out(h, h->m64, d_q, d_phi));
+    else CR_TRY(wave_out(h, h->m32, d_q, d_phi));
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_wave_potential");
+}
+
+int cr_spread(cr_handle *h, const double *d_q, double *d_grid, int precision) {
+    CR_TRY(need_geometry(h));
+    if (!d_grid) return fail(h, CR_BAD_PARAM, "null vector");
+    const long G = grid_size(h);
+    if (h->N == 0) return check_cuda(h, cudaMemset(d_grid, 0, G * sizeof(double)), "cr_spread");
+    if (!d_q) return fail(h, CR_BAD_PARAM, "null vector");
+    if (precision == CR_FP64) {
+        CR_TRY(cast_charges(h, h->m64, d_q));
+        CR_TRY(spread_only(h, h->m64));
+        CR_CUDA(h, cudaMemcpyAsync(d_grid, h->m64.grid, G * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        CR_TRY(cast_charges(h, h->m32, d_q));
+        CR_TRY(spread_only(h, h->m32));
+        CR_TRY(cast_to_double(h, h->m32.grid, d_grid, G));
+    }
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_spread");
+}
+
+int cr_apply_M(cr_handle *h, const double *d_q, double *d_Mq, int precision) {
+    CR_TRY(need_geometry(h));
+    if (h->N == 0) return CR_OK;
+    if (!d_q || !d_Mq) return fail(h, CR_BAD_PARAM, "null vector");
+    if (precision == CR_FP64) {
+        CR_TRY(cast_charges(h, h->m64, d_q));
+        CR_TRY(wave_potential(h, h->m64));
+        CR_TRY(real_space_apply(h, h->m64, nullptr, d_Mq));
+    } else {
+        CR_TRY(cast_charges(h, h->m32, d_q));
+        CR_TRY(wave_potential(h, h->m32));
+        CR_TRY(real_space_apply(h, h->m32, nullptr, d_Mq));
+    }
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_apply_M");
+}
+
+int cr_forces(cr_handle *h, const double *d_q, double *d_force, int precision) {
+    CR_TRY(need_geometry(h));
+    if (h->N == 0) return CR_OK;
+    if (!d_q || !d_force) return fail(h, CR_BAD_PARAM, "null vector");
+    if (precision == CR_FP64) {
+        CR_TRY(cast_charges(h, h->m64, d_q));
+        CR_TRY(wave_force(h, h->m64));
+        CR_TRY(real_space_force(h, h->m64, d_force));
+    } else {
+        CR_TRY(cast_charges(h, h->m32, d_q));
+        CR_TRY(wave_force(h, h->m32));
+        CR_TRY(real_space_force(h, h->m32, d_force));
+    }
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_forces");
+}
+
+int cr_neighbor_list(cr_handle *h, double r_list, int *d_count, int64_t *d_head, int *d_list, int64_t capacity,
+                     int64_t *total) {
+    CR_TRY(need_geometry(h));
+    if (!total || capacity < 0) return fail(h, CR_BAD_PARAM, "null output");
+    if (h->N == 0) {
+        *total = 0;
+        return CR_OK;
+    }
+    if (!d_count || !d_head) return fail(h, CR_BAD_PARAM, "null output");
+    return neighbor_list_build(h, r_list, d_count, d_head, capacity > 0 ? d_list : nullptr, capacity, total);
+}
+
+// gpu_ComputeForce (ConductorRigid.cu:1153-1286): geometry, right-hand side, solve
+// from the warm start, write back charges and potentials, then the force pass.
+int cr_compute(cr_handle *h, const double *d_pos, const double *d_body_pos, double *d_q, double *d_phi,
+               double *d_force, cr_solve_stats *stats) {
+    CR_TRY(need_ready(h));
+    if ((!d_pos || !d_q || !d_force) && h->N > 0) return fail(h, CR_BAD_PARAM, "null array");
+    if ((!d_phi || !d_body_pos) && h->B > 0) return fail(h, CR_BAD_PARAM, "null body array");
+    const int N = h->N, B = h->B;
+    cr_solve_stats st{};
+    if (N == 0) {
+        st.converged = 1;
+        if (stats) *stats = st;
+        return CR_OK;
+    }
+    CR_TRY(geometry_update(h, d_pos, d_body_pos));
+    Krylov &K = h->kry;
+    CR_TRY(objective(h, K.b));
+    CR_CUDA(h, cudaMemcpyAsync(K.x, d_q, N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (B) CR_CUDA(h, cudaMemcpyAsync(K.x + N, d_phi, B * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CR_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+    const int sst = solve(h, K.x, K.b, &st);
+    if (sst != CR_OK && sst != CR_NOT_CONVERGED) return sst;
+    CR_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+    CR_CUDA(h, cudaMemcpyAsync(d_q, K.x, N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (B) CR_CUDA(h, cudaMemcpyAsync(d_phi, K.x + N, B * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    // force pass in FP64
+    CR_TRY(cast_charges(h, h->m64, K.x));
+    CR_TRY(wave_force(h, h->m64));
+    CR_TRY(real_space_force(h, h->m64, d_force));
+    CR_CUDA(h, cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    st.solve_ms = ms;
+    if (stats) *stats = st;
+    if (sst == CR_NOT_CONVERGED) fail(h, CR_NOT_CONVERGED, "GMRES reached its iteration limit");
+    return sst;
+}
+
+int cr_compute_host(cr_handle *h, const double *pos, const double *body_pos, double *q, double *phi, double *force,
+                    cr_solve_stats *stats) {
+    CR_TRY(need_ready(h));
+    const int N = h->N, B = h->B;
+    if ((!pos || !q || !force) && N > 0) return fail(h, CR_BAD_PARAM, "null array");
+    if ((!phi || !body_pos) && B > 0) return fail(h, CR_BAD_PARAM, "null body array");
+    if (!h->d_io_pos) {
+        CR_TRY(dalloc(h, &h->d_io_pos, 3 * (size_t)std::max(N, 1)));
+        CR_TRY(dalloc(h, &h->d_io_bpos, 3 * (size_t)std::max(B, 1)));
+        CR_TRY(dalloc(h, &h->d_io_q, (size_t)std::max(N, 1)));
+        CR_TRY(dalloc(h, &h->d_io_phi, (size_t)std::max(B, 1)));
+        CR_TRY(dalloc(h, &h->d_io_force, 3 * (size_t)std::max(N, 1)));
+    }
+    cudaStream_t s = h->stream;
+    CR_CUDA(h, cudaMemcpyAsync(h->d_io_pos, pos, 3 * (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s));
+    CR_CUDA(h, cudaMemcpyAsync(h->d_io_q, q, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (B) {
+        CR_CUDA(h, cudaMemcpyAsync(h->d_io_bpos, body_pos, 3 * (size_t)B * sizeof(double), cudaMemcpyHostToDevice, s));
+        CR_CUDA(h, cudaMemcpyAsync(h->d_io_phi, phi, (size_t)B * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    const int st = cr_compute(h, h->d_io_pos, h->d_io_bpos, h->d_io_q, h->d_io_phi, h->d_io_force, stats);
+    if (st != CR_OK && st != CR_NOT_CONVERGED) return st;
+    CR_CUDA(h, cudaMemcpyAsync(q, h->d_io_q, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (B) CR_CUDA(h, cudaMemcpyAsync(phi, h->d_io_phi, (size_t)B * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(h, cudaMemcpyAsync(force, h->d_io_force, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(h, cudaStreamSynchronize(s));
+    return st;
+}
+
+}  // extern "C"
+

@@ -1,0 +1,218 @@
+// cr_internal.cuh -- internal types of the CUDA implementation behind conductor_rigid.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/conductor_rigid.h"
+
+namespace cr {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// ---- precision traits ----
+template <typename R> struct Prec;
+template <> struct Prec<float> {
+    typedef float4 R4;
+    typedef float2 R2;
+    typedef cufftComplex C;
+    static constexpr cufftType kR2C = CUFFT_R2C;
+    static constexpr cufftType kC2R = CUFFT_C2R;
+};
+template <> struct Prec<double> {
+    typedef double4 R4;
+    typedef double2 R2;
+    typedef cufftDoubleComplex C;
+    static constexpr cufftType kR2C = CUFFT_D2Z;
+    static constexpr cufftType kC2R = CUFFT_Z2D;
+};
+
+inline cufftResult fft_forward(cufftHandle p, float *in, cufftComplex *out) { return cufftExecR2C(p, in, out); }
+inline cufftResult fft_forward(cufftHandle p, double *in, cufftDoubleComplex *out) { return cufftExecD2Z(p, in, out); }
+inline cufftResult fft_inverse(cufftHandle p, cufftComplex *in, float *out) { return cufftExecC2R(p, in, out); }
+inline cufftResult fft_inverse(cufftHandle p, cufftDoubleComplex *in, double *out) { return cufftExecZ2D(p, in, out); }
+
+// Device buffers of one operator precision.
+template <typename R> struct MeshBuffers {
+    typedef typename Prec<R>::R4 R4;
+    typedef typename Prec<R>::R2 R2;
+    typedef typename Prec<R>::C C;
+    R4 *pos = nullptr;          // [N] bead positions in the box (x, y, z, 0)
+    R2 *phiq = nullptr;         // [n_table+1] potential table (value, next value)
+    R2 *gradphiq = nullptr;     // [n_table+1] gradient table
+    R *grid = nullptr;          // [Nx*Ny*Nz] real mesh
+    C *spec = nullptr;          // [Nx*Ny*(Nz/2+1)] half spectrum
+    R *scale = nullptr;         // [Nx*Ny*(Nz/2+1)] influence function S(k)/Ngrid
+    R *q = nullptr;             // [N] charges in this precision
+    R *phi = nullptr;           // [N] wave-space potential scratch
+    R *force = nullptr;         // [3N] wave-space force scratch
+    cufftHandle plan_fwd = 0, plan_inv = 0;
+    bool ready = false;
+};
+
+// Geometry of the current positions (fixed during one solve).
+struct Geometry {
+    int4 *wstart = nullptr;     // [N] first window node per dim (wrapped), .w = tile id
+    int *tile_start = nullptr;  // [ntiles+1]
+    int *tile_beads = nullptr;  // [N] beads sorted by tile (ascending bead index within a tile)
+    int *tile_count = nullptr;  // [ntiles]
+    // neighbour list within rc (CSR; per-bead ascending order)
+    int *nl_count = nullptr;    // [N]
+    int64_t *nl_head = nullptr; // [N]
+    int *nl_list = nullptr;     // [capacity]
+    int64_t nl_capacity = 0;
+    int64_t nl_total = 0;
+    // cell list used to build it
+    int *cell_of = nullptr;     // [N]
+    int *cell_start = nullptr;  // [ncell+1]
+    int *cell_beads = nullptr;  // [N]
+    int ncell[3] = {0, 0, 0};
+    size_t ncell_alloc = 0;
+    bool valid = false;
+};
+
+// GMRES workspace (FP64).
+struct Krylov {
+    int n = 0, m = 0;
+    double *V = nullptr;        // [(m+1) * n] orthonormal basis
+    double *Z = nullptr;        // [m * n] preconditioned directions (flexible GMRES)
+    double *w = nullptr;        // [n]
+    double *r = nullptr;        // [n]
+    double *b = nullptr;        // [n]
+    double *x = nullptr;        // [n]
+    double *d = nullptr;        // [n] refinement correction
+    double *rr = nullptr;       // [n] refinement residual (right-hand side of the inner solve)
+    double *partial = nullptr;  // [nblocks * (m+2)] dot-product partials
+    double *hcol = nullptr;     // [m+2] reduced dot products
+    double *yvec = nullptr;     // [m] least-squares coefficients
+    double *h_pinned = nullptr; // pinned host mirror of hcol
+    int nblocks = 0;
+};
+
+}  // namespace cr
+
+struct cr_handle {
+    cr_params user{};
+    cr_derived d{};
+    double L[3] = {0, 0, 0};
+    double field[3] = {0, 0, 0};
+    int N = 0, B = 0;
+    bool have_topology = false;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+
+    // topology
+    uint32_t *d_body = nullptr;       // [N]
+    uint8_t *d_rigid = nullptr;       // [B]
+    double *d_Q = nullptr;            // [B]
+    int *d_bsize = nullptr;           // [B]
+    int *d_body_start = nullptr;      // [B+1] CSR of members
+    int *d_body_members = nullptr;    // [N]
+    double4 *d_bpos = nullptr;        // [B] body centres
+
+    // tables on the host (FP64)
+    std::vector<double> h_phiq, h_gradphiq;
+
+    // mesh tiling
+    int tile = 8;                     // tile edge in nodes
+    int ntiles_dim[3] = {0, 0, 0};
+    int ntiles = 0;
+
+    cr::MeshBuffers<double> m64;
+    cr::MeshBuffers<float> m32;
+    cr::Geometry geo;
+    cr::Krylov kry;
+
+    // scratch
+    double *d_tmp_n = nullptr;        // [N+B]
+    double *d_tmp_n2 = nullptr;       // [N+B]
+    double *d_force = nullptr;        // [3N]
+    int *d_flag = nullptr;            // device error flag
+    void *d_sort_tmp = nullptr;       // CUB temporary storage
+    size_t sort_tmp_bytes = 0;
+    int *d_keys = nullptr, *d_keys_alt = nullptr, *d_vals = nullptr, *d_vals_alt = nullptr;  // [N]
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // staging for cr_compute_host
+    double *d_io_pos = nullptr, *d_io_bpos = nullptr, *d_io_q = nullptr, *d_io_phi = nullptr, *d_io_force = nullptr;
+};
+
+namespace cr {
+
+// Error plumbing: record the message on the handle and return a status.
+int fail(cr_handle *h, int status, const std::string &msg);
+int check_cuda(cr_handle *h, cudaError_t e, const char *what);
+int check_cufft(cr_handle *h, cufftResult r, const char *what);
+
+#define CR_TRY(expr)                      \
+    do {                                  \
+        int _st = (expr);                 \
+        if (_st != CR_OK) return _st;     \
+    } while (0)
+#define CR_CUDA(h, expr) CR_TRY(::cr::check_cuda((h), (expr), #expr))
+#define CR_CUFFT(h, expr) CR_TRY(::cr::check_cufft((h), (expr), #expr))
+#define CR_LAUNCH(h, what) CR_TRY(::cr::check_cuda((h), cudaGetLastError(), (what)))
+
+template <typename T> int dalloc(cr_handle *h, T **p, size_t count) {
+    if (*p) { cudaFree(*p); *p = nullptr; }
+    if (count == 0) return CR_OK;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(h, e == cudaErrorMemoryAllocation ? CR_OUT_OF_MEMORY : CR_CUDA_ERROR,
+                    std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return CR_OK;
+}
+template <typename T> void dfree(T **p) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+}
+
+inline int grid_size(const cr_handle *h) { return h->d.grid[0] * h->d.grid[1] * h->d.grid[2]; }
+inline int spec_size(const cr_handle *h) { return h->d.grid[0] * h->d.grid[1] * (h->d.grid[2] / 2 + 1); }
+inline int blocks_for(long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+// ---- module entry points (mesh.cu, realspace.cu, body.cu, solver.cu) ----
+template <typename R> int mesh_init(cr_handle *h, MeshBuffers<R> &m);
+template <typename R> void mesh_free(MeshBuffers<R> &m);
+int geometry_alloc(cr_handle *h);
+void geometry_free(cr_handle *h);
+// Positions (device, double[N*3]) -> wrapped positions, window starts, tile bins,
+// neighbour list within rc.
+int geometry_update(cr_handle *h, const double *d_pos, const double *d_body_pos);
+// Charges (double) -> precision copy used by the operator kernels.
+template <typename R> int cast_charges(cr_handle *h, MeshBuffers<R> &m, const double *d_q);
+// out[i] = (double) in[i]
+template <typename R> int cast_to_double(cr_handle *h, const R *in, double *out, long n);
+// Wave-space potential into m.phi (R) for the charges in m.q.
+template <typename R> int wave_potential(cr_handle *h, MeshBuffers<R> &m);
+// Wave-space force into m.force (R) for the charges in m.q.
+template <typename R> int wave_force(cr_handle *h, MeshBuffers<R> &m);
+// Spread m.q into m.grid only.
+template <typename R> int spread_only(cr_handle *h, MeshBuffers<R> &m);
+// Real-space: out_i = Phi_b(i) - (phi_k + self q + sum T q)   (phi_body != NULL)
+//             out_i = phi_k + self q + sum T q               (phi_body == NULL)
+template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out);
+// Forces: out = wave force + q E0 + real-space force (FP64 out).
+template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, double *force_out);
+int neighbor_list_build(cr_handle *h, double r_list, int *d_count, int64_t *d_head, int *d_list,
+                        int64_t capacity, int64_t *total);
+// Body rows y[N+b] = sum_{i in b} x_i (FP64).
+int body_sums(cr_handle *h, const double *x, double *y);
+// Member lists of the bodies from d_body (stable device sort).
+int topology_build(cr_handle *h);
+int objective(cr_handle *h, double *rhs);
+int precondition(cr_handle *h, const double *x, double *y);
+// y = A x in the given precision (full operator).
+int apply_operator(cr_handle *h, const double *x, double *y, int precision);
+// Solve A x = b (x holds the warm start).
+int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st);
+int krylov_alloc(cr_handle *h);
+void krylov_free(cr_handle *h);
+
+}  // namespace cr

@@ -1,0 +1,405 @@
+// mesh.cu -- wave-space part of the operator: spread, FFT, influence function,
+// inverse FFT, contract (ConductorRigid.cu:144-466, 919-937, 1256-1274).
+//
+// Layout: real mesh [Nx][Ny][Nz] (x slowest, the reference's i*Ny*Nz + j*Nz + k,
+// ConductorRigid.cu:229), half spectrum [Nx][Ny][Nz/2+1] from an R2C/D2Z transform.
+// The reference transforms the real charge mesh with a full C2C FFT and keeps the
+// real part of the inverse; with a real, even influence function the half-spectrum
+// pair R2C/C2R gives the same numbers with half the traffic.
+//
+// Spread and contract work on tiles of T^3 mesh nodes.  Beads are binned by the tile
+// that holds the first node of their P^3 window; one CTA owns a tile and a
+// (T+P-1)^3 shared-memory halo buffer.  Spread accumulates every bead of the tile in
+// the buffer with shared-memory atomics and adds the buffer to the mesh once; contract
+// loads the buffer once and serves all beads of the tile from shared memory.  One
+// warp handles one bead: lanes compute the 3P separable Gaussian factors
+// exp(-2 xi^2 r_d^2 / eta_d) (the reference evaluates exp of their sum per node,
+// ConductorRigid.cu:219-223), then sweep the P^2 (y,z) columns with the x loop inside.
+#include <cub/cub.cuh>
+
+#include "cr_internal.cuh"
+
+namespace cr {
+
+namespace {
+
+template <typename R> struct Vec3 { R x, y, z; };
+
+struct MeshShape {
+    int Ng[3];     // mesh nodes per dimension
+    int ntd[3];    // tiles per dimension
+    int T;         // tile edge
+    int P;         // support
+    int Bd;        // halo buffer edge T + P - 1
+};
+
+template <typename R> struct WindowConst {
+    R h[3], halfL[3], inv_eta[3];
+    R xiterm;
+};
+
+__device__ __forceinline__ int wrapmod(int s, int n) {
+    int r = s % n;
+    return r < 0 ? r + n : r;
+}
+
+__device__ __forceinline__ float dexp(float x) { return __expf(x); }
+__device__ __forceinline__ double dexp(double x) { return exp(x); }
+
+template <typename R> __device__ __forceinline__ R warp_sum(R v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Per-warp Gaussian factors for one bead: w[d*P + t] = exp(-xiterm (node - x)^2 / eta_d)
+// with node = h_d (start_d + t) - L_d/2 (ConductorRigid.cu:212-223); u[d*P + t] =
+// (x - node)/eta_d for the force.
+template <typename R, bool WANT_U>
+__device__ __forceinline__ void window_factors(const WindowConst<R> &wc, int P, R px, R py, R pz, int4 s,
+                                               R *w, R *u, int lane) {
+    for (int t = lane; t < 3 * P; t += 32) {
+        int d = t >= 2 * P ? 2 : (t >= P ? 1 : 0);
+        int tt = t - d * P;
+        R x = d == 0 ? px : (d == 1 ? py : pz);
+        int st = d == 0 ? s.x : (d == 1 ? s.y : s.z);
+        R r = wc.h[d] * (R)(st + tt) - wc.halfL[d] - x;
+        w[t] = dexp(-wc.xiterm * r * r * wc.inv_eta[d]);
+        if (WANT_U) u[t] = -r * wc.inv_eta[d];
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) spread_tiles_kernel(
+    const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
+    const int *__restrict__ tile_start, const int *__restrict__ tile_beads, MeshShape ms, WindowConst<R> wc,
+    R prefac, R *__restrict__ grid) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *buf = reinterpret_cast<R *>(smem_raw);
+    const int Bd = ms.Bd, P = ms.P, T = ms.T;
+    const int nbuf = Bd * Bd * Bd;
+    const int tile = blockIdx.x;
+    const int b0 = tile_start[tile], b1 = tile_start[tile + 1];
+    if (b0 == b1) return;  // uniform across the block
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    R *w = buf + nbuf + warp * 3 * P;
+    for (int i = threadIdx.x; i < nbuf; i += blockDim.x) buf[i] = (R)0;
+    __syncthreads();
+    const int tz = tile % ms.ntd[2], ty = (tile / ms.ntd[2]) % ms.ntd[1], tx = tile / (ms.ntd[2] * ms.ntd[1]);
+    for (int k = b0 + warp; k < b1; k += nw) {
+        const int i = tile_beads[k];
+        const typename Prec<R>::R4 p = pos[i];
+        const int4 s = wstart[i];
+        window_factors<R, false>(wc, P, p.x, p.y, p.z, s, w, nullptr, lane);
+        __syncwarp();
+        const int ox = wrapmod(s.x, ms.Ng[0]) - tx * T;
+        const int oy = wrapmod(s.y, ms.Ng[1]) - ty * T;
+        const int oz = wrapmod(s.z, ms.Ng[2]) - tz * T;
+        const R c = prefac * q[i];
+        if (ox >= 0 && ox < T && oy >= 0 && oy < T && oz >= 0 && oz < T) {
+            for (int e = lane; e < P * P; e += 32) {
+                const int b = e / P, cc = e - b * P;
+                const R wyz = c * w[P + b] * w[2 * P + cc];
+                R *col = buf + ((size_t)ox * Bd + (oy + b)) * Bd + (oz + cc);
+                for (int a = 0; a < P; ++a) atomicAdd(col + (size_t)a * Bd * Bd, wyz * w[a]);
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < nbuf; n += blockDim.x) {
+        const R v = buf[n];
+        if (v == (R)0) continue;
+        const int bz = n % Bd, by = (n / Bd) % Bd, bx = n / (Bd * Bd);
+        const int gx = (tx * T + bx) % ms.Ng[0];
+        const int gy = (ty * T + by) % ms.Ng[1];
+        const int gz = (tz * T + bz) % ms.Ng[2];
+        atomicAdd(grid + ((size_t)gx * ms.Ng[1] + gy) * ms.Ng[2] + gz, v);
+    }
+}
+
+template <typename R, bool FORCE>
+__global__ void __launch_bounds__(256) contract_tiles_kernel(
+    const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
+    const int *__restrict__ tile_start, const int *__restrict__ tile_beads, MeshShape ms, WindowConst<R> wc,
+    R coeff, const R *__restrict__ grid, R *__restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *buf = reinterpret_cast<R *>(smem_raw);
+    const int Bd = ms.Bd, P = ms.P, T = ms.T;
+    const int nbuf = Bd * Bd * Bd;
+    const int tile = blockIdx.x;
+    const int b0 = tile_start[tile], b1 = tile_start[tile + 1];
+    if (b0 == b1) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    R *w = buf + nbuf + warp * 6 * P;
+    R *u = w + 3 * P;
+    const int tz = tile % ms.ntd[2], ty = (tile / ms.ntd[2]) % ms.ntd[1], tx = tile / (ms.ntd[2] * ms.ntd[1]);
+    for (int n = threadIdx.x; n < nbuf; n += blockDim.x) {
+        const int bz = n % Bd, by = (n / Bd) % Bd, bx = n / (Bd * Bd);
+        const int gx = (tx * T + bx) % ms.Ng[0];
+        const int gy = (ty * T + by) % ms.Ng[1];
+        const int gz = (tz * T + bz) % ms.Ng[2];
+        buf[n] = grid[((size_t)gx * ms.Ng[1] + gy) * ms.Ng[2] + gz];
+    }
+    __syncthreads();
+    for (int k = b0 + warp; k < b1; k += nw) {
+        const int i = tile_beads[k];
+        const typename Prec<R>::R4 p = pos[i];
+        const int4 s = wstart[i];
+        window_factors<R, FORCE>(wc, P, p.x, p.y, p.z, s, w, u, lane);
+        __syncwarp();
+        const int ox = wrapmod(s.x, ms.Ng[0]) - tx * T;
+        const int oy = wrapmod(s.y, ms.Ng[1]) - ty * T;
+        const int oz = wrapmod(s.z, ms.Ng[2]) - tz * T;
+        R acc = 0, fx = 0, fy = 0, fz = 0;
+        if (ox >= 0 && ox < T && oy >= 0 && oy < T && oz >= 0 && oz < T) {
+            for (int e = lane; e < P * P; e += 32) {
+                const int b = e / P, cc = e - b * P;
+                const R wyz = w[P + b] * w[2 * P + cc];
+                const R *col = buf + ((size_t)ox * Bd + (oy + b)) * Bd + (oz + cc);
+                R s0 = 0, sx = 0;
+                for (int a = 0; a < P; ++a) {
+                    const R g = w[a] * col[(size_t)a * Bd * Bd];
+                    s0 += g;
+                    if (FORCE) sx += g * u[a];
+                }
+                if (FORCE) {
+                    fx += wyz * sx;
+                    fy += wyz * s0 * u[P + b];
+                    fz += wyz * s0 * u[2 * P + cc];
+                } else {
+                    acc += wyz * s0;
+                }
+            }
+        }
+        if (FORCE) {
+            fx = warp_sum(fx);
+            fy = warp_sum(fy);
+            fz = warp_sum(fz);
+            if (lane == 0) {
+                const R c = coeff * q[i];  // 2 quadW prefac xiterm q_i (ConductorRigid.cu:449,1274)
+                out[3 * (size_t)i + 0] = c * fx;
+                out[3 * (size_t)i + 1] = c * fy;
+                out[3 * (size_t)i + 2] = c * fz;
+            }
+        } else {
+            acc = warp_sum(acc);
+            if (lane == 0) out[i] = coeff * acc;  // quadW prefac (ConductorRigid.cu:936-937)
+        }
+        __syncwarp();
+    }
+}
+
+template <typename R, typename C>
+__global__ void scale_kernel(C *__restrict__ spec, const R *__restrict__ scale, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const R s = scale[i];
+        C v = spec[i];
+        v.x *= s;
+        v.y *= s;
+        spec[i] = v;
+    }
+}
+
+// Influence function on the half spectrum (ConductorRigid.cc:245-274): for k != 0,
+// j0(|k|)^2 exp(-sum_d (1 - eta_d) k_d^2 / (4 xi^2)) / |k|^2 / Ngrid with j0 = sin x / x.
+template <typename R>
+__global__ void scale_init_kernel(R *scale, int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                                  double ex, double ey, double ez, double xi) {
+    const int Nzh = Nz / 2 + 1;
+    const long n = (long)Nx * Ny * Nzh;
+    long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const int k = (int)(idx % Nzh);
+    const int j = (int)((idx / Nzh) % Ny);
+    const int i = (int)(idx / ((long)Nzh * Ny));
+    const double kx = ((i < (Nx + 1) / 2) ? i : i - Nx) * 2.0 * kPi / Lx;
+    const double ky = ((j < (Ny + 1) / 2) ? j : j - Ny) * 2.0 * kPi / Ly;
+    const double kz = ((k < (Nz + 1) / 2) ? k : k - Nz) * 2.0 * kPi / Lz;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    if (i == 0 && j == 0 && k == 0) {
+        scale[idx] = (R)0;
+        return;
+    }
+    const double etak2 = (1.0 - ex) * kx * kx + (1.0 - ey) * ky * ky + (1.0 - ez) * kz * kz;
+    const double kk = sqrt(k2);
+    const double j0 = sin(kk) / kk;
+    scale[idx] = (R)(j0 * j0 * exp(-etak2 / (4.0 * xi * xi)) / k2 / ((double)Nx * Ny * Nz));
+}
+
+template <typename R> __global__ void cast_kernel(const double *__restrict__ in, R *__restrict__ out, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (R)in[i];
+}
+
+template <typename R> MeshShape mesh_shape(const cr_handle *h) {
+    MeshShape ms;
+    for (int d = 0; d < 3; ++d) {
+        ms.Ng[d] = h->d.grid[d];
+        ms.ntd[d] = h->ntiles_dim[d];
+    }
+    ms.T = h->tile;
+    ms.P = h->d.support;
+    ms.Bd = h->tile + h->d.support - 1;
+    return ms;
+}
+
+template <typename R> WindowConst<R> window_const(const cr_handle *h) {
+    WindowConst<R> wc;
+    for (int d = 0; d < 3; ++d) {
+        wc.h[d] = (R)h->d.h[d];
+        wc.halfL[d] = (R)(0.5 * h->L[d]);
+        wc.inv_eta[d] = (R)(1.0 / h->d.eta[d]);
+    }
+    wc.xiterm = (R)h->d.xiterm;
+    return wc;
+}
+
+template <typename R> size_t spread_smem(const cr_handle *h) {
+    const int Bd = h->tile + h->d.support - 1;
+    return ((size_t)Bd * Bd * Bd + 8 * 3 * (size_t)h->d.support) * sizeof(R);
+}
+template <typename R> size_t contract_smem(const cr_handle *h) {
+    const int Bd = h->tile + h->d.support - 1;
+    return ((size_t)Bd * Bd * Bd + 8 * 6 * (size_t)h->d.support) * sizeof(R);
+}
+
+}  // namespace
+
+template <typename R> int mesh_init(cr_handle *h, MeshBuffers<R> &m) {
+    typedef typename Prec<R>::R4 R4;
+    typedef typename Prec<R>::R2 R2;
+    typedef typename Prec<R>::C C;
+    mesh_free(m);
+    const int N = h->N;
+    const long G = grid_size(h), S = spec_size(h);
+    const int nt = h->d.n_table + 1;
+    CR_TRY(dalloc(h, &m.pos, (size_t)N));
+    CR_TRY(dalloc(h, &m.q, (size_t)N));
+    CR_TRY(dalloc(h, &m.phi, (size_t)N));
+    CR_TRY(dalloc(h, &m.force, 3 * (size_t)N));
+    CR_TRY(dalloc(h, &m.phiq, (size_t)nt));
+    CR_TRY(dalloc(h, &m.gradphiq, (size_t)nt));
+    CR_TRY(dalloc(h, &m.grid, (size_t)G));
+    CR_TRY(dalloc(h, &m.spec, (size_t)S));
+    CR_TRY(dalloc(h, &m.scale, (size_t)S));
+    std::vector<R2> t1(nt), t2(nt);
+    for (int i = 0; i < nt; ++i) {
+        t1[i].x = (R)h->h_phiq[2 * i];
+        t1[i].y = (R)h->h_phiq[2 * i + 1];
+        t2[i].x = (R)h->h_gradphiq[2 * i];
+        t2[i].y = (R)h->h_gradphiq[2 * i + 1];
+    }
+    CR_CUDA(h, cudaMemcpy(m.phiq, t1.data(), nt * sizeof(R2), cudaMemcpyHostToDevice));
+    CR_CUDA(h, cudaMemcpy(m.gradphiq, t2.data(), nt * sizeof(R2), cudaMemcpyHostToDevice));
+    scale_init_kernel<R><<<blocks_for(S, 256), 256>>>(m.scale, h->d.grid[0], h->d.grid[1], h->d.grid[2], h->L[0],
+                                                       h->L[1], h->L[2], h->d.eta[0], h->d.eta[1], h->d.eta[2],
+                                                       h->user.xi);
+    CR_LAUNCH(h, "scale_init_kernel");
+    CR_CUFFT(h, cufftPlan3d(&m.plan_fwd, h->d.grid[0], h->d.grid[1], h->d.grid[2], Prec<R>::kR2C));
+    CR_CUFFT(h, cufftPlan3d(&m.plan_inv, h->d.grid[0], h->d.grid[1], h->d.grid[2], Prec<R>::kC2R));
+    size_t s1 = spread_smem<R>(h), s2 = contract_smem<R>(h);
+    if (s1 > 227 * 1024 || s2 > 227 * 1024)
+        return fail(h, CR_BAD_PARAM, "support too large for the shared-memory tile buffer");
+    CR_CUDA(h, cudaFuncSetAttribute(spread_tiles_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+    CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)s2));
+    CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)s2));
+    CR_CUDA(h, cudaDeviceSynchronize());
+    m.ready = true;
+    (void)sizeof(R4);
+    (void)sizeof(C);
+    return CR_OK;
+}
+
+template <typename R> void mesh_free(MeshBuffers<R> &m) {
+    dfree(&m.pos);
+    dfree(&m.q);
+    dfree(&m.phi);
+    dfree(&m.force);
+    dfree(&m.phiq);
+    dfree(&m.gradphiq);
+    dfree(&m.grid);
+    dfree(&m.spec);
+    dfree(&m.scale);
+    if (m.plan_fwd) cufftDestroy(m.plan_fwd);
+    if (m.plan_inv) cufftDestroy(m.plan_inv);
+    m.plan_fwd = m.plan_inv = 0;
+    m.ready = false;
+}
+
+template <typename R> int cast_charges(cr_handle *h, MeshBuffers<R> &m, const double *d_q) {
+    cast_kernel<R><<<blocks_for(h->N, 256), 256, 0, h->stream>>>(d_q, m.q, h->N);
+    CR_LAUNCH(h, "cast_kernel");
+    return CR_OK;
+}
+
+template <typename R> __global__ void to_double_kernel(const R *__restrict__ in, double *__restrict__ out, long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (double)in[i];
+}
+
+template <typename R> int cast_to_double(cr_handle *h, const R *in, double *out, long n) {
+    if (n == 0) return CR_OK;
+    to_double_kernel<R><<<blocks_for(n, 256), 256, 0, h->stream>>>(in, out, n);
+    CR_LAUNCH(h, "to_double_kernel");
+    return CR_OK;
+}
+
+template <typename R> int spread_only(cr_handle *h, MeshBuffers<R> &m) {
+    const long G = grid_size(h);
+    CR_CUDA(h, cudaMemsetAsync(m.grid, 0, G * sizeof(R), h->stream));
+    spread_tiles_kernel<R><<<h->ntiles, 256, spread_smem<R>(h), h->stream>>>(
+        m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
+        (R)h->d.prefac, m.grid);
+    CR_LAUNCH(h, "spread_tiles_kernel");
+    return CR_OK;
+}
+
+template <typename R> static int wave_mesh(cr_handle *h, MeshBuffers<R> &m) {
+    CR_TRY(spread_only(h, m));
+    CR_CUFFT(h, cufftSetStream(m.plan_fwd, h->stream));
+    CR_CUFFT(h, cufftSetStream(m.plan_inv, h->stream));
+    CR_CUFFT(h, fft_forward(m.plan_fwd, m.grid, m.spec));
+    const int S = spec_size(h);
+    scale_kernel<R, typename Prec<R>::C><<<blocks_for(S, 256), 256, 0, h->stream>>>(m.spec, m.scale, S);
+    CR_LAUNCH(h, "scale_kernel");
+    CR_CUFFT(h, fft_inverse(m.plan_inv, m.spec, m.grid));
+    return CR_OK;
+}
+
+template <typename R> int wave_potential(cr_handle *h, MeshBuffers<R> &m) {
+    CR_TRY(wave_mesh(h, m));
+    contract_tiles_kernel<R, false><<<h->ntiles, 256, contract_smem<R>(h), h->stream>>>(
+        m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
+        (R)(h->d.quadW * h->d.prefac), m.grid, m.phi);
+    CR_LAUNCH(h, "contract_tiles_kernel");
+    return CR_OK;
+}
+
+template <typename R> int wave_force(cr_handle *h, MeshBuffers<R> &m) {
+    CR_TRY(wave_mesh(h, m));
+    contract_tiles_kernel<R, true><<<h->ntiles, 256, contract_smem<R>(h), h->stream>>>(
+        m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
+        (R)(2.0 * h->d.quadW * h->d.prefac * h->d.xiterm), m.grid, m.force);
+    CR_LAUNCH(h, "contract_force_tiles_kernel");
+    return CR_OK;
+}
+
+template int mesh_init<float>(cr_handle *, MeshBuffers<float> &);
+template int mesh_init<double>(cr_handle *, MeshBuffers<double> &);
+template void mesh_free<float>(MeshBuffers<float> &);
+template void mesh_free<double>(MeshBuffers<double> &);
+template int cast_charges<float>(cr_handle *, MeshBuffers<float> &, const double *);
+template int cast_charges<double>(cr_handle *, MeshBuffers<double> &, const double *);
+template int cast_to_double<float>(cr_handle *, const float *, double *, long);
+template int cast_to_double<double>(cr_handle *, const double *, double *, long);
+template int spread_only<float>(cr_handle *, MeshBuffers<float> &);
+template int spread_only<double>(cr_handle *, MeshBuffers<double> &);
+template int wave_potential<float>(cr_handle *, MeshBuffers<float> &);
+template int wave_potential<double>(cr_handle *, MeshBuffers<double> &);
+template int wave_force<float>(cr_handle *, MeshBuffers<float> &);
+template int wave_force<double>(cr_handle *, MeshBuffers<double> &);
+
+}  // namespace cr

@@ -1,0 +1,324 @@
+// solver.cu -- matrix-free flexible GMRES for the saddle-point system.
+//
+// Replaces the reference's cusp::krylov::gmres(M, q, rhs, 10, monitor, Pr) call
+// (ConductorRigid.cu:1134-1136): restarted GMRES with the same diagonal
+// preconditioner and warm start.  Differences, all of which leave the fixed point
+// A x = b untouched:
+//   - the preconditioner is applied on the right (flexible GMRES, so a varying
+//     preconditioner such as the learned correction is allowed), and convergence is
+//     judged on the true residual ||b - A x|| <= tol ||b|| recomputed with the FP64
+//     operator, where CUSP stops on the left-preconditioned residual;
+//   - the Krylov basis, Gram-Schmidt dot products (classical Gram-Schmidt with one
+//     reorthogonalisation), Givens rotations and the least-squares update are FP64;
+//   - CR_MIXED runs the inner iterations with the FP32 operator and wraps them in
+//     FP64 iterative refinement: r = b - A64 x, solve A32 d ~= r, x += d.
+// All vectors stay on the device; each Arnoldi step copies its j+2 Hessenberg
+// entries to pinned host memory for the Givens update (one small copy per step).
+#include <cmath>
+
+#include "cr_internal.cuh"
+
+namespace cr {
+
+namespace {
+
+constexpr int kDotThreads = 256;
+
+// partial[blk * k + j] = sum over this block's rows of V_j[i] * w[i]   (j < k)
+__global__ void __launch_bounds__(kDotThreads) multi_dot_kernel(int n, int k, const double *__restrict__ V,
+                                                                const double *__restrict__ w,
+                                                                double *__restrict__ partial) {
+    __shared__ double red[kDotThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = 0; j < k; ++j) {
+        const double *v = V + (size_t)j * n;
+        double s = 0.0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += v[i] * w[i];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) red[warp] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int q = 0; q < kDotThreads / 32; ++q) t += red[q];
+            partial[(size_t)blockIdx.x * k + j] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// out[j] = sum_blk partial[blk * k + j], in block order (deterministic).
+__global__ void reduce_partials_kernel(int nblk, int k, const double *__restrict__ partial, double *__restrict__ out) {
+    const int j = blockIdx.x;
+    const int lane = threadIdx.x;
+    double s = 0.0;
+    for (int b = lane; b < nblk; b += 32) s += partial[(size_t)b * k + j];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[j] = s;
+}
+
+// w -= sum_j h[j] V_j
+__global__ void project_kernel(int n, int k, const double *__restrict__ V, const double *__restrict__ hv,
+                               double *__restrict__ w) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = w[i];
+        for (int j = 0; j < k; ++j) s -= hv[j] * V[(size_t)j * n + i];
+        w[i] = s;
+    }
+}
+
+__global__ void scale_kernel(int n, double a, const double *__restrict__ x, double *__restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a * x[i];
+}
+
+// y = b - y
+__global__ void residual_kernel(int n, const double *__restrict__ b, double *__restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = b[i] - y[i];
+}
+
+// x += sum_j c[j] Z_j
+__global__ void update_kernel(int n, int k, const double *__restrict__ Z, const double *__restrict__ c,
+                              double *__restrict__ x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = x[i];
+        for (int j = 0; j < k; ++j) s += c[j] * Z[(size_t)j * n + i];
+        x[i] = s;
+    }
+}
+
+__global__ void axpy_kernel(int n, double a, const double *__restrict__ x, double *__restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
+}
+
+int vec_blocks(int n) { return std::max(1, std::min(4 * 148, blocks_for(n, 256))); }
+
+// hcol[0..k) = V[0..k)^T w   (device result)
+int dots(cr_handle *h, int k, const double *V, const double *w, double *out) {
+    Krylov &K = h->kry;
+    multi_dot_kernel<<<K.nblocks, kDotThreads, 0, h->stream>>>(K.n, k, V, w, K.partial);
+    CR_LAUNCH(h, "multi_dot_kernel");
+    reduce_partials_kernel<<<k, 32, 0, h->stream>>>(K.nblocks, k, K.partial, out);
+    CR_LAUNCH(h, "reduce_partials_kernel");
+    return CR_OK;
+}
+
+int norm(cr_handle *h, const double *v, double *result) {
+    Krylov &K = h->kry;
+    CR_TRY(dots(h, 1, v, v, K.hcol));
+    CR_CUDA(h, cudaMemcpyAsync(K.h_pinned, K.hcol, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CR_CUDA(h, cudaStreamSynchronize(h->stream));
+    *result = std::sqrt(std::max(0.0, K.h_pinned[0]));
+    return CR_OK;
+}
+
+struct OpCount {
+    int fp64 = 0, fp32 = 0;
+};
+
+int op_apply(cr_handle *h, int precision, const double *x, double *y, OpCount &oc) {
+    if (precision == CR_FP64) ++oc.fp64;
+    else ++oc.fp32;
+    return apply_operator(h, x, y, precision);
+}
+
+// Restarted right-preconditioned FGMRES(m) on A_prec x = b with absolute tolerance
+// `atol` on ||b - A_prec x||.  x holds the initial guess.  Returns CR_OK or
+// CR_NOT_CONVERGED; *iters accumulates iterations, *restarts restart cycles.
+enum { kResidualCompute = 0, kResidualIsB = 1, kResidualReady = 2 };
+
+int fgmres(cr_handle *h, int precision, double *x, const double *b, int r_mode, double atol, int maxit,
+           int *iters, int *restarts, double *final_norm, OpCount &oc) {
+    Krylov &K = h->kry;
+    const int n = K.n, m = K.m;
+    const int nb = vec_blocks(n);
+    double *r = K.r;
+    if (r_mode == kResidualIsB) {
+        CR_CUDA(h, cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    } else if (r_mode == kResidualCompute) {
+        CR_TRY(op_apply(h, precision, x, r, oc));
+        residual_kernel<<<nb, 256, 0, h->stream>>>(n, b, r);
+        CR_LAUNCH(h, "residual_kernel");
+    }
+    double beta = 0;
+    CR_TRY(norm(h, r, &beta));
+    if (!std::isfinite(beta)) return fail(h, CR_NUMERICAL, "non-finite residual");
+    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), y(m);
+    int it = 0;
+    while (beta > atol && it < maxit) {
+        scale_kernel<<<nb, 256, 0, h->stream>>>(n, 1.0 / beta, r, K.V);
+        CR_LAUNCH(h, "scale_kernel");
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int j = 0;
+        bool stop = false;
+        for (; j < m && it < maxit && !stop; ++j) {
+            double *vj = K.V + (size_t)j * n;
+            double *zj = K.Z + (size_t)j * n;
+            CR_TRY(precondition(h, vj, zj));
+            CR_TRY(op_apply(h, precision, zj, K.w, oc));
+            // classical Gram-Schmidt, twice
+            CR_TRY(dots(h, j + 1, K.V, K.w, K.hcol));
+            project_kernel<<<nb, 256, 0, h->stream>>>(n, j + 1, K.V, K.hcol, K.w);
+            CR_LAUNCH(h, "project_kernel");
+            CR_TRY(dots(h, j + 1, K.V, K.w, K.hcol + (m + 1)));
+            project_kernel<<<nb, 256, 0, h->stream>>>(n, j + 1, K.V, K.hcol + (m + 1), K.w);
+            CR_LAUNCH(h, "project_kernel");
+            CR_TRY(dots(h, 1, K.w, K.w, K.hcol + 2 * (m + 1)));
+            CR_CUDA(h, cudaMemcpyAsync(K.h_pinned, K.hcol, 3 * (m + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                                       h->stream));
+            CR_CUDA(h, cudaStreamSynchronize(h->stream));
+            const double *h1 = K.h_pinned, *h2 = K.h_pinned + (m + 1);
+            const double hn = std::sqrt(std::max(0.0, K.h_pinned[2 * (m + 1)]));
+            if (!std::isfinite(hn)) return fail(h, CR_NUMERICAL, "non-finite Arnoldi norm");
+            for (int k = 0; k <= j; ++k) H[(size_t)k * m + j] = h1[k] + h2[k];
+            H[(size_t)(j + 1) * m + j] = hn;
+            if (hn > 0) {
+                scale_kernel<<<nb, 256, 0, h->stream>>>(n, 1.0 / hn, K.w, K.V + (size_t)(j + 1) * n);
+                CR_LAUNCH(h, "scale_kernel");
+            }
+            for (int k = 0; k < j; ++k) {
+                const double a = H[(size_t)k * m + j], c = H[(size_t)(k + 1) * m + j];
+                H[(size_t)k * m + j] = cs[k] * a + sn[k] * c;
+                H[(size_t)(k + 1) * m + j] = -sn[k] * a + cs[k] * c;
+            }
+            const double a = H[(size_t)j * m + j], c = H[(size_t)(j + 1) * m + j];
+            const double den = std::hypot(a, c);
+            cs[j] = den > 0 ? a / den : 1.0;
+            sn[j] = den > 0 ? c / den : 0.0;
+            H[(size_t)j * m + j] = den;
+            H[(size_t)(j + 1) * m + j] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            ++it;
+            if (std::fabs(g[j + 1]) <= atol || hn == 0.0) stop = true;
+        }
+        // y = H^{-1} g (upper triangular j x j), x += Z y
+        for (int rr = j - 1; rr >= 0; --rr) {
+            double acc = g[rr];
+            for (int k = rr + 1; k < j; ++k) acc -= H[(size_t)rr * m + k] * y[k];
+            y[rr] = H[(size_t)rr * m + rr] != 0.0 ? acc / H[(size_t)rr * m + rr] : 0.0;
+        }
+        CR_CUDA(h, cudaMemcpyAsync(K.yvec, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        update_kernel<<<nb, 256, 0, h->stream>>>(n, j, K.Z, K.yvec, x);
+        CR_LAUNCH(h, "update_kernel");
+        ++*restarts;
+        // true residual of this operator
+        CR_TRY(op_apply(h, precision, x, r, oc));
+        residual_kernel<<<nb, 256, 0, h->stream>>>(n, b, r);
+        CR_LAUNCH(h, "residual_kernel");
+        CR_TRY(norm(h, r, &beta));
+        if (!std::isfinite(beta)) return fail(h, CR_NUMERICAL, "non-finite residual");
+    }
+    *iters += it;
+    *final_norm = beta;
+    return beta <= atol ? CR_OK : CR_NOT_CONVERGED;
+}
+
+}  // namespace
+
+int krylov_alloc(cr_handle *h) {
+    Krylov &K = h->kry;
+    krylov_free(h);
+    K.n = h->N + h->B;
+    K.m = h->user.restart > 0 ? h->user.restart : 10;
+    K.nblocks = vec_blocks(K.n);
+    const size_t n = (size_t)K.n, m = (size_t)K.m;
+    CR_TRY(dalloc(h, &K.V, (m + 1) * n));
+    CR_TRY(dalloc(h, &K.Z, m * n));
+    CR_TRY(dalloc(h, &K.w, n));
+    CR_TRY(dalloc(h, &K.r, n));
+    CR_TRY(dalloc(h, &K.b, n));
+    CR_TRY(dalloc(h, &K.x, n));
+    CR_TRY(dalloc(h, &K.d, n));
+    CR_TRY(dalloc(h, &K.rr, n));
+    CR_TRY(dalloc(h, &K.partial, (size_t)K.nblocks * (m + 2)));
+    CR_TRY(dalloc(h, &K.hcol, 3 * (m + 1)));
+    CR_TRY(dalloc(h, &K.yvec, m));
+    CR_CUDA(h, cudaMallocHost((void **)&K.h_pinned, 3 * (m + 1) * sizeof(double)));
+    return CR_OK;
+}
+
+void krylov_free(cr_handle *h) {
+    Krylov &K = h->kry;
+    dfree(&K.V);
+    dfree(&K.Z);
+    dfree(&K.w);
+    dfree(&K.r);
+    dfree(&K.b);
+    dfree(&K.x);
+    dfree(&K.d);
+    dfree(&K.rr);
+    dfree(&K.partial);
+    dfree(&K.hcol);
+    dfree(&K.yvec);
+    if (K.h_pinned) cudaFreeHost(K.h_pinned);
+    K.h_pinned = nullptr;
+}
+
+int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {
+    Krylov &K = h->kry;
+    const int n = K.n;
+    const int nb = vec_blocks(n);
+    const double tol = h->user.gmres_tol > 0 ? h->user.gmres_tol : h->user.errortol;
+    const int maxit = h->user.maxiter > 0 ? h->user.maxiter : 100;
+    cr_solve_stats s{};
+    OpCount oc;
+    double bnorm = 0, rnorm = 0;
+    CR_TRY(norm(h, b, &bnorm));
+    if (!std::isfinite(bnorm)) return fail(h, CR_NUMERICAL, "non-finite right-hand side");
+    const double atol = tol * bnorm;
+    // initial FP64 residual r0 = b - A x0
+    CR_TRY(op_apply(h, CR_FP64, x, K.r, oc));
+    residual_kernel<<<nb, 256, 0, h->stream>>>(n, b, K.r);
+    CR_LAUNCH(h, "residual_kernel");
+    CR_TRY(norm(h, K.r, &rnorm));
+    if (!std::isfinite(rnorm)) return fail(h, CR_NUMERICAL, "non-finite residual");
+    s.initial_residual = bnorm > 0 ? rnorm / bnorm : rnorm;
+    int status = CR_OK;
+    if (h->user.precision != CR_MIXED) {
+        status = fgmres(h, h->user.precision == CR_FP32 ? CR_FP32 : CR_FP64, x, b, kResidualReady, atol, maxit,
+                        &s.iterations, &s.restarts, &rnorm, oc);
+        if (status != CR_OK && status != CR_NOT_CONVERGED) return status;
+    } else {
+        // FP64 iterative refinement around FP32 inner solves: K.rr = b - A64 x,
+        // solve A32 d ~= K.rr from d = 0, x += d.
+        CR_CUDA(h, cudaMemcpyAsync(K.rr, K.r, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        for (int outer = 0; outer < 20; ++outer) {
+            if (rnorm <= atol || s.iterations >= maxit) break;
+            ++s.refinements;
+            // inner accuracy: enough to land below the target, not below the FP32 floor
+            const double inner_rel = std::min(0.5, std::max(0.3 * atol / rnorm, 1e-5));
+            CR_CUDA(h, cudaMemsetAsync(K.d, 0, n * sizeof(double), h->stream));
+            double inner_norm = 0;
+            int ist = fgmres(h, CR_FP32, K.d, K.rr, kResidualIsB, inner_rel * rnorm, maxit - s.iterations,
+                             &s.iterations, &s.restarts, &inner_norm, oc);
+            if (ist != CR_OK && ist != CR_NOT_CONVERGED) return ist;
+            axpy_kernel<<<nb, 256, 0, h->stream>>>(n, 1.0, K.d, x);
+            CR_LAUNCH(h, "axpy_kernel");
+            CR_TRY(op_apply(h, CR_FP64, x, K.rr, oc));
+            residual_kernel<<<nb, 256, 0, h->stream>>>(n, b, K.rr);
+            CR_LAUNCH(h, "residual_kernel");
+            CR_TRY(norm(h, K.rr, &rnorm));
+            if (!std::isfinite(rnorm)) return fail(h, CR_NUMERICAL, "non-finite residual");
+        }
+        status = rnorm <= atol ? CR_OK : CR_NOT_CONVERGED;
+    }
+    if (h->user.precision == CR_FP32) {
+        // the FP32 loop judged its own operator; report the FP64 residual
+        CR_TRY(op_apply(h, CR_FP64, x, K.w, oc));
+        residual_kernel<<<nb, 256, 0, h->stream>>>(n, b, K.w);
+        CR_LAUNCH(h, "residual_kernel");
+        CR_TRY(norm(h, K.w, &rnorm));
+    }
+    s.final_residual = bnorm > 0 ? rnorm / bnorm : rnorm;
+    s.converged = rnorm <= atol ? 1 : 0;
+    s.matvecs_fp64 = oc.fp64;
+    s.matvecs_fp32 = oc.fp32;
+    if (st) {
+        const double ms = st->solve_ms;
+        *st = s;
+        st->solve_ms = ms;
+    }
+    return s.converged ? CR_OK : (status == CR_OK ? CR_NOT_CONVERGED : status);
+}
+
+}  // namespace cr

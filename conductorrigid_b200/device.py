@@ -1,0 +1,170 @@
+"""Handle-level wrapper of the C ABI over device arrays.
+
+PyTorch provides device memory and streams only; every computation is a call into
+libconductor_rigid.so.  Arrays are float64 CUDA tensors; positions are (N, 3).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Handle:
+    """One cr_handle: parameters, tables, mesh, FFT plans and workspaces."""
+
+    def __init__(self, params: _lib.CrParams, L, stream=None):
+        import torch
+
+        self.torch = torch
+        self.L = np.ascontiguousarray(np.broadcast_to(np.asarray(L, dtype=np.float64), (3,)))
+        self.params = params
+        self.h = C.c_void_p()
+        _lib.check(_lib.lib().cr_create(C.byref(params), _lib.dptr(self.L), C.byref(self.h)), "cr_create")
+        if stream is not None:
+            self.set_stream(stream)
+        self.N = 0
+        self.B = 0
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if self.h:
+            _lib.lib().cr_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, where, allow=(_lib.CR_OK,)):
+        return _lib.check(st, where, self.h, allow)
+
+    def set_stream(self, stream):
+        self._check(_lib.lib().cr_set_stream(self.h, C.c_void_p(stream.cuda_stream)), "cr_set_stream")
+
+    def derived(self) -> _lib.CrDerived:
+        d = _lib.CrDerived()
+        self._check(_lib.lib().cr_get_derived(self.h, C.byref(d)), "cr_get_derived")
+        return d
+
+    def set_field(self, field):
+        f = np.ascontiguousarray(field, dtype=np.float64)
+        self._check(_lib.lib().cr_set_field(self.h, _lib.dptr(f)), "cr_set_field")
+
+    def set_params(self, params: _lib.CrParams, L=None):
+        if L is not None:
+            self.L = np.ascontiguousarray(np.broadcast_to(np.asarray(L, dtype=np.float64), (3,)))
+        self.params = params
+        self._check(_lib.lib().cr_set_params(self.h, C.byref(params), _lib.dptr(self.L)), "cr_set_params")
+
+    def set_topology(self, body, rigid, body_charge):
+        body = np.ascontiguousarray(body, dtype=np.uint32)
+        rigid = np.ascontiguousarray(rigid, dtype=np.uint8)
+        Q = np.ascontiguousarray(body_charge, dtype=np.float64)
+        self._check(_lib.lib().cr_set_topology(self.h, len(body), body.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                               len(Q), rigid.ctypes.data_as(C.POINTER(C.c_uint8)), _lib.dptr(Q)),
+                    "cr_set_topology")
+        self.N, self.B = len(body), len(Q)
+
+    # -- device helpers ------------------------------------------------------
+    def dev(self, a):
+        t = self.torch
+        if isinstance(a, t.Tensor):
+            return a.to(device="cuda", dtype=t.float64).contiguous()
+        return t.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+
+    def empty(self, *shape):
+        return self.torch.empty(*shape, dtype=self.torch.float64, device="cuda")
+
+    # -- operators -----------------------------------------------------------
+    def set_positions(self, pos, body_pos):
+        self._pos = self.dev(pos).reshape(-1, 3)
+        self._bpos = self.dev(body_pos).reshape(-1, 3)
+        self._check(_lib.lib().cr_set_positions(self.h, _ptr(self._pos), _ptr(self._bpos)), "cr_set_positions")
+
+    def apply_operator(self, x, precision=_lib.CR_FP64):
+        x = self.dev(x)
+        y = self.empty(self.N + self.B)
+        self._check(_lib.lib().cr_apply_operator(self.h, _ptr(x), _ptr(y), int(precision)), "cr_apply_operator")
+        return y
+
+    def precondition(self, x):
+        x = self.dev(x)
+        y = self.empty(self.N + self.B)
+        self._check(_lib.lib().cr_precondition(self.h, _ptr(x), _ptr(y)), "cr_precondition")
+        return y
+
+    def objective(self):
+        y = self.empty(self.N + self.B)
+        self._check(_lib.lib().cr_objective(self.h, _ptr(y)), "cr_objective")
+        return y
+
+    def wave_potential(self, q, precision=_lib.CR_FP64):
+        q = self.dev(q)
+        y = self.empty(self.N)
+        self._check(_lib.lib().cr_wave_potential(self.h, _ptr(q), _ptr(y), int(precision)), "cr_wave_potential")
+        return y
+
+    def spread(self, q, precision=_lib.CR_FP64):
+        q = self.dev(q)
+        d = self.derived()
+        g = self.empty(d.grid[0] * d.grid[1] * d.grid[2])
+        self._check(_lib.lib().cr_spread(self.h, _ptr(q), _ptr(g), int(precision)), "cr_spread")
+        return g.reshape(d.grid[0], d.grid[1], d.grid[2])
+
+    def apply_M(self, q, precision=_lib.CR_FP64):
+        q = self.dev(q)
+        y = self.empty(self.N)
+        self._check(_lib.lib().cr_apply_M(self.h, _ptr(q), _ptr(y), int(precision)), "cr_apply_M")
+        return y
+
+    def forces(self, q, precision=_lib.CR_FP64):
+        q = self.dev(q)
+        f = self.empty(self.N, 3)
+        self._check(_lib.lib().cr_forces(self.h, _ptr(q), _ptr(f), int(precision)), "cr_forces")
+        return f
+
+    def neighbor_list(self, r_list: float):
+        t = self.torch
+        count = t.empty(self.N, dtype=t.int32, device="cuda")
+        head = t.empty(self.N, dtype=t.int64, device="cuda")
+        total = C.c_int64(0)
+        self._check(_lib.lib().cr_neighbor_list(self.h, float(r_list), _ptr(count), _ptr(head), None, 0,
+                                                C.byref(total)), "cr_neighbor_list")
+        lst = t.empty(max(total.value, 1), dtype=t.int32, device="cuda")
+        self._check(_lib.lib().cr_neighbor_list(self.h, float(r_list), _ptr(count), _ptr(head), _ptr(lst),
+                                                total.value, C.byref(total)), "cr_neighbor_list")
+        return count, head, lst[: total.value]
+
+    # -- the step --------------------------------------------------------------
+    def compute(self, pos, body_pos, q, phi, allow_not_converged=False):
+        """Device arrays in, solve + forces; q and phi are updated in place."""
+        pos = self.dev(pos).reshape(-1, 3)
+        bpos = self.dev(body_pos).reshape(-1, 3)
+        force = self.empty(self.N, 3)
+        st = _lib.CrSolveStats()
+        allow = (_lib.CR_OK, _lib.CR_NOT_CONVERGED) if allow_not_converged else (_lib.CR_OK,)
+        self._check(_lib.lib().cr_compute(self.h, _ptr(pos), _ptr(bpos), _ptr(q), _ptr(phi), _ptr(force),
+                                          C.byref(st)), "cr_compute", allow)
+        return force, st.as_dict()
+
+    def compute_host(self, pos, body_pos, q, phi, force=None, allow_not_converged=False):
+        """Host (NumPy) arrays in and out; q and phi are updated in place."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        bpos = np.ascontiguousarray(body_pos, dtype=np.float64)
+        if force is None:
+            force = np.zeros((len(q), 3))
+        st = _lib.CrSolveStats()
+        allow = (_lib.CR_OK, _lib.CR_NOT_CONVERGED) if allow_not_converged else (_lib.CR_OK,)
+        self._check(_lib.lib().cr_compute_host(self.h, _lib.dptr(pos), _lib.dptr(bpos), _lib.dptr(q),
+                                               _lib.dptr(phi), _lib.dptr(force), C.byref(st)),
+                    "cr_compute_host", allow)
+        return force, st.as_dict()

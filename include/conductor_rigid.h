@@ -1,0 +1,180 @@
+/*
+ * conductor_rigid.h -- C ABI of the B200-native induced-charge conductor solve.
+ *
+ * This is the drop-in boundary for the hot path of zeesherman/ConductorRigid: the
+ * C-style CUDA drivers of cppmodule/ConductorRigid.cuh (gpu_ZeroForce :19-21,
+ * gpu_ComputeForce :23-73, MatrixVectorMultiply :76-114, Precondition :117-129) and
+ * the parameter derivation of ConductorRigid::SetParams (ConductorRigid.cc:116-379).
+ * Plain pointers and sizes only.  Every call returns a cr_status; the reference
+ * called exit() on CUDA errors (ConductorRigid.cu:25-33) and on oversize grids
+ * (ConductorRigid.cc:181-189) and ignored GMRES non-convergence
+ * (ConductorRigid.cu:1142-1147).
+ *
+ * Conventions:
+ *   - N beads indexed 0..N-1 (the reference's active group in index order);
+ *     positions are double[N*3] (x,y,z) inside the orthorhombic box [-L/2, L/2).
+ *   - B isolated bodies: body[i] is the body tag of bead i (the reference's `body`
+ *     list, ConductorRigid.cc:88-95); rigid[b] != 0 for a rigid body (centre
+ *     body_pos[b]), 0 for a free bead; body_charge[b] is the known total charge
+ *     (the `charge` list, ConductorRigid.cc:98-105).
+ *   - Unknowns x = [q (N); Phi (B)], as in the reference's GMRES vector
+ *     (ConductorRigid.cu:1118-1128).
+ *   - "d_" arguments are device pointers, others host pointers.
+ */
+#ifndef CONDUCTOR_RIGID_H
+#define CONDUCTOR_RIGID_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CR_ABI_VERSION 1
+
+typedef enum {
+    CR_OK = 0,
+    CR_NOT_CONVERGED = 1,   /* iteration limit reached before the tolerance */
+    CR_BAD_PARAM = 2,       /* invalid argument or call order */
+    CR_CUDA_ERROR = 3,      /* CUDA / cuFFT / kernel launch failure */
+    CR_TIMEOUT = 4,         /* a bounded device wait ran out */
+    CR_OUT_OF_MEMORY = 5,
+    CR_GRID_TOO_LARGE = 6,  /* a grid dimension above 4096 (ConductorRigid.cc:181-189) */
+    CR_NOT_READY = 7,       /* topology or positions not set */
+    CR_NUMERICAL = 8        /* NaN or Inf in inputs or residuals */
+} cr_status;
+
+typedef enum {
+    CR_FP64 = 0,    /* every operator and reduction in FP64 (the plain solve) */
+    CR_MIXED = 1,   /* FP32 operator inside FP64-Arnoldi flexible GMRES, FP64 refinement */
+    CR_FP32 = 2     /* FP32 operator only (testing) */
+} cr_precision;
+
+/* User parameters.  The first five mirror the Python ConductorRigid(...) keyword
+ * arguments (pymodule/compute.py:19: field, xi, errortol); the rest are the
+ * overrides the reference hard-codes or derives from errortol. */
+typedef struct {
+    double field[3];    /* external field E0 (compute.py:19) */
+    double xi;          /* Ewald splitting parameter (compute.py:19, default 0.5) */
+    double errortol;    /* drives rc, kcut, grid, P (ConductorRigid.cc:123-207) */
+    int grid[3];        /* >0 overrides the derived grid (cc:125-178) */
+    int support;        /* >0 overrides the derived support P (cc:201) */
+    double rcut;        /* >0 overrides rc = sqrt(-ln errortol)/xi (cc:123) */
+    double gmres_tol;   /* >0 overrides the GMRES relative tolerance (errortol, cu:1134) */
+    int restart;        /* >0 overrides the GMRES restart length (10, cu:1135) */
+    int maxiter;        /* >0 overrides the iteration limit (100, cu:1134) */
+    int precision;      /* cr_precision */
+    int learned;        /* 1: use the learned initial guess / preconditioner correction */
+} cr_params;
+
+/* Derived parameters (ConductorRigid.cc:116-207, ConductorRigid.cu:912-917). */
+typedef struct {
+    int grid[3];
+    int support;            /* P after the clamp to the grid (cc:205-207) */
+    int support_unclamped;  /* P used for eta (cc:202) */
+    double h[3];
+    double eta[3];
+    double rcut;
+    double kcut;
+    int n_table;            /* entries - 1 of the real-space tables (cc:279) */
+    double dr;              /* table spacing 0.001 (cc:278) */
+    double selfcoeff;       /* shell self term (cu:917) */
+    double xiterm;          /* 2 xi^2 (cu:915) */
+    double prefac;          /* spreading prefactor (cu:916) */
+    double quadW;           /* h_x h_y h_z (cu:913) */
+} cr_derived;
+
+typedef struct {
+    int iterations;           /* Krylov iterations, all levels */
+    int restarts;             /* GMRES restart cycles */
+    int refinements;          /* outer FP64 refinement steps (CR_MIXED) */
+    int matvecs_fp64;
+    int matvecs_fp32;
+    int converged;            /* 1 when final_residual <= tolerance */
+    int used_learned_guess;   /* 1 when the network's initial guess was kept */
+    double initial_residual;  /* ||b - A x0|| / ||b|| */
+    double final_residual;    /* true FP64 relative residual ||b - A x|| / ||b|| */
+    double solve_ms;          /* device time of the solve (CUDA events) */
+} cr_solve_stats;
+
+typedef struct cr_handle cr_handle;
+
+/* ---- version and errors ---- */
+int cr_abi_version(void);
+const char *cr_status_string(int status);
+/* Message of the last failure on this handle ("" if none). */
+const char *cr_last_error(const cr_handle *h);
+
+/* ---- host-only parameter derivation (no GPU needed) ---- */
+/* SetParams derivation (ConductorRigid.cc:116-207) for box edges L. */
+int cr_derive_params(const cr_params *p, const double L[3], cr_derived *out);
+/* Real-space tables (ConductorRigid.cc:278-354): phiq and gradphiq are
+ * [n_table+1][2] doubles (.x value at (i+1)*dr, .y the next entry's value). */
+int cr_build_tables(const cr_derived *d, double xi, double *phiq, double *gradphiq);
+
+/* ---- lifecycle (ConductorRigid ctor cc:24-106 + SetParams cc:116-379) ---- */
+int cr_create(const cr_params *p, const double L[3], cr_handle **out);
+int cr_destroy(cr_handle *h);
+int cr_get_derived(const cr_handle *h, cr_derived *out);
+/* UpdateField (ConductorRigid.cc:382-387). */
+int cr_set_field(cr_handle *h, const double field[3]);
+/* UpdateParams + SetParams (ConductorRigid.cc:390-400, compute.py:58-60); keeps the
+ * topology, rebuilds tables, grid and FFT plans. */
+int cr_set_params(cr_handle *h, const cr_params *p, const double L[3]);
+/* Body topology (host arrays): body[n_beads], rigid[n_bodies], body_charge[n_bodies]. */
+int cr_set_topology(cr_handle *h, int n_beads, const uint32_t *body, int n_bodies,
+                    const uint8_t *rigid, const double *body_charge);
+/* Stream for all later work on this handle (a cudaStream_t; NULL = legacy default). */
+int cr_set_stream(cr_handle *h, void *stream);
+
+/* ---- the step (gpu_ComputeForce, ConductorRigid.cu:1153-1286) ----
+ * Solves for the bead charges and body potentials (warm start from d_q / d_phi,
+ * results written back, as the reference writes HOOMD's charges and
+ * m_isolated_potential, cu:1126-1140) and writes bead forces d_force[N*3]
+ * (overwritten, as contract_force does, cu:464).  stats may be NULL. */
+int cr_compute(cr_handle *h, const double *d_pos, const double *d_body_pos, double *d_q,
+               double *d_phi, double *d_force, cr_solve_stats *stats);
+/* Same step on host buffers: copies inputs to the device and results back. */
+int cr_compute_host(cr_handle *h, const double *pos, const double *body_pos, double *q,
+                    double *phi, double *force, cr_solve_stats *stats);
+
+/* ---- operators (for tests and custom solvers) ----
+ * cr_set_positions fixes the geometry that the operators below use. */
+int cr_set_positions(cr_handle *h, const double *d_pos, const double *d_body_pos);
+/* y = A x, x = [q; Phi], y = [Phi_b - M q; sum_b q] (MatrixVectorMultiply,
+ * ConductorRigid.cu:953-1020), with the operator in `precision` (CR_FP64/CR_FP32). */
+int cr_apply_operator(cr_handle *h, const double *d_x, double *d_y, int precision);
+/* Diagonal preconditioner (Precondition, ConductorRigid.cu:1023-1044). */
+int cr_precondition(cr_handle *h, const double *d_x, double *d_y);
+/* Right-hand side [-(r_i - R_b).E0 ; Q_b] (compute_objective, cu:764-813). */
+int cr_objective(cr_handle *h, double *d_rhs);
+/* Wave-space potential of charges q (spread, FFT, scale, inverse FFT, contract;
+ * ConductorRigid.cu:919-937). */
+int cr_wave_potential(cr_handle *h, const double *d_q, double *d_phi, int precision);
+/* Spread only: real grid [Nx][Ny][Nz] (spread, ConductorRigid.cu:144-234). */
+int cr_spread(cr_handle *h, const double *d_q, double *d_grid, int precision);
+/* M q = wave + self + real-space potential (PotentialChargeMultiply without the
+ * Phi_b subtraction, ConductorRigid.cu:862-946). */
+int cr_apply_M(cr_handle *h, const double *d_q, double *d_Mq, int precision);
+/* Bead forces for charges q (force pass, ConductorRigid.cu:1256-1278). */
+int cr_forces(cr_handle *h, const double *d_q, double *d_force, int precision);
+/* Full neighbour list within r_list of the current positions (the pair set of the
+ * reference's NeighborListGPUBinned, compute.py:38-44; both directions, no
+ * exclusions).  d_count[N], d_head[N]; d_list gets up to `capacity` entries in
+ * per-bead ascending order; *total receives the entry count (call once with
+ * capacity 0 to size the list). */
+int cr_neighbor_list(cr_handle *h, double r_list, int *d_count, int64_t *d_head, int *d_list,
+                     int64_t capacity, int64_t *total);
+
+/* ---- synthetic systems (host utilities for the benchmark workloads) ---- */
+int cr_util_icosphere_count(int level);
+int cr_util_icosphere(int level, double *verts);
+int cr_util_place_spheres(int n, const double *radii, const double L[3], uint64_t seed,
+                          int64_t max_attempts, double *centres);
+int cr_util_uniform(uint64_t seed, int64_t n, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CONDUCTOR_RIGID_H */

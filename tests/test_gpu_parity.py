@@ -1,0 +1,194 @@
+"""CUDA product against the oracle and the golden fixtures, through the C ABI.
+
+Bars: integer/index work bit-exact (neighbour lists, spreading windows through the
+spread grid); FP64 operators within 1e-11 of the FP64 fixtures (summation order is
+the only difference); FP32 operators within 2e-5 relative to the largest entry;
+solves compared with tightly converged oracle solutions.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def rel(a, b):
+    a = a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+    b = np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def make_handle(product_lib, s, params, **over):
+    from conductorrigid_b200.device import Handle
+
+    kw = dict(params)
+    kw.update(over)
+    kw.setdefault("field", tuple(s.field))
+    p = product_lib.make_params(**kw)
+    h = Handle(p, s.L)
+    h.set_topology(s.body, s.rigid, s.body_charge)
+    h.set_positions(s.pos, s.body_pos)
+    return h
+
+
+@pytest.fixture(scope="module")
+def gold(cuda, product_lib):
+    from conductorrigid_b200.systems import ConductorSystem
+
+    g = np.load(GOLD / "small_system.npz")
+    s = ConductorSystem(L=g["L"], pos=g["pos"], body=g["body"], rigid=g["rigid"], body_charge=g["Q"],
+                        body_pos=g["body_pos"], radius=np.ones(len(g["Q"])), field=g["E0"])
+    params = dict(xi=float(g["xi"]), errortol=float(g["errortol"]), grid=int(g["grid"]), support=int(g["support"]),
+                  rcut=float(g["rcut"]))
+    h = make_handle(product_lib, s, params)
+    yield g, s, h
+    h.close()
+
+
+def test_stages_fp64_match_golden(gold, product_lib):
+    g, s, h = gold
+    N = s.n_beads
+    x = g["x"]
+    assert rel(h.spread(x[:N]), g["grid_spread"]) < 1e-12
+    assert rel(h.wave_potential(x[:N]), g["phi_wave"]) < 1e-11
+    assert rel(h.apply_M(x[:N]), g["Mq"]) < 1e-11
+    assert rel(h.apply_operator(x), g["y"]) < 1e-11
+    assert rel(h.objective(), g["rhs"]) < 1e-14
+    assert rel(h.precondition(x), g["Px"]) < 1e-15
+    assert rel(h.forces(x[:N]), g["force"]) < 1e-11
+
+
+def test_stages_fp32_match_golden(gold, product_lib):
+    g, s, h = gold
+    N = s.n_beads
+    x = g["x"]
+    F32 = product_lib.CR_FP32
+    assert rel(h.spread(x[:N], F32), g["grid_spread"]) < 2e-6
+    assert rel(h.wave_potential(x[:N], F32), g["phi_wave"]) < 2e-5
+    assert rel(h.apply_M(x[:N], F32), g["Mq"]) < 2e-5
+    assert rel(h.apply_operator(x, F32), g["y"]) < 2e-5
+    assert rel(h.forces(x[:N], F32), g["force"]) < 2e-5
+
+
+def test_operator_matches_oracle_plain_small(cuda, product_lib, oracle_lib):
+    from conductorrigid_b200 import systems
+
+    w = systems.workload("plain_small")
+    s, p = w.system, w.params
+    h = make_handle(product_lib, s, {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")})
+    orc = oracle_lib.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    x = np.random.default_rng(11).standard_normal(s.n_beads + s.n_bodies)
+    ref = orc.matvec(x)
+    assert rel(h.apply_operator(x), ref) < 1e-11
+    assert rel(h.apply_operator(x, product_lib.CR_FP32), ref) < 2e-5
+    assert rel(h.forces(x[: s.n_beads]), orc.forces(x[: s.n_beads], s.field)) < 1e-11
+    assert rel(h.objective(), orc.objective(s.field)) < 1e-14
+    h.close()
+
+
+@pytest.mark.parametrize("r_list", [4.0, 4.4])
+def test_neighbor_list_bit_exact(cuda, product_lib, oracle_lib, r_list):
+    from conductorrigid_b200 import systems
+
+    w = systems.workload("plain_small")
+    s, p = w.system, w.params
+    h = make_handle(product_lib, s, {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")})
+    count, head, lst = h.neighbor_list(r_list)
+    oc, oh, ol = oracle_lib.neighbor_list(s.pos, s.L, r_list)
+    assert np.array_equal(count.cpu().numpy(), oc)
+    assert np.array_equal(head.cpu().numpy(), oh)
+    assert np.array_equal(lst.cpu().numpy(), ol)
+    h.close()
+
+
+def _solve_pair(product_lib, oracle_lib, precision, scale=0.3):
+    from conductorrigid_b200 import systems
+
+    w = systems.workload("plain_small", scale=scale)
+    s, p = w.system, w.params
+    orc = oracle_lib.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    ref = orc.solve(s.field, restart=100, maxiter=4000, tol=1e-11)
+    h = make_handle(product_lib, s, {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")},
+                    gmres_tol=1e-6, restart=50, maxiter=4000, precision=precision)
+    q = h.dev(np.zeros(s.n_beads))
+    phi = h.dev(np.zeros(s.n_bodies))
+    F, st = h.compute(s.pos, s.body_pos, q, phi)
+    h.close()
+    return ref, q.cpu().numpy(), phi.cpu().numpy(), F.cpu().numpy(), st
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_solve_matches_oracle(cuda, product_lib, oracle_lib, precision):
+    ref, q, phi, F, st = _solve_pair(product_lib, oracle_lib, precision)
+    eq, ep, ef = rel(q, ref["q"]), rel(phi, ref["phi"]), rel(F, ref["force"])
+    print(f"\n{precision}: iters={st['iterations']} fp64 mv={st['matvecs_fp64']} fp32 mv={st['matvecs_fp32']} "
+          f"resid={st['final_residual']:.2e} err q={eq:.2e} phi={ep:.2e} F={ef:.2e}")
+    assert st["converged"] == 1 and st["final_residual"] <= 1e-6
+    assert eq < 1e-3 and ep < 1e-3 and ef < 1e-3
+
+
+def test_compute_host_matches_device(cuda, product_lib):
+    from conductorrigid_b200 import systems
+
+    w = systems.workload("plain_small", scale=0.3)
+    s, p = w.system, w.params
+    h = make_handle(product_lib, s, {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")},
+                    gmres_tol=1e-6, restart=50, maxiter=4000)
+    q = np.zeros(s.n_beads)
+    phi = np.zeros(s.n_bodies)
+    F, st = h.compute_host(s.pos, s.body_pos, q, phi)
+    qd = h.dev(np.zeros(s.n_beads))
+    pd = h.dev(np.zeros(s.n_bodies))
+    Fd, _ = h.compute(s.pos, s.body_pos, qd, pd)
+    assert rel(qd, q) < 1e-9 and rel(Fd, F) < 1e-9
+    # a warm start from the solution converges at once
+    F2, st2 = h.compute_host(s.pos, s.body_pos, q, phi)
+    assert st2["iterations"] <= 1 and st2["final_residual"] <= 1e-6
+    h.close()
+
+
+def test_errors_do_not_touch_the_device(cuda, product_lib):
+    """Bad inputs come back as status codes."""
+    import ctypes as C
+
+    from conductorrigid_b200 import systems
+    from conductorrigid_b200._lib import CrError
+
+    w = systems.workload("plain_small", scale=0.3)
+    s, p = w.system, w.params
+    h = make_handle(product_lib, s, {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")})
+    bad = s.pos.copy()
+    bad[17, 1] = np.nan
+    with pytest.raises(CrError) as e:
+        h.set_positions(bad, s.body_pos)
+    assert e.value.status == product_lib.CR_NUMERICAL
+    # the handle stays usable
+    h.set_positions(s.pos, s.body_pos)
+    y = h.apply_operator(np.ones(s.n_beads + s.n_bodies))
+    assert np.isfinite(y.cpu().numpy()).all()
+    h.close()
+    # calls before the topology is set
+    from conductorrigid_b200.device import Handle
+
+    h2 = Handle(product_lib.make_params(**{k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")}), s.L)
+    st = product_lib.lib().cr_objective(h2.h, None)
+    assert st == product_lib.CR_NOT_READY
+    h2.close()
+
+
+def test_empty_system(cuda, product_lib):
+    from conductorrigid_b200.device import Handle
+
+    h = Handle(product_lib.make_params(xi=0.9, errortol=1e-5, grid=16, support=5, rcut=3.0), [10.0, 10.0, 10.0])
+    h.set_topology(np.zeros(0, np.uint32), np.zeros(0, np.uint8), np.zeros(0))
+    h.set_positions(np.zeros((0, 3)), np.zeros((0, 3)))
+    q = h.dev(np.zeros(0))
+    phi = h.dev(np.zeros(0))
+    F, st = h.compute(np.zeros((0, 3)), np.zeros((0, 3)), q, phi)
+    assert F.shape == (0, 3) and st["converged"] == 1
+    g = h.spread(np.zeros(0))
+    assert float(g.abs().max()) == 0.0
+    h.close()
