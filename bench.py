@@ -1,0 +1,401 @@
+"""Benchmark: induced-charge solves per second on the 162k-charge conductor system.
+
+One step = one full solve of the workload: right-hand side, flexible GMRES to a true
+relative residual of 1e-6, and the bead forces, through the C ABI (cr_compute).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm times the headline solver (FP32 operator inside FP64-Arnoldi flexible GMRES
+with FP64 refinement; the learned warm start when enabled) and, in the same run, the
+plain FP64 solve of the same method on the same B200.  Inputs are resident in HBM for
+``value``; ``e2e`` repeats the step through cr_compute_host with host buffers, the
+copies inside the timed region.  Multi-GPU runs are independent replicas (one system
+per rank, no collective on the data path).  ``--impl reference`` times the reference
+method's CPU implementation (the FP64 oracle port) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "precision_162k"
+METRIC = "solves/s at 1e-6 residual: learned+FP32 vs plain FP64, same B200; spread GB/s"
+UNIT = "solves/s"
+RESTART = 50
+TOL = 1e-6
+#: operator applications of one plain FP64 solve of the 162k-charge workload (seed 1),
+#: measured on B200 with this repository's FGMRES(50); scales the CPU timings of a
+#: bounded sample of applications to a full solve
+MATVECS_PER_SOLVE_FP64 = {"precision_162k": None}
+
+PROFILE_BYTES_DOC = {
+    "spread": "N*(16+s) + G*s (positions and charges in, one real mesh written)",
+    "contract": "G*s + N*(16+s)",
+    "real_space": "4*L_pairs + N*(16+2s) (stored neighbour entries plus per-bead data)",
+    "fft": "2*G*s per R2C/C2R transform (real side) + 2*G*s (half-spectrum complex side)",
+}
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str):
+        self.device_id = device_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", self.device_id], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        pw = [num(r[3]) for r in rows if num(r[3]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(n)
+        under = sorted(sm)[len(sm) // 4:] if sm else []
+        return {"sm_mhz": statistics.median(under) if under else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def algorithmic_bytes(kind: str, prec_bytes: int, N: int, G: int, pairs: int) -> float:
+    s = prec_bytes
+    pos = 16 if s == 4 else 32
+    if kind == "spread":
+        return N * (pos + s) + G * s
+    if kind == "contract":
+        return G * s + N * (pos + s)
+    if kind == "contract_force":
+        return G * s + N * (pos + s) + N * 3 * s
+    if kind == "real_space":
+        return 4.0 * pairs + N * (pos + 2 * s)
+    if kind == "real_space_force":
+        return 4.0 * pairs + N * (pos + 2 * s) + N * 3 * 8
+    if kind == "fft":
+        return 2.0 * G * s + 2.0 * G * s
+    if kind == "scale":
+        return (G / 2) * (2 * s * 2 + s)
+    return float("nan")
+
+
+def run_reference(args) -> None:
+    """The reference method's CPU implementation (FP64 oracle port) on the host cores."""
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return
+    import oracle
+    from conductorrigid_b200 import systems
+
+    w = systems.workload(WORKLOAD, seed=1)
+    s, p = w.system, w.params
+    t0 = time.perf_counter()
+    orc = oracle.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    setup = time.perf_counter() - t0
+    x = np.random.default_rng(0).standard_normal(s.n_beads + s.n_bodies)
+    n_mv = 1
+    for _ in range(args.warmup):
+        orc.matvec(x)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        for _ in range(n_mv):
+            orc.matvec(x)
+        times.append((time.perf_counter() - t) / n_mv)
+    t_mv = float(np.median(times))
+    mps = MATVECS_PER_SOLVE_FP64.get(WORKLOAD) or 0
+    solve_s = setup + mps * t_mv if mps else float("nan")
+    value = 1.0 / solve_s if mps else None
+    cores = oracle.lib().orc_num_threads()
+    sample = (f"{args.steps} timed FP64 operator applications of the {s.n_beads}-charge system on {cores} host "
+              f"threads ({t_mv:.3f} s each) plus the neighbour-list setup ({setup:.2f} s), scaled to the "
+              f"{mps} applications of one plain FP64 solve")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_s * 1e3 if mps else None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "charges": s.n_beads, "bodies": s.n_bodies, "mesh": p["grid"],
+                   "support": p["support"], "rcut": p["rcut"], "tol": TOL},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--learned", type=int, default=0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from conductorrigid_b200 import _lib, systems
+    from conductorrigid_b200.device import Handle
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = systems.workload(WORKLOAD, seed=1 + rank)
+    s, p = w.system, w.params
+    base = {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")}
+    common = dict(field=tuple(s.field), gmres_tol=TOL, restart=RESTART, maxiter=20000, **base)
+    stream = torch.cuda.Stream()
+    h_fast = Handle(_lib.make_params(precision="mixed", learned=bool(args.learned), **common), s.L, stream=stream)
+    h_plain = Handle(_lib.make_params(precision="fp64", **common), s.L, stream=stream)
+    for h in (h_fast, h_plain):
+        h.set_topology(s.body, s.rigid, s.body_charge)
+    pos = h_fast.dev(s.pos)
+    bpos = h_fast.dev(s.body_pos)
+    q = torch.zeros(s.n_beads, dtype=torch.float64, device="cuda")
+    phi = torch.zeros(s.n_bodies, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+
+    def timed(h, steps, profile=False):
+        """Per-step device time (CUDA events on the solver's stream), L2 flushed before each step."""
+        stats = []
+        total_ms = 0.0
+        if profile:
+            h.profile(True)
+        c0 = h.counters()
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                q.zero_()
+                phi.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            F, st = h.compute(pos, bpos, q, phi)
+            e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            stats.append(st)
+        c1 = h.counters()
+        prof = h.profile_read() if profile else None
+        if profile:
+            h.profile(False)
+        launches = c1["kernel_launches"] - c0["kernel_launches"]
+        return total_ms / steps, stats, prof, launches, c1["fft_execs"] - c0["fft_execs"]
+
+    # warm-up (untimed)
+    for h in (h_fast, h_plain):
+        timed(h, args.warmup)
+
+    dev_id = str(local)
+    try:
+        uuid = torch.cuda.get_device_properties(local).uuid
+        dev_id = "GPU-" + str(uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(dev_id)
+    torch.cuda.synchronize()
+    barrier()
+    clocks.start()
+    ms_fast, st_fast, prof, launches, ffts = timed(h_fast, args.steps, profile=True)
+    torch.cuda.synchronize()
+    barrier()
+    ms_plain, st_plain, _, _, _ = timed(h_plain, args.steps)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms_fast = max_over_ranks(ms_fast)
+    ms_plain = max_over_ranks(ms_plain)
+
+    # end to end through the public C ABI on host buffers (pinned)
+    hp = torch.from_numpy(s.pos.copy()).pin_memory()
+    hb = torch.from_numpy(s.body_pos.copy()).pin_memory()
+    hq = torch.zeros(s.n_beads, dtype=torch.float64).pin_memory()
+    hphi = torch.zeros(s.n_bodies, dtype=torch.float64).pin_memory()
+    hf = torch.zeros((s.n_beads, 3), dtype=torch.float64).pin_memory()
+    e2e_s = []
+    for _ in range(args.steps):
+        hq.zero_()
+        hphi.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h_fast.compute_host(hp.numpy(), hb.numpy(), hq.numpy(), hphi.numpy(), hf.numpy())
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks(1e3 * float(np.mean(e2e_s)))
+    h2d = 8 * (3 * s.n_beads + 3 * s.n_bodies + s.n_beads + s.n_bodies)
+    d2h = 8 * (s.n_beads + s.n_bodies + 3 * s.n_beads)
+
+    # roofline of the dominant kernel class in the timed headline solves
+    geo = h_fast.geometry_info()
+    G = int(np.prod([p["grid"]] * 3))
+    dom = max((k for k in prof if k not in ("geometry",)), key=lambda k: prof[k]["ms"])
+    dom_ms = prof[dom]["ms"] / max(prof[dom]["launches"], 1)
+    alg = algorithmic_bytes(dom, 4, s.n_beads, G, geo["real_space_pairs"])
+    peak, peak_kind = load_peaks()
+    achieved = alg / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = ROOT / "profiles" / "ncu_traffic.json"
+    if tpath.exists():
+        try:
+            traffic = json.loads(tpath.read_text()).get(WORKLOAD, {}).get(dom)
+        except Exception:
+            traffic = None
+    total_prof_ms = sum(v["ms"] for v in prof.values())
+    shares = {k: round(v["ms"] / total_prof_ms, 4) for k, v in prof.items() if total_prof_ms > 0}
+
+    value = world * 1e3 / ms_fast
+    plain_value = world * 1e3 / ms_plain
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_fast, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 operator / f64 Krylov", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "charges": s.n_beads, "bodies": s.n_bodies, "mesh": p["grid"],
+                   "support": p["support"], "rcut": p["rcut"], "tol": TOL, "restart": RESTART,
+                   "learned": bool(args.learned), "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MB write) before every step"},
+        "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain,
+                       "iterations": st_plain[-1]["iterations"], "matvecs_fp64": st_plain[-1]["matvecs_fp64"],
+                       "final_residual": st_plain[-1]["final_residual"]},
+        "speedup_vs_plain_fp64": value / plain_value,
+        "solve": {"iterations": st_fast[-1]["iterations"], "refinements": st_fast[-1]["refinements"],
+                  "matvecs_fp32": st_fast[-1]["matvecs_fp32"], "matvecs_fp64": st_fast[-1]["matvecs_fp64"],
+                  "final_residual": st_fast[-1]["final_residual"]},
+        "kernel_share": shares,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "launches": prof[dom]["launches"], "avg_launch_ms": dom_ms,
+                     "algorithmic_bytes_per_launch": alg},
+        "e2e": {"value": world * 1e3 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "cufft_execs": int(ffts),
+        "clocks": clk,
+    }
+    # spread GB/s (named by the metric)
+    if "spread" in prof and prof["spread"]["launches"]:
+        sp_ms = prof["spread"]["ms"] / prof["spread"]["launches"]
+        sp_alg = algorithmic_bytes("spread", 4, s.n_beads, G, 0)
+        line["spread"] = {"achieved_gbs": sp_alg / (sp_ms * 1e-3) / 1e9, "avg_launch_ms": sp_ms,
+                          "frac": sp_alg / (sp_ms * 1e-3) / 1e9 / peak}
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(s, p, st_plain[-1]["matvecs_fp64"])
+    MATVECS_PER_SOLVE_FP64[WORKLOAD] = st_plain[-1]["matvecs_fp64"]
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for h in (h_fast, h_plain):
+        h.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(s, p, matvecs_per_solve: int) -> dict:
+    """The FP64 oracle (port of the reference method) on the host cores: a bounded
+    sample of operator applications, scaled to one plain solve."""
+    import oracle
+
+    t0 = time.perf_counter()
+    orc = oracle.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    setup = time.perf_counter() - t0
+    x = np.random.default_rng(0).standard_normal(s.n_beads + s.n_bodies)
+    orc.matvec(x)
+    n, t1 = 0, time.perf_counter()
+    while n < 3 or (time.perf_counter() - t1 < 10.0 and n < 20):
+        orc.matvec(x)
+        n += 1
+    t_mv = (time.perf_counter() - t1) / n
+    cores = oracle.lib().orc_num_threads()
+    solve_s = setup + matvecs_per_solve * t_mv
+    return {"value": 1.0 / solve_s, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"{n} FP64 operator applications of the {s.n_beads}-charge system on {cores} host threads "
+                       f"({t_mv:.3f} s each) plus neighbour-list setup ({setup:.2f} s), scaled to the "
+                       f"{matvecs_per_solve} applications of the plain FP64 solve in this run")}
+
+
+if __name__ == "__main__":
+    main()

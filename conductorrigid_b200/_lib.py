@@ -29,6 +29,10 @@ CR_FP32 = 2
 
 PRECISIONS = {"fp64": CR_FP64, "mixed": CR_MIXED, "fp32": CR_FP32}
 
+#: kernel classes of cr_profile_read
+PROFILE_CLASSES = ["spread", "fft", "scale", "contract", "real_space", "contract_force", "real_space_force",
+                   "krylov", "body", "geometry"]
+
 
 class CrParams(C.Structure):
     _fields_ = [
@@ -89,6 +93,16 @@ class CrSolveStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class CrGeometryInfo(C.Structure):
+    _fields_ = [
+        ("real_space_pairs", C.c_int64),
+        ("tile_edge", C.c_int),
+        ("n_tiles", C.c_int),
+        ("n_beads", C.c_int),
+        ("n_bodies", C.c_int),
+    ]
+
+
 class CrError(RuntimeError):
     def __init__(self, status: int, where: str, msg: str = ""):
         self.status = status
@@ -124,6 +138,10 @@ _SIGS = {
     "cr_apply_M": ([_P, _P, _P, _I], _I),
     "cr_forces": ([_P, _P, _P, _I], _I),
     "cr_neighbor_list": ([_P, C.c_double, _P, _P, _P, C.c_int64, C.POINTER(C.c_int64)], _I),
+    "cr_profile": ([_P, _I], _I),
+    "cr_profile_read": ([_P, _I, C.POINTER(C.c_int), C.POINTER(C.c_double)], _I),
+    "cr_counters": ([_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], _I),
+    "cr_get_geometry_info": ([_P, C.POINTER(CrGeometryInfo)], _I),
     "cr_util_icosphere_count": ([_I], _I),
     "cr_util_icosphere": ([_I, _D], _I),
     "cr_util_place_spheres": ([_I, _D, _D, C.c_uint64, C.c_int64, _D], _I),

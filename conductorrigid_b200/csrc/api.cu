@@ -3,6 +3,7 @@
 // The handle plays the part of the reference's ConductorRigid ForceCompute
 // (ConductorRigid.h:21-112): it owns the derived parameters, tables, mesh, FFT plans,
 // per-solve geometry and the Krylov workspace; the caller owns the particle arrays.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -27,6 +28,32 @@ int check_cufft(cr_handle *h, cufftResult r, const char *what) {
     if (r == CUFFT_SUCCESS) return CR_OK;
     return fail(h, r == CUFFT_ALLOC_FAILED ? CR_OUT_OF_MEMORY : CR_CUDA_ERROR,
                 std::string(what) + ": cuFFT error " + std::to_string((int)r));
+}
+
+long prof_begin(cr_handle *h, int id) {
+    if (!h->prof.on) return -1;
+    Profiler &p = h->prof;
+    if (p.used + 2 > p.pool.size()) {
+        const size_t grow = std::max<size_t>(1024, p.pool.size());
+        for (size_t k = 0; k < grow; ++k) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                cudaGetLastError();
+                return -1;
+            }
+            p.pool.push_back(e);
+        }
+    }
+    const size_t s = p.used;
+    p.used += 2;
+    cudaEventRecord(p.pool[s], h->stream);
+    p.marks.emplace_back(id, s);
+    return (long)s;
+}
+
+void prof_end(cr_handle *h, long token) {
+    if (token < 0 || !h->prof.on) return;
+    cudaEventRecord(h->prof.pool[(size_t)token + 1], h->stream);
 }
 
 namespace {
@@ -175,6 +202,7 @@ int cr_destroy(cr_handle *h) {
     free_all(h);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
     delete h;
     return CR_OK;
 }
@@ -343,6 +371,53 @@ int cr_forces(cr_handle *h, const double *d_q, double *d_force, int precision) {
         CR_TRY(real_space_force(h, h->m32, d_force));
     }
     return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_forces");
+}
+
+int cr_profile(cr_handle *h, int enable) {
+    if (!h) return CR_BAD_PARAM;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    else cudaDeviceSynchronize();
+    h->prof.on = enable != 0;
+    h->prof.used = 0;
+    h->prof.marks.clear();
+    return CR_OK;
+}
+
+int cr_profile_read(cr_handle *h, int kernel_class, int *launches, double *total_ms) {
+    if (!h || !launches || !total_ms || kernel_class < 0 || kernel_class >= PROF_COUNT) return CR_BAD_PARAM;
+    CR_CUDA(h, h->stream ? cudaStreamSynchronize(h->stream) : cudaDeviceSynchronize());
+    int n = 0;
+    double t = 0.0;
+    for (const auto &m : h->prof.marks) {
+        if (m.first != kernel_class) continue;
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, h->prof.pool[m.second], h->prof.pool[m.second + 1]) == cudaSuccess) {
+            ++n;
+            t += ms;
+        } else {
+            cudaGetLastError();
+        }
+    }
+    *launches = n;
+    *total_ms = t;
+    return CR_OK;
+}
+
+int cr_get_geometry_info(const cr_handle *h, cr_geometry_info *out) {
+    if (!h || !out) return CR_BAD_PARAM;
+    out->real_space_pairs = h->geo.valid ? h->geo.nl_total : 0;
+    out->tile_edge = h->tile;
+    out->n_tiles = h->ntiles;
+    out->n_beads = h->N;
+    out->n_bodies = h->B;
+    return CR_OK;
+}
+
+int cr_counters(const cr_handle *h, long long *kernel_launches, long long *fft_execs) {
+    if (!h || !kernel_launches || !fft_execs) return CR_BAD_PARAM;
+    *kernel_launches = h->launches;
+    *fft_execs = h->fft_execs;
+    return CR_OK;
 }
 
 int cr_neighbor_list(cr_handle *h, double r_list, int *d_count, int64_t *d_head, int *d_list, int64_t capacity,

@@ -115,6 +115,7 @@ int topology_build(cr_handle *h) {
 
 int body_sums(cr_handle *h, const double *x, double *y) {
     if (h->B == 0) return CR_OK;
+    ProfScope ps(h, PROF_BODY);
     body_sums_kernel<<<blocks_for((long)h->B * 32, 256), 256, 0, h->stream>>>(h->N, h->B, h->d_body_start,
                                                                                h->d_body_members, x, y);
     CR_LAUNCH(h, "body_sums_kernel");

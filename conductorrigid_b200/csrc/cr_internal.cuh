@@ -93,6 +93,28 @@ struct Krylov {
     int nblocks = 0;
 };
 
+// Kernel classes timed by the built-in profiler (CUDA events on the handle's stream).
+enum ProfId {
+    PROF_SPREAD = 0,
+    PROF_FFT,
+    PROF_SCALE,
+    PROF_CONTRACT,
+    PROF_REAL,
+    PROF_CONTRACT_FORCE,
+    PROF_REAL_FORCE,
+    PROF_KRYLOV,
+    PROF_BODY,
+    PROF_GEOMETRY,
+    PROF_COUNT
+};
+
+struct Profiler {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;                 // reusable events
+    size_t used = 0;
+    std::vector<std::pair<int, size_t>> marks;     // (class, index of the start event)
+};
+
 }  // namespace cr
 
 struct cr_handle {
@@ -136,6 +158,9 @@ struct cr_handle {
     size_t sort_tmp_bytes = 0;
     int *d_keys = nullptr, *d_keys_alt = nullptr, *d_vals = nullptr, *d_vals_alt = nullptr;  // [N]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cr::Profiler prof;
+    long long launches = 0;           // kernels of this library launched (all entry points)
+    long long fft_execs = 0;          // cuFFT executions
     // staging for cr_compute_host
     double *d_io_pos = nullptr, *d_io_bpos = nullptr, *d_io_q = nullptr, *d_io_phi = nullptr, *d_io_force = nullptr;
 };
@@ -154,7 +179,21 @@ int check_cufft(cr_handle *h, cufftResult r, const char *what);
     } while (0)
 #define CR_CUDA(h, expr) CR_TRY(::cr::check_cuda((h), (expr), #expr))
 #define CR_CUFFT(h, expr) CR_TRY(::cr::check_cufft((h), (expr), #expr))
-#define CR_LAUNCH(h, what) CR_TRY(::cr::check_cuda((h), cudaGetLastError(), (what)))
+#define CR_LAUNCH(h, what)                                                 \
+    do {                                                                   \
+        ++(h)->launches;                                                   \
+        CR_TRY(::cr::check_cuda((h), cudaGetLastError(), (what)));         \
+    } while (0)
+
+// Profiler marks: prof_begin returns a token passed to prof_end (no-ops when off).
+long prof_begin(cr_handle *h, int id);
+void prof_end(cr_handle *h, long token);
+struct ProfScope {
+    cr_handle *h;
+    long tok;
+    ProfScope(cr_handle *h_, int id) : h(h_), tok(prof_begin(h_, id)) {}
+    ~ProfScope() { prof_end(h, tok); }
+};
 
 template <typename T> int dalloc(cr_handle *h, T **p, size_t count) {
     if (*p) { cudaFree(*p); *p = nullptr; }

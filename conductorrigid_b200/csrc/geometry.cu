@@ -349,6 +349,7 @@ static int cell_bins(cr_handle *h, const CellGrid &cg, int *cell_of, int **start
 }
 
 int geometry_update(cr_handle *h, const double *d_pos, const double *d_body_pos) {
+    ProfScope ps(h, PROF_GEOMETRY);
     Geometry &g = h->geo;
     const int N = h->N;
     g.valid = false;

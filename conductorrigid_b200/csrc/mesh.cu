@@ -348,6 +348,7 @@ template <typename R> int cast_to_double(cr_handle *h, const R *in, double *out,
 }
 
 template <typename R> int spread_only(cr_handle *h, MeshBuffers<R> &m) {
+    ProfScope ps(h, PROF_SPREAD);
     const long G = grid_size(h);
     CR_CUDA(h, cudaMemsetAsync(m.grid, 0, G * sizeof(R), h->stream));
     spread_tiles_kernel<R><<<h->ntiles, 256, spread_smem<R>(h), h->stream>>>(
@@ -361,16 +362,28 @@ template <typename R> static int wave_mesh(cr_handle *h, MeshBuffers<R> &m) {
     CR_TRY(spread_only(h, m));
     CR_CUFFT(h, cufftSetStream(m.plan_fwd, h->stream));
     CR_CUFFT(h, cufftSetStream(m.plan_inv, h->stream));
-    CR_CUFFT(h, fft_forward(m.plan_fwd, m.grid, m.spec));
+    {
+        ProfScope ps(h, PROF_FFT);
+        CR_CUFFT(h, fft_forward(m.plan_fwd, m.grid, m.spec));
+        ++h->fft_execs;
+    }
     const int S = spec_size(h);
-    scale_kernel<R, typename Prec<R>::C><<<blocks_for(S, 256), 256, 0, h->stream>>>(m.spec, m.scale, S);
-    CR_LAUNCH(h, "scale_kernel");
-    CR_CUFFT(h, fft_inverse(m.plan_inv, m.spec, m.grid));
+    {
+        ProfScope ps(h, PROF_SCALE);
+        scale_kernel<R, typename Prec<R>::C><<<blocks_for(S, 256), 256, 0, h->stream>>>(m.spec, m.scale, S);
+        CR_LAUNCH(h, "scale_kernel");
+    }
+    {
+        ProfScope ps(h, PROF_FFT);
+        CR_CUFFT(h, fft_inverse(m.plan_inv, m.spec, m.grid));
+        ++h->fft_execs;
+    }
     return CR_OK;
 }
 
 template <typename R> int wave_potential(cr_handle *h, MeshBuffers<R> &m) {
     CR_TRY(wave_mesh(h, m));
+    ProfScope ps(h, PROF_CONTRACT);
     contract_tiles_kernel<R, false><<<h->ntiles, 256, contract_smem<R>(h), h->stream>>>(
         m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
         (R)(h->d.quadW * h->d.prefac), m.grid, m.phi);
@@ -380,6 +393,7 @@ template <typename R> int wave_potential(cr_handle *h, MeshBuffers<R> &m) {
 
 template <typename R> int wave_force(cr_handle *h, MeshBuffers<R> &m) {
     CR_TRY(wave_mesh(h, m));
+    ProfScope ps(h, PROF_CONTRACT_FORCE);
     contract_tiles_kernel<R, true><<<h->ntiles, 256, contract_smem<R>(h), h->stream>>>(
         m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
         (R)(2.0 * h->d.quadW * h->d.prefac * h->d.xiterm), m.grid, m.force);

@@ -136,6 +136,7 @@ template <typename R> RSConst<R> rs_const(const cr_handle *h) {
 template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out) {
     const int N = h->N;
     if (N == 0) return CR_OK;
+    ProfScope ps(h, PROF_REAL);
     real_potential_kernel<R><<<blocks_for((long)N * 32, 256), 256, 0, h->stream>>>(
         N, m.pos, m.q, h->geo.nl_count, h->geo.nl_head, h->geo.nl_list, m.phiq, rs_const<R>(h), m.phi, phi_body,
         h->d_body, out);
@@ -146,6 +147,7 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
 template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, double *force_out) {
     const int N = h->N;
     if (N == 0) return CR_OK;
+    ProfScope ps(h, PROF_REAL_FORCE);
     real_force_kernel<R><<<blocks_for((long)N * 32, 256), 256, 0, h->stream>>>(
         N, m.pos, m.q, h->geo.nl_count, h->geo.nl_head, h->geo.nl_list, m.gradphiq, rs_const<R>(h), m.force,
         force_out);

@@ -93,6 +93,7 @@ int vec_blocks(int n) { return std::max(1, std::min(4 * 148, blocks_for(n, 256))
 
 // hcol[0..k) = V[0..k)^T w   (device result)
 int dots(cr_handle *h, int k, const double *V, const double *w, double *out) {
+    ProfScope ps(h, PROF_KRYLOV);
     Krylov &K = h->kry;
     multi_dot_kernel<<<K.nblocks, kDotThreads, 0, h->stream>>>(K.n, k, V, w, K.partial);
     CR_LAUNCH(h, "multi_dot_kernel");

@@ -144,6 +144,28 @@ class Handle:
                                                 total.value, C.byref(total)), "cr_neighbor_list")
         return count, head, lst[: total.value]
 
+    # -- instrumentation -------------------------------------------------------
+    def profile(self, enable: bool = True):
+        self._check(_lib.lib().cr_profile(self.h, int(enable)), "cr_profile")
+
+    def profile_read(self) -> dict:
+        out = {}
+        for k, name in enumerate(_lib.PROFILE_CLASSES):
+            n, ms = C.c_int(0), C.c_double(0)
+            self._check(_lib.lib().cr_profile_read(self.h, k, C.byref(n), C.byref(ms)), "cr_profile_read")
+            out[name] = {"launches": n.value, "ms": ms.value}
+        return out
+
+    def geometry_info(self) -> dict:
+        g = _lib.CrGeometryInfo()
+        self._check(_lib.lib().cr_get_geometry_info(self.h, C.byref(g)), "cr_get_geometry_info")
+        return {name: getattr(g, name) for name, _ in g._fields_}
+
+    def counters(self) -> dict:
+        a, b = C.c_longlong(0), C.c_longlong(0)
+        self._check(_lib.lib().cr_counters(self.h, C.byref(a), C.byref(b)), "cr_counters")
+        return {"kernel_launches": a.value, "fft_execs": b.value}
+
     # -- the step --------------------------------------------------------------
     def compute(self, pos, body_pos, q, phi, allow_not_converged=False):
         """Device arrays in, solve + forces; q and phi are updated in place."""

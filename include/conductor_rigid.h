@@ -167,6 +167,25 @@ int cr_forces(cr_handle *h, const double *d_q, double *d_force, int precision);
 int cr_neighbor_list(cr_handle *h, double r_list, int *d_count, int64_t *d_head, int *d_list,
                      int64_t capacity, int64_t *total);
 
+/* ---- instrumentation ----
+ * With profiling on, every kernel class below is bracketed by CUDA events on the
+ * handle's stream; cr_profile_read returns launches and summed device time of one
+ * class since the last reset.  Classes: 0 spread, 1 FFT, 2 influence-function scale,
+ * 3 contract, 4 real-space potential, 5 contract force, 6 real-space force,
+ * 7 Krylov vector ops, 8 body rows, 9 per-solve geometry (binning, neighbour list). */
+int cr_profile(cr_handle *h, int enable);   /* enable/disable; also resets the record */
+int cr_profile_read(cr_handle *h, int kernel_class, int *launches, double *total_ms);
+/* Sizes of the current per-solve geometry (for traffic and roofline arithmetic). */
+typedef struct {
+    int64_t real_space_pairs;  /* neighbour entries the real-space kernels walk per application */
+    int tile_edge;             /* spread/contract tile edge in mesh nodes */
+    int n_tiles;               /* mesh tiles */
+    int n_beads, n_bodies;
+} cr_geometry_info;
+int cr_get_geometry_info(const cr_handle *h, cr_geometry_info *out);
+/* Kernels of this library launched through the handle, and cuFFT executions. */
+int cr_counters(const cr_handle *h, long long *kernel_launches, long long *fft_execs);
+
 /* ---- synthetic systems (host utilities for the benchmark workloads) ---- */
 int cr_util_icosphere_count(int level);
 int cr_util_icosphere(int level, double *verts);
