@@ -29,9 +29,13 @@ CR_FP32 = 2
 
 PRECISIONS = {"fp64": CR_FP64, "mixed": CR_MIXED, "fp32": CR_FP32}
 
+CR_PRECOND_DIAGONAL = 0
+CR_PRECOND_CONDUCTOR = 1
+PRECONDITIONERS = {"diagonal": CR_PRECOND_DIAGONAL, "conductor": CR_PRECOND_CONDUCTOR}
+
 #: kernel classes of cr_profile_read
 PROFILE_CLASSES = ["spread", "fft", "scale", "contract", "real_space", "contract_force", "real_space_force",
-                   "krylov", "body", "geometry"]
+                   "krylov", "body", "geometry", "precondition"]
 
 
 class CrParams(C.Structure):
@@ -47,6 +51,7 @@ class CrParams(C.Structure):
         ("maxiter", C.c_int),
         ("precision", C.c_int),
         ("learned", C.c_int),
+        ("precond", C.c_int),
     ]
 
 
@@ -203,6 +208,7 @@ def make_params(
     maxiter: int = 0,
     precision="fp64",
     learned: bool = False,
+    precond="diagonal",
 ) -> CrParams:
     p = CrParams()
     p.field[:] = [float(v) for v in field]
@@ -217,6 +223,7 @@ def make_params(
     p.maxiter = int(maxiter)
     p.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     p.learned = int(bool(learned))
+    p.precond = PRECONDITIONERS[precond] if isinstance(precond, str) else int(precond)
     return p
 
 

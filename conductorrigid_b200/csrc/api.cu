@@ -59,6 +59,7 @@ void prof_end(cr_handle *h, long token) {
 namespace {
 
 void free_all(cr_handle *h) {
+    conductor_free(h);
     mesh_free(h->m64);
     mesh_free(h->m32);
     geometry_free(h);
@@ -132,6 +133,8 @@ int need_geometry(cr_handle *h) {
 }
 
 bool finite_params(const cr_params *p) {
+    if (p->precond != CR_PRECOND_DIAGONAL && p->precond != CR_PRECOND_CONDUCTOR) return false;
+    if (p->precision < CR_FP64 || p->precision > CR_FP32) return false;
     if (!std::isfinite(p->xi) || !std::isfinite(p->errortol) || !std::isfinite(p->rcut) ||
         !std::isfinite(p->gmres_tol))
         return false;
@@ -231,6 +234,7 @@ int cr_set_params(cr_handle *h, const cr_params *p, const double L[3]) {
     CR_TRY(derive(h, p, L));
     h->geo.valid = false;
     if (h->have_topology) {
+        conductor_free(h);
         mesh_free(h->m64);
         mesh_free(h->m32);
         geometry_free(h);
@@ -266,6 +270,14 @@ int cr_set_topology(cr_handle *h, int n_beads, const uint32_t *body, int n_bodie
     h->have_topology = false;
     h->N = n_beads;
     h->B = n_bodies;
+    // host member lists: beads of each body in ascending bead index
+    h->h_body_start.assign((size_t)n_bodies + 1, 0);
+    for (int b = 0; b < n_bodies; ++b) h->h_body_start[b + 1] = h->h_body_start[b] + size[b];
+    h->h_body_members.assign((size_t)n_beads, 0);
+    {
+        std::vector<int> fill(h->h_body_start.begin(), h->h_body_start.end() - 1);
+        for (int i = 0; i < n_beads; ++i) h->h_body_members[fill[body[i]]++] = i;
+    }
     CR_TRY(dalloc(h, &h->d_body, (size_t)std::max(n_beads, 1)));
     CR_TRY(dalloc(h, &h->d_rigid, (size_t)std::max(n_bodies, 1)));
     CR_TRY(dalloc(h, &h->d_Q, (size_t)std::max(n_bodies, 1)));
@@ -364,11 +376,11 @@ int cr_forces(cr_handle *h, const double *d_q, double *d_force, int precision) {
     if (precision == CR_FP64) {
         CR_TRY(cast_charges(h, h->m64, d_q));
         CR_TRY(wave_force(h, h->m64));
-        CR_TRY(real_space_force(h, h->m64, d_force));
+        CR_TRY(real_space_force(h, h->m64, d_q, d_force));
     } else {
         CR_TRY(cast_charges(h, h->m32, d_q));
         CR_TRY(wave_force(h, h->m32));
-        CR_TRY(real_space_force(h, h->m32, d_force));
+        CR_TRY(real_space_force(h, h->m32, d_q, d_force));
     }
     return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_forces");
 }
@@ -460,7 +472,7 @@ int cr_compute(cr_handle *h, const double *d_pos, const double *d_body_pos, doub
     // force pass in FP64
     CR_TRY(cast_charges(h, h->m64, K.x));
     CR_TRY(wave_force(h, h->m64));
-    CR_TRY(real_space_force(h, h->m64, d_force));
+    CR_TRY(real_space_force(h, h->m64, K.x, d_force));
     CR_CUDA(h, cudaStreamSynchronize(h->stream));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);

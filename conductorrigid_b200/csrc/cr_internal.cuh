@@ -75,6 +75,27 @@ struct Geometry {
     bool valid = false;
 };
 
+// Real-space operator of the current geometry: 32-bead clusters, cluster pairs
+// (I <= J) within rc, and per pair a 32x32 block of tabulated kernel values.
+struct RealSpace {
+    int nclus = 0;
+    int *sorted = nullptr;          // [N] beads in Morton order
+    int *members = nullptr;         // [nclus*32] bead index or -1
+    double4 *centre = nullptr;      // [nclus]
+    double4 *extent = nullptr;      // [nclus] half extents
+    int *count = nullptr;           // [nclus] pairs owned by cluster I
+    long long *head = nullptr;      // [nclus] first pair of cluster I
+    int *pair_i = nullptr, *pair_j = nullptr;
+    long long npairs = 0, pair_cap = 0;
+    float *blocks32 = nullptr;      // [npairs*1024]
+    double *blocks64 = nullptr;     // [npairs*1024]
+    long long blocks32_cap = 0, blocks64_cap = 0;
+    bool valid32 = false, valid64 = false;
+    float *acc32 = nullptr;         // [N] product accumulators
+    double *acc64 = nullptr;
+    double *freal = nullptr;        // [3N] real-space forces
+};
+
 // GMRES workspace (FP64).
 struct Krylov {
     int n = 0, m = 0;
@@ -93,6 +114,19 @@ struct Krylov {
     int nblocks = 0;
 };
 
+// Conductor-response preconditioner: one K^-1 per distinct body shape.
+struct ConductorPrecond {
+    bool ready = false;
+    int n_shapes = 0, max_n = 0;
+    int *d_body_shape = nullptr;        // [B]
+    int *d_shape_n = nullptr;           // [S] beads per shape
+    long long *d_shape_mat = nullptr;   // [S] offset of the shape's K^-1 (column-major n x n)
+    int *d_shape_vec = nullptr;         // [S] offset of the shape's u = K^-1 1
+    double *d_kinv = nullptr;
+    double *d_u = nullptr;
+    double *d_invs = nullptr;           // [S] 1 / (1^T K^-1 1)
+};
+
 // Kernel classes timed by the built-in profiler (CUDA events on the handle's stream).
 enum ProfId {
     PROF_SPREAD = 0,
@@ -105,6 +139,7 @@ enum ProfId {
     PROF_KRYLOV,
     PROF_BODY,
     PROF_GEOMETRY,
+    PROF_PRECOND,
     PROF_COUNT
 };
 
@@ -135,6 +170,8 @@ struct cr_handle {
     int *d_body_start = nullptr;      // [B+1] CSR of members
     int *d_body_members = nullptr;    // [N]
     double4 *d_bpos = nullptr;        // [B] body centres
+    std::vector<int> h_body_start, h_body_members;  // host copy of the member lists
+    cr::ConductorPrecond cond;
 
     // tables on the host (FP64)
     std::vector<double> h_phiq, h_gradphiq;
@@ -147,6 +184,7 @@ struct cr_handle {
     cr::MeshBuffers<double> m64;
     cr::MeshBuffers<float> m32;
     cr::Geometry geo;
+    cr::RealSpace rs;
     cr::Krylov kry;
 
     // scratch
@@ -237,8 +275,12 @@ template <typename R> int spread_only(cr_handle *h, MeshBuffers<R> &m);
 // Real-space: out_i = Phi_b(i) - (phi_k + self q + sum T q)   (phi_body != NULL)
 //             out_i = phi_k + self q + sum T q               (phi_body == NULL)
 template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out);
-// Forces: out = wave force + q E0 + real-space force (FP64 out).
-template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, double *force_out);
+// Forces: out = wave force (m.force) + q E0 + real-space force for FP64 charges q64.
+template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, const double *q64, double *force_out);
+int realspace_alloc(cr_handle *h);
+void realspace_free(cr_handle *h);
+// Clusters and cluster pairs of the current positions.
+int realspace_build(cr_handle *h);
 int neighbor_list_build(cr_handle *h, double r_list, int *d_count, int64_t *d_head, int *d_list,
                         int64_t capacity, int64_t *total);
 // Body rows y[N+b] = sum_{i in b} x_i (FP64).
@@ -246,7 +288,11 @@ int body_sums(cr_handle *h, const double *x, double *y);
 // Member lists of the bodies from d_body (stable device sort).
 int topology_build(cr_handle *h);
 int objective(cr_handle *h, double *rhs);
+// The handle's preconditioner (diagonal or conductor response).
 int precondition(cr_handle *h, const double *x, double *y);
+int conductor_setup(cr_handle *h);
+int conductor_apply(cr_handle *h, const double *x, double *y);
+void conductor_free(cr_handle *h);
 // y = A x in the given precision (full operator).
 int apply_operator(cr_handle *h, const double *x, double *y, int precision);
 // Solve A x = b (x holds the warm start).

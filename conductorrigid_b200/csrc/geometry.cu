@@ -213,13 +213,19 @@ int geometry_alloc(cr_handle *h) {
     CR_TRY(dalloc(h, &h->d_keys_alt, (size_t)N));
     CR_TRY(dalloc(h, &h->d_vals, (size_t)N));
     CR_TRY(dalloc(h, &h->d_vals_alt, (size_t)N));
+    CR_TRY(realspace_alloc(h));
     // CUB scratch: the largest of the sorts and scans used here
     size_t b1 = 0, b2 = 0, b3 = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, b1, h->d_keys, h->d_keys_alt, h->d_vals, h->d_vals_alt, N);
     cub::DeviceScan::ExclusiveSum(nullptr, b2, g.tile_count, g.tile_start, std::max(h->ntiles + 1, N + 1));
     cub::TransformInputIterator<int64_t, ToI64, const int *> it(g.nl_count, ToI64());
     cub::DeviceScan::ExclusiveSum(nullptr, b3, it, g.nl_head, N);
-    size_t need = std::max(b1, std::max(b2, b3)) + 256;
+    size_t b4 = 0;
+    {
+        long long *lh = nullptr;
+        cub::DeviceScan::ExclusiveSum(nullptr, b4, g.tile_count, lh, N + 1);
+    }
+    size_t need = std::max(std::max(b1, b4), std::max(b2, b3)) + 256;
     if (need > h->sort_tmp_bytes) {
         dfree(reinterpret_cast<char **>(&h->d_sort_tmp));
         CR_TRY(dalloc(h, reinterpret_cast<char **>(&h->d_sort_tmp), need));
@@ -249,6 +255,7 @@ void geometry_free(cr_handle *h) {
     dfree(&h->d_keys_alt);
     dfree(&h->d_vals);
     dfree(&h->d_vals_alt);
+    realspace_free(h);
     dfree(reinterpret_cast<char **>(&h->d_sort_tmp));
     h->sort_tmp_bytes = 0;
 }
@@ -377,10 +384,8 @@ int geometry_update(cr_handle *h, const double *d_pos, const double *d_body_pos)
     CR_CUDA(h, cudaStreamSynchronize(h->stream));
     if (bad) return fail(h, CR_NUMERICAL, "non-finite or out-of-range bead position");
     CR_TRY(bin_beads(h, h->d_keys, h->ntiles, g.tile_count, g.tile_start, g.tile_beads));
-    CR_TRY(cell_bins(h, cg, g.cell_of, &g.cell_start, &g.ncell_alloc, g.cell_beads));
-    for (int d = 0; d < 3; ++d) g.ncell[d] = cg.nc[d];
-    CR_TRY(build_list(h, cg, g.cell_of, g.cell_start, g.cell_beads, h->d.rcut, g.nl_count, g.nl_head, &g.nl_list,
-                      &g.nl_capacity, &g.nl_total, true));
+    CR_TRY(realspace_build(h));
+    if (h->user.precond == CR_PRECOND_CONDUCTOR && !h->cond.ready) CR_TRY(conductor_setup(h));
     if (d_body_pos && h->B > 0) {
         CR_CUDA(h, cudaMemcpy2DAsync(h->d_bpos, sizeof(double4), d_body_pos, 3 * sizeof(double), 3 * sizeof(double),
                                      h->B, cudaMemcpyDeviceToDevice, h->stream));

@@ -1,163 +1,475 @@
 // realspace.cu -- real-space part of the operator and of the force pass
 // (ConductorRigid.cu:469-664).
 //
-// One warp per bead walks its neighbour list (built once per solve within rc); lanes
-// stride over the neighbours, gather positions and charges through the read-only
-// cache, apply the minimum image (ConductorRigid.cu:536), the cutoff window
-// dr^2 <= d^2 < rc^2 (cu:540) and the tabulated, linearly interpolated kernel
-// (index floor(Ntable (d - dr)/(rc - dr)), weight d/dr - index - 1, cu:549-554).  The
-// index is clamped to the table so that rounding at either end of the window never
-// reads outside it.
+// The reference walks a per-bead neighbour list in every matrix-vector product and
+// re-evaluates the tabulated kernel for each pair.  Here the geometry is fixed for a
+// whole solve, so the real-space operator is built once per solve as a symmetric
+// block-sparse matrix and every GMRES iteration streams it:
+//
+//  * clusters: beads sorted along a Morton curve of the box, cut into clusters of 32
+//    (the last one padded);
+//  * cluster pairs (I <= J) whose bounding boxes come within rc under any periodic
+//    image, found once per solve;
+//  * per pair a dense 32x32 block of T(d_ij) for dr^2 <= d^2 < rc^2 (else 0), with the
+//    minimum image, table index floor(Ntable (d - dr)/(rc - dr)) and linear weight
+//    d/dr - index - 1 of ConductorRigid.cu:536-554, evaluated in FP64 and stored in the
+//    operator precision, column-major so that lane i reads B[i][j] coalesced;
+//  * the product y_I += B x_J and, for I != J, y_J += B^T x_I (T(d_ij) = T(d_ji)), one
+//    warp per cluster I, the transpose through a padded shared-memory tile.
+//
+// The force pass (once per solve) evaluates the gradient table on the fly over the same
+// cluster pairs in FP64, with F_j -= f_ij for the mirrored half.
+#include <cub/cub.cuh>
+
 #include "cr_internal.cuh"
 
 namespace cr {
 
 namespace {
 
-template <typename R> struct RSConst {
-    R L[3], Linv[3];
-    R rc2, rmin2, dr, inv_dr, tab_scale;  // tab_scale = Ntable / (rc - dr)
+constexpr int CS = 32;  // beads per cluster
+
+struct RSBuild {
+    double L[3], Linv[3];
+    double rc, rc2, rmin2, dr, inv_dr;
     int ntab;
-    R selfc;
-    R E0[3];
 };
 
-__device__ __forceinline__ float rint_r(float x) { return rintf(x); }
-__device__ __forceinline__ double rint_r(double x) { return rint(x); }
-__device__ __forceinline__ float floor_r(float x) { return floorf(x); }
-__device__ __forceinline__ double floor_r(double x) { return floor(x); }
-__device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
-__device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
+__device__ __forceinline__ double mimg(double dx, double L, double Linv) { return dx - L * rint(dx * Linv); }
 
-template <typename R> __device__ __forceinline__ R warp_sum(R v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+// Morton key of a position on a 1024^3 lattice of the box.
+__device__ __forceinline__ unsigned spread_bits(unsigned v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
     return v;
 }
 
-template <typename R> __device__ __forceinline__ R table_lerp(const typename Prec<R>::R2 *tab, const RSConst<R> &c, R d) {
-    int ind = (int)floor_r((d - c.dr) * c.tab_scale);
+__global__ void morton_kernel(int N, const double4 *__restrict__ pos, double Lx, double Ly, double Lz, int *key,
+                              int *iota) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double4 p = pos[i];
+    const int ix = min(max((int)((p.x / Lx + 0.5) * 1024.0), 0), 1023);
+    const int iy = min(max((int)((p.y / Ly + 0.5) * 1024.0), 0), 1023);
+    const int iz = min(max((int)((p.z / Lz + 0.5) * 1024.0), 0), 1023);
+    key[i] = (int)((spread_bits(ix) << 2) | (spread_bits(iy) << 1) | spread_bits(iz));
+    iota[i] = i;
+}
+
+// Cluster members (padded with -1), centre and half extent (relative to the first
+// member under the minimum image, so clusters that cross the boundary stay compact).
+__global__ void cluster_kernel(int N, int nclus, const int *__restrict__ sorted, const double4 *__restrict__ pos,
+                               RSBuild c, int *members, double4 *centre, double4 *extent) {
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (I >= nclus) return;
+    const int k = I * CS + lane;
+    const int i = k < N ? sorted[k] : -1;
+    members[k] = i;
+    const int i0 = sorted[I * CS];
+    const double4 p0 = pos[i0];
+    double r[3] = {0, 0, 0};
+    if (i >= 0) {
+        const double4 p = pos[i];
+        r[0] = mimg(p.x - p0.x, c.L[0], c.Linv[0]);
+        r[1] = mimg(p.y - p0.y, c.L[1], c.Linv[1]);
+        r[2] = mimg(p.z - p0.z, c.L[2], c.Linv[2]);
+    }
+    double lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = i >= 0 ? r[d] : 1e300;
+        hi[d] = i >= 0 ? r[d] : -1e300;
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+            hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+        }
+    }
+    if (lane == 0) {
+        centre[I] = make_double4(p0.x + 0.5 * (lo[0] + hi[0]), p0.y + 0.5 * (lo[1] + hi[1]),
+                                 p0.z + 0.5 * (lo[2] + hi[2]), 0.0);
+        extent[I] = make_double4(0.5 * (hi[0] - lo[0]), 0.5 * (hi[1] - lo[1]), 0.5 * (hi[2] - lo[2]), 0.0);
+    }
+}
+
+// Smallest bounding-box gap between clusters I and J over the periodic images.
+__device__ __forceinline__ double box_gap2(const double4 &ci, const double4 &ei, const double4 &cj, const double4 &ej,
+                                           const RSBuild &c) {
+    const double dc[3] = {cj.x - ci.x, cj.y - ci.y, cj.z - ci.z};
+    const double es[3] = {ei.x + ej.x, ei.y + ej.y, ei.z + ej.z};
+    double g2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        const double m = mimg(dc[d], c.L[d], c.Linv[d]);
+        double best = 1e300;
+        for (int s = -1; s <= 1; ++s) {
+            const double v = fabs(m + s * c.L[d]) - es[d];
+            best = fmin(best, v > 0.0 ? v : 0.0);
+        }
+        g2 += best * best;
+    }
+    return g2;
+}
+
+// One warp per cluster I scans J >= I; FILL writes J in ascending order.
+template <bool FILL>
+__global__ void pair_search_kernel(int nclus, const double4 *__restrict__ centre, const double4 *__restrict__ extent,
+                                   RSBuild c, int *count, const long long *__restrict__ head, int *pair_j) {
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (I >= nclus) return;
+    const double4 ci = centre[I], ei = extent[I];
+    int n = 0;
+    const long long h0 = FILL ? head[I] : 0;
+    for (int base = I; base < nclus; base += 32) {
+        const int J = base + lane;
+        bool hit = false;
+        if (J < nclus) hit = J == I || box_gap2(ci, ei, centre[J], extent[J], c) < c.rc2;
+        const unsigned mask = __ballot_sync(0xffffffffu, hit);
+        if (FILL && hit) pair_j[h0 + n + __popc(mask & ((1u << lane) - 1u))] = J;
+        n += __popc(mask);
+    }
+    if (!FILL && lane == 0) count[I] = n;
+}
+
+__global__ void pair_owner_kernel(int nclus, const long long *__restrict__ head, const int *__restrict__ count,
+                                  int *pair_i) {
+    const int I = blockIdx.x;
+    if (I >= nclus) return;
+    for (int k = threadIdx.x; k < count[I]; k += blockDim.x) pair_i[head[I] + k] = I;
+}
+
+__device__ __forceinline__ double table_lerp64(const double2 *__restrict__ tab, const RSBuild &c, double d) {
+    int ind = (int)floor(c.ntab * (d - c.dr) / (c.rc - c.dr));
     ind = min(max(ind, 0), c.ntab - 1);
-    const R lin = d * c.inv_dr - (R)ind - (R)1;
-    const typename Prec<R>::R2 e = __ldg(tab + ind);
+    const double lin = d * c.inv_dr - ind - 1.0;
+    const double2 e = tab[ind];
     return e.x + (e.y - e.x) * lin;
 }
 
-// out_i = Phi_body(i) - (phik_i + self q_i + sum_j T(d_ij) q_j)   (phi_body != NULL)
-// out_i = phik_i + self q_i + sum_j T(d_ij) q_j                   (phi_body == NULL)
+// 32x32 block of tabulated potentials for every cluster pair, stored column-major
+// (entry (i, j) at j*32 + i) in the operator precision R.
 template <typename R>
-__global__ void __launch_bounds__(256) real_potential_kernel(
-    int N, const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int *__restrict__ count,
-    const int64_t *__restrict__ head, const int *__restrict__ list, const typename Prec<R>::R2 *__restrict__ tab,
-    RSConst<R> c, const R *__restrict__ phik, const double *__restrict__ phi_body, const uint32_t *__restrict__ body,
-    double *__restrict__ out) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__global__ void block_fill_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
+                                  const int *__restrict__ members, const double4 *__restrict__ pos,
+                                  const double2 *__restrict__ tab, RSBuild c, R *__restrict__ blocks) {
+    const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (i >= N) return;
-    const typename Prec<R>::R4 pi = pos[i];
-    const int64_t h0 = head[i];
-    const int n = count[i];
-    R acc = 0;
-    for (int k = lane; k < n; k += 32) {
-        const int j = __ldg(list + h0 + k);
-        const typename Prec<R>::R4 pj = pos[j];
-        R dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        dx -= c.L[0] * rint_r(dx * c.Linv[0]);
-        dy -= c.L[1] * rint_r(dy * c.Linv[1]);
-        dz -= c.L[2] * rint_r(dz * c.Linv[2]);
-        const R d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 < c.rc2 && d2 >= c.rmin2) acc += table_lerp<R>(tab, c, sqrt_r(d2)) * __ldg(q + j);
-    }
-    acc = warp_sum(acc);
-    if (lane == 0) {
-        const double total = (double)phik[i] + (double)(c.selfc * q[i]) + (double)acc;
-        out[i] = phi_body ? phi_body[body[i]] - total : total;
+    if (p >= npairs) return;
+    const int I = pair_i[p], J = pair_j[p];
+    const int bi = members[I * CS + lane];
+    const int bj = members[J * CS + lane];
+    const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
+    const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
+    R *blk = blocks + p * (CS * CS);
+    for (int j = 0; j < CS; ++j) {
+        const int vj = __shfl_sync(0xffffffffu, bj, j);
+        const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
+        const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
+        const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
+        double v = 0.0;
+        if (bi >= 0 && vj >= 0) {
+            const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
+            const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
+            const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < c.rc2 && d2 >= c.rmin2) v = table_lerp64(tab, c, sqrt(d2));
+        }
+        blk[j * CS + lane] = (R)v;
     }
 }
 
-// force_i = wave force_i + q_i E0 + sum_j -T'(d_ij) q_i q_j rhat_ij   (cu:596-662)
+// acc[bead] += sum over the cluster-pair blocks (both halves).  One warp per cluster I.
 template <typename R>
-__global__ void __launch_bounds__(256) real_force_kernel(
-    int N, const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int *__restrict__ count,
-    const int64_t *__restrict__ head, const int *__restrict__ list, const typename Prec<R>::R2 *__restrict__ tab,
-    RSConst<R> c, const R *__restrict__ fk, double *__restrict__ out) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (i >= N) return;
-    const typename Prec<R>::R4 pi = pos[i];
-    const int64_t h0 = head[i];
-    const int n = count[i];
-    R fx = 0, fy = 0, fz = 0;
-    for (int k = lane; k < n; k += 32) {
-        const int j = __ldg(list + h0 + k);
-        const typename Prec<R>::R4 pj = pos[j];
-        R dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        dx -= c.L[0] * rint_r(dx * c.Linv[0]);
-        dy -= c.L[1] * rint_r(dy * c.Linv[1]);
-        dz -= c.L[2] * rint_r(dz * c.Linv[2]);
-        const R d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 < c.rc2 && d2 >= c.rmin2) {
-            const R d = sqrt_r(d2);
-            const R a = table_lerp<R>(tab, c, d) * __ldg(q + j) / d;
-            fx -= a * dx;
-            fy -= a * dy;
-            fz -= a * dz;
+__global__ void __launch_bounds__(128) block_spmv_kernel(int nclus, const long long *__restrict__ head,
+                                                         const int *__restrict__ count,
+                                                         const int *__restrict__ pair_j,
+                                                         const int *__restrict__ members, const R *__restrict__ q,
+                                                         const R *__restrict__ blocks, R *__restrict__ acc) {
+    __shared__ R tile[4][CS][CS + 1];
+    __shared__ R xs[4][CS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int I = blockIdx.x * 4 + w;
+    if (I >= nclus) return;
+    const int bi = members[I * CS + lane];
+    const R xI = bi >= 0 ? q[bi] : (R)0;
+    xs[w][lane] = xI;
+    __syncwarp();
+    R yI = 0;
+    const long long h0 = head[I];
+    const int n = count[I];
+    for (int k = 0; k < n; ++k) {
+        const long long p = h0 + k;
+        const int J = pair_j[p];
+        const int bj = members[J * CS + lane];
+        const R xJ = bj >= 0 ? q[bj] : (R)0;
+        const R *blk = blocks + p * (CS * CS);
+        R b[CS];
+#pragma unroll
+        for (int j = 0; j < CS; ++j) b[j] = __ldg(blk + j * CS + lane);
+#pragma unroll
+        for (int j = 0; j < CS; ++j) yI += b[j] * __shfl_sync(0xffffffffu, xJ, j);
+        if (J != I) {
+#pragma unroll
+            for (int j = 0; j < CS; ++j) tile[w][j][lane] = b[j];
+            __syncwarp();
+            R t = 0;
+#pragma unroll
+            for (int i = 0; i < CS; ++i) t += tile[w][lane][i] * xs[w][i];
+            __syncwarp();
+            if (bj >= 0) atomicAdd(acc + bj, t);
         }
     }
-    fx = warp_sum(fx);
-    fy = warp_sum(fy);
-    fz = warp_sum(fz);
-    if (lane == 0) {
-        const R qi = q[i];
-        out[3 * (size_t)i + 0] = (double)fk[3 * (size_t)i + 0] + (double)(qi * c.E0[0]) + (double)(qi * fx);
-        out[3 * (size_t)i + 1] = (double)fk[3 * (size_t)i + 1] + (double)(qi * c.E0[1]) + (double)(qi * fy);
-        out[3 * (size_t)i + 2] = (double)fk[3 * (size_t)i + 2] + (double)(qi * c.E0[2]) + (double)(qi * fz);
-    }
+    if (bi >= 0) atomicAdd(acc + bi, yI);
 }
 
-template <typename R> RSConst<R> rs_const(const cr_handle *h) {
-    RSConst<R> c;
-    for (int d = 0; d < 3; ++d) {
-        c.L[d] = (R)h->L[d];
-        c.Linv[d] = (R)(1.0 / h->L[d]);
-        c.E0[d] = (R)h->field[d];
+// out_i = Phi_body(i) - (phik_i + self q_i + acc_i)   or   phik_i + self q_i + acc_i
+template <typename R>
+__global__ void combine_kernel(int N, const R *__restrict__ phik, const R *__restrict__ q, const R *__restrict__ acc,
+                               double selfc, const double *__restrict__ phi_body, const uint32_t *__restrict__ body,
+                               double *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double total = (double)phik[i] + selfc * (double)q[i] + (double)acc[i];
+    out[i] = phi_body ? phi_body[body[i]] - total : total;
+}
+
+// Real-space forces over the cluster pairs, on the fly in FP64: f_ij = -T'(d) q_i q_j
+// r_ij / d (ConductorRigid.cu:637-654), F_i += f_ij, F_j -= f_ij for I != J.
+__global__ void __launch_bounds__(128) pair_force_kernel(long long npairs, const int *__restrict__ pair_i,
+                                                         const int *__restrict__ pair_j,
+                                                         const int *__restrict__ members,
+                                                         const double4 *__restrict__ pos, const double *__restrict__ q,
+                                                         const double2 *__restrict__ tab, RSBuild c,
+                                                         double *__restrict__ F) {
+    const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (p >= npairs) return;
+    const int I = pair_i[p], J = pair_j[p];
+    const int bi = members[I * CS + lane];
+    const int bj = members[J * CS + lane];
+    const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
+    const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
+    const double qi = bi >= 0 ? q[bi] : 0.0;
+    const double qjl = bj >= 0 ? q[bj] : 0.0;
+    double fi[3] = {0, 0, 0};
+    double fjmine[3] = {0, 0, 0};
+    for (int j = 0; j < CS; ++j) {
+        const int vj = __shfl_sync(0xffffffffu, bj, j);
+        const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
+        const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
+        const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
+        const double qj = __shfl_sync(0xffffffffu, qjl, j);
+        double f[3] = {0, 0, 0};
+        if (bi >= 0 && vj >= 0) {
+            const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
+            const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
+            const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < c.rc2 && d2 >= c.rmin2) {
+                const double d = sqrt(d2);
+                const double a = -table_lerp64(tab, c, d) * qi * qj / d;
+                f[0] = a * dx;
+                f[1] = a * dy;
+                f[2] = a * dz;
+            }
+        }
+        for (int e = 0; e < 3; ++e) fi[e] += f[e];
+        if (J != I) {
+            double s[3] = {f[0], f[1], f[2]};
+            for (int e = 0; e < 3; ++e)
+                for (int o = 16; o > 0; o >>= 1) s[e] += __shfl_xor_sync(0xffffffffu, s[e], o);
+            if (lane == j)
+                for (int e = 0; e < 3; ++e) fjmine[e] = s[e];
+        }
     }
-    c.rc2 = (R)(h->d.rcut * h->d.rcut);
-    c.rmin2 = (R)(h->d.dr * h->d.dr);
-    c.dr = (R)h->d.dr;
-    c.inv_dr = (R)(1.0 / h->d.dr);
-    c.tab_scale = (R)(h->d.n_table / (h->d.rcut - h->d.dr));
+    if (bi >= 0)
+        for (int e = 0; e < 3; ++e) atomicAdd(F + 3 * (size_t)bi + e, fi[e]);
+    if (J != I && bj >= 0)
+        for (int e = 0; e < 3; ++e) atomicAdd(F + 3 * (size_t)bj + e, -fjmine[e]);
+}
+
+// force_i = wave force_i + q_i E0 + real-space force_i
+template <typename R>
+__global__ void force_combine_kernel(int N, const R *__restrict__ fk, const double *__restrict__ q, double Ex,
+                                     double Ey, double Ez, const double *__restrict__ freal, double *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double qi = q[i];
+    out[3 * (size_t)i + 0] = (double)fk[3 * (size_t)i + 0] + qi * Ex + freal[3 * (size_t)i + 0];
+    out[3 * (size_t)i + 1] = (double)fk[3 * (size_t)i + 1] + qi * Ey + freal[3 * (size_t)i + 1];
+    out[3 * (size_t)i + 2] = (double)fk[3 * (size_t)i + 2] + qi * Ez + freal[3 * (size_t)i + 2];
+}
+
+RSBuild rs_build(const cr_handle *h) {
+    RSBuild c;
+    for (int d = 0; d < 3; ++d) {
+        c.L[d] = h->L[d];
+        c.Linv[d] = 1.0 / h->L[d];
+    }
+    c.rc = h->d.rcut;
+    c.rc2 = h->d.rcut * h->d.rcut;
+    c.rmin2 = h->d.dr * h->d.dr;
+    c.dr = h->d.dr;
+    c.inv_dr = 1.0 / h->d.dr;
     c.ntab = h->d.n_table;
-    c.selfc = (R)h->d.selfcoeff;
     return c;
+}
+
+template <typename R> R *acc_of(RealSpace &r);
+template <> float *acc_of<float>(RealSpace &r) { return r.acc32; }
+template <> double *acc_of<double>(RealSpace &r) { return r.acc64; }
+template <typename R> R *&blocks_of(RealSpace &r);
+template <> float *&blocks_of<float>(RealSpace &r) { return r.blocks32; }
+template <> double *&blocks_of<double>(RealSpace &r) { return r.blocks64; }
+template <typename R> bool &valid_of(RealSpace &r);
+template <> bool &valid_of<float>(RealSpace &r) { return r.valid32; }
+template <> bool &valid_of<double>(RealSpace &r) { return r.valid64; }
+template <typename R> long long &cap_of(RealSpace &r);
+template <> long long &cap_of<float>(RealSpace &r) { return r.blocks32_cap; }
+template <> long long &cap_of<double>(RealSpace &r) { return r.blocks64_cap; }
+
+// Fill the blocks of precision R for the current cluster pairs (once per solve).
+template <typename R> int realspace_blocks(cr_handle *h) {
+    RealSpace &r = h->rs;
+    if (valid_of<R>(r) || h->N == 0) return CR_OK;
+    const long long need = r.npairs * CS * CS;
+    if (need > cap_of<R>(r)) {
+        const long long cap = need + need / 8;
+        CR_TRY(dalloc(h, &blocks_of<R>(r), (size_t)cap));
+        cap_of<R>(r) = cap;
+    }
+    block_fill_kernel<R><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
+        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), blocks_of<R>(r));
+    CR_LAUNCH(h, "block_fill_kernel");
+    valid_of<R>(r) = true;
+    return CR_OK;
 }
 
 }  // namespace
 
-template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out) {
-    const int N = h->N;
-    if (N == 0) return CR_OK;
-    ProfScope ps(h, PROF_REAL);
-    real_potential_kernel<R><<<blocks_for((long)N * 32, 256), 256, 0, h->stream>>>(
-        N, m.pos, m.q, h->geo.nl_count, h->geo.nl_head, h->geo.nl_list, m.phiq, rs_const<R>(h), m.phi, phi_body,
-        h->d_body, out);
-    CR_LAUNCH(h, "real_potential_kernel");
+void realspace_free(cr_handle *h) {
+    RealSpace &r = h->rs;
+    dfree(&r.members);
+    dfree(&r.centre);
+    dfree(&r.extent);
+    dfree(&r.count);
+    dfree(&r.head);
+    dfree(&r.pair_i);
+    dfree(&r.pair_j);
+    dfree(&r.blocks32);
+    dfree(&r.blocks64);
+    dfree(&r.acc32);
+    dfree(&r.acc64);
+    dfree(&r.freal);
+    r.pair_cap = 0;
+    r.blocks32_cap = r.blocks64_cap = 0;
+    r.npairs = 0;
+    r.valid32 = r.valid64 = false;
+}
+
+int realspace_alloc(cr_handle *h) {
+    RealSpace &r = h->rs;
+    realspace_free(h);
+    r.nclus = (h->N + CS - 1) / CS;
+    const size_t nc = (size_t)std::max(r.nclus, 1);
+    CR_TRY(dalloc(h, &r.members, nc * CS));
+    CR_TRY(dalloc(h, &r.centre, nc));
+    CR_TRY(dalloc(h, &r.extent, nc));
+    CR_TRY(dalloc(h, &r.count, nc));
+    CR_TRY(dalloc(h, &r.head, nc));
+    CR_TRY(dalloc(h, &r.sorted, (size_t)std::max(h->N, 1)));
+    CR_TRY(dalloc(h, &r.acc32, (size_t)std::max(h->N, 1)));
+    CR_TRY(dalloc(h, &r.acc64, (size_t)std::max(h->N, 1)));
+    CR_TRY(dalloc(h, &r.freal, 3 * (size_t)std::max(h->N, 1)));
     return CR_OK;
 }
 
-template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, double *force_out) {
+// Clusters and cluster pairs of the current positions; blocks are filled on first
+// use per precision.
+int realspace_build(cr_handle *h) {
+    RealSpace &r = h->rs;
+    const int N = h->N;
+    r.valid32 = r.valid64 = false;
+    if (N == 0) return CR_OK;
+    cudaStream_t s = h->stream;
+    const RSBuild c = rs_build(h);
+    morton_kernel<<<blocks_for(N, 256), 256, 0, s>>>(N, h->m64.pos, h->L[0], h->L[1], h->L[2], h->d_keys,
+                                                     h->d_vals_alt);
+    CR_LAUNCH(h, "morton_kernel");
+    size_t bytes = h->sort_tmp_bytes;
+    CR_CUDA(h, cub::DeviceRadixSort::SortPairs(h->d_sort_tmp, bytes, h->d_keys, h->d_keys_alt, h->d_vals_alt,
+                                               r.sorted, N, 0, 30, s));
+    const int nb = blocks_for((long)r.nclus * 32, 256);
+    cluster_kernel<<<nb, 256, 0, s>>>(N, r.nclus, r.sorted, h->m64.pos, c, r.members, r.centre, r.extent);
+    CR_LAUNCH(h, "cluster_kernel");
+    pair_search_kernel<false><<<nb, 256, 0, s>>>(r.nclus, r.centre, r.extent, c, r.count, nullptr, nullptr);
+    CR_LAUNCH(h, "pair_search_kernel");
+    bytes = h->sort_tmp_bytes;
+    CR_CUDA(h, cub::DeviceScan::ExclusiveSum(h->d_sort_tmp, bytes, r.count, r.head, r.nclus, s));
+    long long last_head = 0;
+    int last_count = 0;
+    CR_CUDA(h, cudaMemcpyAsync(&last_head, r.head + r.nclus - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(h, cudaMemcpyAsync(&last_count, r.count + r.nclus - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(h, cudaStreamSynchronize(s));
+    r.npairs = last_head + last_count;
+    if (r.npairs > r.pair_cap) {
+        const long long cap = r.npairs + r.npairs / 8 + 64;
+        CR_TRY(dalloc(h, &r.pair_i, (size_t)cap));
+        CR_TRY(dalloc(h, &r.pair_j, (size_t)cap));
+        r.pair_cap = cap;
+    }
+    pair_search_kernel<true><<<nb, 256, 0, s>>>(r.nclus, r.centre, r.extent, c, r.count, r.head, r.pair_j);
+    CR_LAUNCH(h, "pair_search_kernel");
+    pair_owner_kernel<<<r.nclus, 128, 0, s>>>(r.nclus, r.head, r.count, r.pair_i);
+    CR_LAUNCH(h, "pair_owner_kernel");
+    // entries the real-space product walks per application (for traffic arithmetic)
+    h->geo.nl_total = r.npairs * CS * CS;
+    return CR_OK;
+}
+
+template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out) {
     const int N = h->N;
     if (N == 0) return CR_OK;
+    RealSpace &r = h->rs;
+    {
+        ProfScope pb(h, PROF_GEOMETRY);
+        CR_TRY(realspace_blocks<R>(h));
+    }
+    R *acc = acc_of<R>(r);
+    {
+        ProfScope ps(h, PROF_REAL);
+        CR_CUDA(h, cudaMemsetAsync(acc, 0, (size_t)N * sizeof(R), h->stream));
+        block_spmv_kernel<R><<<(r.nclus + 3) / 4, 128, 0, h->stream>>>(r.nclus, r.head, r.count, r.pair_j, r.members,
+                                                                       m.q, blocks_of<R>(r), acc);
+        CR_LAUNCH(h, "block_spmv_kernel");
+    }
+    ProfScope pc(h, PROF_BODY);
+    combine_kernel<R><<<blocks_for(N, 256), 256, 0, h->stream>>>(N, m.phi, m.q, acc, h->d.selfcoeff, phi_body,
+                                                                 h->d_body, out);
+    CR_LAUNCH(h, "combine_kernel");
+    return CR_OK;
+}
+
+template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, const double *q64, double *force_out) {
+    const int N = h->N;
+    if (N == 0) return CR_OK;
+    RealSpace &r = h->rs;
     ProfScope ps(h, PROF_REAL_FORCE);
-    real_force_kernel<R><<<blocks_for((long)N * 32, 256), 256, 0, h->stream>>>(
-        N, m.pos, m.q, h->geo.nl_count, h->geo.nl_head, h->geo.nl_list, m.gradphiq, rs_const<R>(h), m.force,
-        force_out);
-    CR_LAUNCH(h, "real_force_kernel");
+    CR_CUDA(h, cudaMemsetAsync(r.freal, 0, 3 * (size_t)N * sizeof(double), h->stream));
+    pair_force_kernel<<<blocks_for(r.npairs * 32, 128), 128, 0, h->stream>>>(
+        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, q64, h->m64.gradphiq, rs_build(h), r.freal);
+    CR_LAUNCH(h, "pair_force_kernel");
+    force_combine_kernel<R><<<blocks_for(N, 256), 256, 0, h->stream>>>(N, m.force, q64, h->field[0], h->field[1],
+                                                                       h->field[2], r.freal, force_out);
+    CR_LAUNCH(h, "force_combine_kernel");
     return CR_OK;
 }
 
 template int real_space_apply<float>(cr_handle *, MeshBuffers<float> &, const double *, double *);
 template int real_space_apply<double>(cr_handle *, MeshBuffers<double> &, const double *, double *);
-template int real_space_force<float>(cr_handle *, MeshBuffers<float> &, double *);
-template int real_space_force<double>(cr_handle *, MeshBuffers<double> &, double *);
+template int real_space_force<float>(cr_handle *, MeshBuffers<float> &, const double *, double *);
+template int real_space_force<double>(cr_handle *, MeshBuffers<double> &, const double *, double *);
 
 }  // namespace cr

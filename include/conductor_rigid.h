@@ -46,6 +46,11 @@ typedef enum {
 } cr_status;
 
 typedef enum {
+    CR_PRECOND_DIAGONAL = 0,  /* the reference's diagonal preconditioner (ConductorRigid.cu:816-859) */
+    CR_PRECOND_CONDUCTOR = 1  /* exact isolated-conductor response per body (block inverse) */
+} cr_preconditioner;
+
+typedef enum {
     CR_FP64 = 0,    /* every operator and reduction in FP64 (the plain solve) */
     CR_MIXED = 1,   /* FP32 operator inside FP64-Arnoldi flexible GMRES, FP64 refinement */
     CR_FP32 = 2     /* FP32 operator only (testing) */
@@ -66,6 +71,7 @@ typedef struct {
     int maxiter;        /* >0 overrides the iteration limit (100, cu:1134) */
     int precision;      /* cr_precision */
     int learned;        /* 1: use the learned initial guess / preconditioner correction */
+    int precond;        /* cr_preconditioner */
 } cr_params;
 
 /* Derived parameters (ConductorRigid.cc:116-207, ConductorRigid.cu:912-917). */
@@ -145,7 +151,8 @@ int cr_set_positions(cr_handle *h, const double *d_pos, const double *d_body_pos
 /* y = A x, x = [q; Phi], y = [Phi_b - M q; sum_b q] (MatrixVectorMultiply,
  * ConductorRigid.cu:953-1020), with the operator in `precision` (CR_FP64/CR_FP32). */
 int cr_apply_operator(cr_handle *h, const double *d_x, double *d_y, int precision);
-/* Diagonal preconditioner (Precondition, ConductorRigid.cu:1023-1044). */
+/* The handle's preconditioner: the reference's diagonal scaling (Precondition,
+ * ConductorRigid.cu:1023-1044) or the conductor response (cr_params.precond). */
 int cr_precondition(cr_handle *h, const double *d_x, double *d_y);
 /* Right-hand side [-(r_i - R_b).E0 ; Q_b] (compute_objective, cu:764-813). */
 int cr_objective(cr_handle *h, double *d_rhs);
@@ -172,7 +179,8 @@ int cr_neighbor_list(cr_handle *h, double r_list, int *d_count, int64_t *d_head,
  * handle's stream; cr_profile_read returns launches and summed device time of one
  * class since the last reset.  Classes: 0 spread, 1 FFT, 2 influence-function scale,
  * 3 contract, 4 real-space potential, 5 contract force, 6 real-space force,
- * 7 Krylov vector ops, 8 body rows, 9 per-solve geometry (binning, neighbour list). */
+ * 7 Krylov vector ops, 8 body rows, 9 per-solve geometry (binning, neighbour list),
+ * 10 preconditioner. */
 int cr_profile(cr_handle *h, int enable);   /* enable/disable; also resets the record */
 int cr_profile_read(cr_handle *h, int kernel_class, int *launches, double *total_ms);
 /* Sizes of the current per-solve geometry (for traffic and roofline arithmetic). */

@@ -192,3 +192,57 @@ def test_empty_system(cuda, product_lib):
     g = h.spread(np.zeros(0))
     assert float(g.abs().max()) == 0.0
     h.close()
+
+
+def _dense_conductor_apply(s, v):
+    """Isolated-conductor block inverse per body with the free-space shell kernel."""
+    N = s.n_beads
+    z = np.zeros_like(v)
+    for b in range(s.n_bodies):
+        idx = np.nonzero(s.body == b)[0]
+        x = s.pos[idx]
+        d = x[:, None, :] - x[None, :, :]
+        d -= s.L * np.rint(d / s.L)
+        D = np.linalg.norm(d, axis=-1)
+        K = np.where(D < 2, (4 - D) / (16 * np.pi), 1 / (4 * np.pi * np.maximum(D, 1e-300)))
+        np.fill_diagonal(K, 1 / (4 * np.pi))
+        n = len(idx)
+        A = np.zeros((n + 1, n + 1))
+        A[:n, :n] = -K
+        A[:n, n] = 1
+        A[n, :n] = 1
+        sol = np.linalg.solve(A, np.r_[v[idx], v[N + b]])
+        z[idx] = sol[:n]
+        z[N + b] = sol[n]
+    return z
+
+
+def test_conductor_preconditioner_matches_dense(gold, product_lib):
+    g, s, _ = gold
+    params = dict(xi=float(g["xi"]), errortol=float(g["errortol"]), grid=int(g["grid"]), support=int(g["support"]),
+                  rcut=float(g["rcut"]))
+    h = make_handle(product_lib, s, params, precond="conductor")
+    v = np.random.default_rng(9).standard_normal(s.n_beads + s.n_bodies)
+    assert rel(h.precondition(v), _dense_conductor_apply(s, v)) < 1e-10
+    h.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_conductor_preconditioned_solve_matches_oracle(cuda, product_lib, oracle_lib, precision):
+    from conductorrigid_b200 import systems
+
+    w = systems.workload("plain_small", scale=0.3)
+    s, p = w.system, w.params
+    orc = oracle_lib.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    ref = orc.solve(s.field, restart=100, maxiter=4000, tol=1e-11)
+    h = make_handle(product_lib, s, {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")},
+                    gmres_tol=1e-6, restart=50, maxiter=4000, precision=precision, precond="conductor")
+    q = h.dev(np.zeros(s.n_beads))
+    phi = h.dev(np.zeros(s.n_bodies))
+    F, st = h.compute(s.pos, s.body_pos, q, phi)
+    h.close()
+    eq, ep, ef = rel(q, ref["q"]), rel(phi, ref["phi"]), rel(F, ref["force"])
+    print(f"\nconductor {precision}: iters={st['iterations']} resid={st['final_residual']:.2e} "
+          f"err q={eq:.2e} phi={ep:.2e} F={ef:.2e}")
+    assert st["converged"] == 1 and st["final_residual"] <= 1e-6
+    assert eq < 1e-3 and ep < 1e-3 and ef < 1e-3
