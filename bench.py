@@ -125,7 +125,7 @@ class ClockSampler:
                 "power_w_max": max(pw) if pw else None, "samples": len(rows), "reasons": sorted(reasons)}
 
 
-def algorithmic_bytes(kind: str, prec_bytes: int, N: int, G: int, pairs: int) -> float:
+def algorithmic_bytes(kind: str, prec_bytes: int, N: int, G: int, pairs: int, cluster_pairs: int = 0) -> float:
     s = prec_bytes
     pos = 16 if s == 4 else 32
     if kind == "spread":
@@ -135,7 +135,9 @@ def algorithmic_bytes(kind: str, prec_bytes: int, N: int, G: int, pairs: int) ->
     if kind == "contract_force":
         return G * s + N * (pos + s) + N * 3 * s
     if kind == "real_space":
-        return 4.0 * pairs + N * (pos + 2 * s)
+        # packed pair values + 128-byte bit mask and 12-byte index/offset per cluster pair
+        # + charges in and potentials out
+        return float(s) * pairs + 140.0 * cluster_pairs + N * (4 + 2 * s)
     if kind == "real_space_force":
         return 4.0 * pairs + N * (pos + 2 * s) + N * 3 * 8
     if kind == "fft":
@@ -316,7 +318,7 @@ def main() -> None:
     G = int(np.prod([p["grid"]] * 3))
     dom = max((k for k in prof if k not in ("geometry",)), key=lambda k: prof[k]["ms"])
     dom_ms = prof[dom]["ms"] / max(prof[dom]["launches"], 1)
-    alg = algorithmic_bytes(dom, 4, s.n_beads, G, geo["real_space_pairs"])
+    alg = algorithmic_bytes(dom, 4, s.n_beads, G, geo["real_space_pairs"], geo["cluster_pairs"])
     peak, peak_kind = load_peaks()
     achieved = alg / (dom_ms * 1e-3) / 1e9
     traffic = None

@@ -105,6 +105,7 @@ class CrGeometryInfo(C.Structure):
         ("n_tiles", C.c_int),
         ("n_beads", C.c_int),
         ("n_bodies", C.c_int),
+        ("cluster_pairs", C.c_int64),
     ]
 
 

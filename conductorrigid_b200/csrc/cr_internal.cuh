@@ -76,7 +76,7 @@ struct Geometry {
 };
 
 // Real-space operator of the current geometry: 32-bead clusters, cluster pairs
-// (I <= J) within rc, and per pair a 32x32 block of tabulated kernel values.
+// (I <= J) within rc, per pair a 32x32 bit mask and the packed kernel values.
 struct RealSpace {
     int nclus = 0;
     int *sorted = nullptr;          // [N] beads in Morton order
@@ -87,8 +87,12 @@ struct RealSpace {
     long long *head = nullptr;      // [nclus] first pair of cluster I
     int *pair_i = nullptr, *pair_j = nullptr;
     long long npairs = 0, pair_cap = 0;
-    float *blocks32 = nullptr;      // [npairs*1024]
-    double *blocks64 = nullptr;     // [npairs*1024]
+    unsigned *masks = nullptr;      // [npairs*32] row bit masks of in-range bead pairs
+    int *nnz_pair = nullptr;        // [npairs] set bits per pair
+    long long *voff = nullptr;      // [npairs] first packed value of each pair
+    long long nnz = 0;              // stored values
+    float *vals32 = nullptr;        // [nnz] packed T(d) values
+    double *vals64 = nullptr;
     long long blocks32_cap = 0, blocks64_cap = 0;
     bool valid32 = false, valid64 = false;
     float *acc32 = nullptr;         // [N] product accumulators

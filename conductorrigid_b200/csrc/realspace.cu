@@ -10,12 +10,16 @@
 //    (the last one padded);
 //  * cluster pairs (I <= J) whose bounding boxes come within rc under any periodic
 //    image, found once per solve;
-//  * per pair a dense 32x32 block of T(d_ij) for dr^2 <= d^2 < rc^2 (else 0), with the
-//    minimum image, table index floor(Ntable (d - dr)/(rc - dr)) and linear weight
-//    d/dr - index - 1 of ConductorRigid.cu:536-554, evaluated in FP64 and stored in the
-//    operator precision, column-major so that lane i reads B[i][j] coalesced;
+//  * per pair a 32x32 bit mask (row i, bit j) of the bead pairs with
+//    dr^2 <= d^2 < rc^2 under the minimum image (ConductorRigid.cu:536-540), and the
+//    values T(d_ij) of just those pairs, packed row by row, with the table index
+//    floor(Ntable (d - dr)/(rc - dr)) and linear weight d/dr - index - 1 of
+//    ConductorRigid.cu:549-554, evaluated in FP64 and stored in the operator
+//    precision (the 32x32 blocks of a 4 A cutoff are only 20-35% full, so the mask
+//    keeps the streamed bytes close to one value per interacting pair);
 //  * the product y_I += B x_J and, for I != J, y_J += B^T x_I (T(d_ij) = T(d_ji)), one
-//    warp per cluster I, the transpose through a padded shared-memory tile.
+//    warp per cluster I, lane i walking the set bits of its row, x_J and the
+//    transposed partial sums in shared memory.
 //
 // The force pass (once per solve) evaluates the gradient table on the fly over the same
 // cluster pairs in FP64, with F_j -= f_ij for the mirrored half.
@@ -148,12 +152,11 @@ __device__ __forceinline__ double table_lerp64(const double2 *__restrict__ tab, 
     return e.x + (e.y - e.x) * lin;
 }
 
-// 32x32 block of tabulated potentials for every cluster pair, stored column-major
-// (entry (i, j) at j*32 + i) in the operator precision R.
-template <typename R>
-__global__ void block_fill_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
-                                  const int *__restrict__ members, const double4 *__restrict__ pos,
-                                  const double2 *__restrict__ tab, RSBuild c, R *__restrict__ blocks) {
+// Bit masks of the in-range bead pairs of every cluster pair (row i = bead i of I,
+// bit j = bead j of J) and the number of set bits per pair.
+__global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
+                                 const int *__restrict__ members, const double4 *__restrict__ pos, RSBuild c,
+                                 unsigned *__restrict__ masks, int *__restrict__ nnz) {
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (p >= npairs) return;
@@ -162,40 +165,81 @@ __global__ void block_fill_kernel(long long npairs, const int *__restrict__ pair
     const int bj = members[J * CS + lane];
     const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
     const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
-    R *blk = blocks + p * (CS * CS);
+    unsigned m = 0;
     for (int j = 0; j < CS; ++j) {
         const int vj = __shfl_sync(0xffffffffu, bj, j);
         const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
         const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
         const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
-        double v = 0.0;
         if (bi >= 0 && vj >= 0) {
             const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
             const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
             const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
             const double d2 = dx * dx + dy * dy + dz * dz;
-            if (d2 < c.rc2 && d2 >= c.rmin2) v = table_lerp64(tab, c, sqrt(d2));
+            if (d2 < c.rc2 && d2 >= c.rmin2) m |= 1u << j;
         }
-        blk[j * CS + lane] = (R)v;
+    }
+    masks[p * CS + lane] = m;
+    int n = __popc(m);
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    if (lane == 0) nnz[p] = n;
+}
+
+__device__ __forceinline__ int warp_exclusive_scan(int v, int lane) {
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    return incl - v;
+}
+
+// Packed values T(d_ij) of the set mask bits, row by row, in the operator precision.
+template <typename R>
+__global__ void pair_values_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
+                                   const int *__restrict__ members, const double4 *__restrict__ pos,
+                                   const double2 *__restrict__ tab, RSBuild c, const unsigned *__restrict__ masks,
+                                   const long long *__restrict__ voff, R *__restrict__ vals) {
+    const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (p >= npairs) return;
+    const int I = pair_i[p], J = pair_j[p];
+    const int bi = members[I * CS + lane];
+    const int bj = members[J * CS + lane];
+    const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
+    const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
+    const unsigned m = masks[p * CS + lane];
+    long long at = voff[p] + warp_exclusive_scan(__popc(m), lane);
+    for (int j = 0; j < CS; ++j) {
+        const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
+        const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
+        const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
+        if (m & (1u << j)) {
+            const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
+            const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
+            const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
+            vals[at++] = (R)table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
+        }
     }
 }
 
-// acc[bead] += sum over the cluster-pair blocks (both halves).  One warp per cluster I.
+// acc[bead] += sum over the cluster pairs (both halves).  One warp per cluster I; lane
+// i walks the set bits of row i.
 template <typename R>
-__global__ void __launch_bounds__(128) block_spmv_kernel(int nclus, const long long *__restrict__ head,
-                                                         const int *__restrict__ count,
-                                                         const int *__restrict__ pair_j,
-                                                         const int *__restrict__ members, const R *__restrict__ q,
-                                                         const R *__restrict__ blocks, R *__restrict__ acc) {
-    __shared__ R tile[4][CS][CS + 1];
-    __shared__ R xs[4][CS];
+__global__ void __launch_bounds__(128) pair_spmv_kernel(int nclus, const long long *__restrict__ head,
+                                                        const int *__restrict__ count, const int *__restrict__ pair_j,
+                                                        const int *__restrict__ members,
+                                                        const unsigned *__restrict__ masks,
+                                                        const long long *__restrict__ voff,
+                                                        const R *__restrict__ vals, const R *__restrict__ q,
+                                                        R *__restrict__ acc) {
+    __shared__ R xJs[4][CS];
+    __shared__ R tJ[4][CS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int I = blockIdx.x * 4 + w;
     if (I >= nclus) return;
     const int bi = members[I * CS + lane];
     const R xI = bi >= 0 ? q[bi] : (R)0;
-    xs[w][lane] = xI;
-    __syncwarp();
     R yI = 0;
     const long long h0 = head[I];
     const int n = count[I];
@@ -203,23 +247,25 @@ __global__ void __launch_bounds__(128) block_spmv_kernel(int nclus, const long l
         const long long p = h0 + k;
         const int J = pair_j[p];
         const int bj = members[J * CS + lane];
-        const R xJ = bj >= 0 ? q[bj] : (R)0;
-        const R *blk = blocks + p * (CS * CS);
-        R b[CS];
-#pragma unroll
-        for (int j = 0; j < CS; ++j) b[j] = __ldg(blk + j * CS + lane);
-#pragma unroll
-        for (int j = 0; j < CS; ++j) yI += b[j] * __shfl_sync(0xffffffffu, xJ, j);
-        if (J != I) {
-#pragma unroll
-            for (int j = 0; j < CS; ++j) tile[w][j][lane] = b[j];
-            __syncwarp();
-            R t = 0;
-#pragma unroll
-            for (int i = 0; i < CS; ++i) t += tile[w][lane][i] * xs[w][i];
-            __syncwarp();
-            if (bj >= 0) atomicAdd(acc + bj, t);
+        xJs[w][lane] = bj >= 0 ? q[bj] : (R)0;
+        tJ[w][lane] = (R)0;
+        unsigned m = masks[p * CS + lane];
+        const R *v = vals + voff[p] + warp_exclusive_scan(__popc(m), lane);
+        __syncwarp();
+        const bool mirror = J != I;
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            const R t = __ldg(v++);
+            yI += t * xJs[w][j];
+            if (mirror) atomicAdd(&tJ[w][j], t * xI);
         }
+        __syncwarp();
+        if (mirror && bj >= 0) {
+            const R t = tJ[w][lane];
+            if (t != (R)0) atomicAdd(acc + bj, t);
+        }
+        __syncwarp();
     }
     if (bi >= 0) atomicAdd(acc + bi, yI);
 }
@@ -321,8 +367,8 @@ template <typename R> R *acc_of(RealSpace &r);
 template <> float *acc_of<float>(RealSpace &r) { return r.acc32; }
 template <> double *acc_of<double>(RealSpace &r) { return r.acc64; }
 template <typename R> R *&blocks_of(RealSpace &r);
-template <> float *&blocks_of<float>(RealSpace &r) { return r.blocks32; }
-template <> double *&blocks_of<double>(RealSpace &r) { return r.blocks64; }
+template <> float *&blocks_of<float>(RealSpace &r) { return r.vals32; }
+template <> double *&blocks_of<double>(RealSpace &r) { return r.vals64; }
 template <typename R> bool &valid_of(RealSpace &r);
 template <> bool &valid_of<float>(RealSpace &r) { return r.valid32; }
 template <> bool &valid_of<double>(RealSpace &r) { return r.valid64; }
@@ -330,19 +376,20 @@ template <typename R> long long &cap_of(RealSpace &r);
 template <> long long &cap_of<float>(RealSpace &r) { return r.blocks32_cap; }
 template <> long long &cap_of<double>(RealSpace &r) { return r.blocks64_cap; }
 
-// Fill the blocks of precision R for the current cluster pairs (once per solve).
+// Packed values of precision R for the current cluster pairs (once per solve).
 template <typename R> int realspace_blocks(cr_handle *h) {
     RealSpace &r = h->rs;
     if (valid_of<R>(r) || h->N == 0) return CR_OK;
-    const long long need = r.npairs * CS * CS;
+    const long long need = std::max(r.nnz, 1LL);
     if (need > cap_of<R>(r)) {
         const long long cap = need + need / 8;
         CR_TRY(dalloc(h, &blocks_of<R>(r), (size_t)cap));
         cap_of<R>(r) = cap;
     }
-    block_fill_kernel<R><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
-        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), blocks_of<R>(r));
-    CR_LAUNCH(h, "block_fill_kernel");
+    pair_values_kernel<R><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
+        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.voff,
+        blocks_of<R>(r));
+    CR_LAUNCH(h, "pair_values_kernel");
     valid_of<R>(r) = true;
     return CR_OK;
 }
@@ -358,12 +405,16 @@ void realspace_free(cr_handle *h) {
     dfree(&r.head);
     dfree(&r.pair_i);
     dfree(&r.pair_j);
-    dfree(&r.blocks32);
-    dfree(&r.blocks64);
+    dfree(&r.vals32);
+    dfree(&r.vals64);
+    dfree(&r.masks);
+    dfree(&r.nnz_pair);
+    dfree(&r.voff);
     dfree(&r.acc32);
     dfree(&r.acc64);
     dfree(&r.freal);
     r.pair_cap = 0;
+    r.nnz = 0;
     r.blocks32_cap = r.blocks64_cap = 0;
     r.npairs = 0;
     r.valid32 = r.valid64 = false;
@@ -418,14 +469,36 @@ int realspace_build(cr_handle *h) {
         const long long cap = r.npairs + r.npairs / 8 + 64;
         CR_TRY(dalloc(h, &r.pair_i, (size_t)cap));
         CR_TRY(dalloc(h, &r.pair_j, (size_t)cap));
+        CR_TRY(dalloc(h, &r.masks, (size_t)cap * CS));
+        CR_TRY(dalloc(h, &r.nnz_pair, (size_t)cap));
+        CR_TRY(dalloc(h, &r.voff, (size_t)cap));
         r.pair_cap = cap;
+        // scan scratch for npairs entries
+        size_t b = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, b, r.nnz_pair, r.voff, (int)cap);
+        if (b + 256 > h->sort_tmp_bytes) {
+            dfree(reinterpret_cast<char **>(&h->d_sort_tmp));
+            CR_TRY(dalloc(h, reinterpret_cast<char **>(&h->d_sort_tmp), b + 256));
+            h->sort_tmp_bytes = b + 256;
+        }
     }
     pair_search_kernel<true><<<nb, 256, 0, s>>>(r.nclus, r.centre, r.extent, c, r.count, r.head, r.pair_j);
     CR_LAUNCH(h, "pair_search_kernel");
     pair_owner_kernel<<<r.nclus, 128, 0, s>>>(r.nclus, r.head, r.count, r.pair_i);
     CR_LAUNCH(h, "pair_owner_kernel");
-    // entries the real-space product walks per application (for traffic arithmetic)
-    h->geo.nl_total = r.npairs * CS * CS;
+    const int pb = blocks_for(r.npairs * 32, 256);
+    pair_mask_kernel<<<pb, 256, 0, s>>>(r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, c, r.masks, r.nnz_pair);
+    CR_LAUNCH(h, "pair_mask_kernel");
+    bytes = h->sort_tmp_bytes;
+    CR_CUDA(h, cub::DeviceScan::ExclusiveSum(h->d_sort_tmp, bytes, r.nnz_pair, r.voff, (int)r.npairs, s));
+    long long last_off = 0;
+    int last_nnz = 0;
+    CR_CUDA(h, cudaMemcpyAsync(&last_off, r.voff + r.npairs - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(h, cudaMemcpyAsync(&last_nnz, r.nnz_pair + r.npairs - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(h, cudaStreamSynchronize(s));
+    r.nnz = last_off + last_nnz;
+    // stored values the real-space product streams per application
+    h->geo.nl_total = r.nnz;
     return CR_OK;
 }
 
@@ -441,9 +514,9 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
     {
         ProfScope ps(h, PROF_REAL);
         CR_CUDA(h, cudaMemsetAsync(acc, 0, (size_t)N * sizeof(R), h->stream));
-        block_spmv_kernel<R><<<(r.nclus + 3) / 4, 128, 0, h->stream>>>(r.nclus, r.head, r.count, r.pair_j, r.members,
-                                                                       m.q, blocks_of<R>(r), acc);
-        CR_LAUNCH(h, "block_spmv_kernel");
+        pair_spmv_kernel<R><<<(r.nclus + 3) / 4, 128, 0, h->stream>>>(r.nclus, r.head, r.count, r.pair_j, r.members,
+                                                                      r.masks, r.voff, blocks_of<R>(r), m.q, acc);
+        CR_LAUNCH(h, "pair_spmv_kernel");
     }
     ProfScope pc(h, PROF_BODY);
     combine_kernel<R><<<blocks_for(N, 256), 256, 0, h->stream>>>(N, m.phi, m.q, acc, h->d.selfcoeff, phi_body,

@@ -127,7 +127,7 @@ int op_apply(cr_handle *h, int precision, const double *x, double *y, OpCount &o
 enum { kResidualCompute = 0, kResidualIsB = 1, kResidualReady = 2 };
 
 int fgmres(cr_handle *h, int precision, double *x, const double *b, int r_mode, double atol, int maxit,
-           int *iters, int *restarts, double *final_norm, OpCount &oc) {
+           int *iters, int *restarts, double *final_norm, OpCount &oc, bool single_cycle = false) {
     Krylov &K = h->kry;
     const int n = K.n, m = K.m;
     const int nb = vec_blocks(n);
@@ -202,6 +202,11 @@ int fgmres(cr_handle *h, int precision, double *x, const double *b, int r_mode, 
         update_kernel<<<nb, 256, 0, h->stream>>>(n, j, K.Z, K.yvec, x);
         CR_LAUNCH(h, "update_kernel");
         ++*restarts;
+        if (single_cycle) {
+            // the caller recomputes the residual in higher precision
+            beta = std::fabs(g[j]);
+            break;
+        }
         // true residual of this operator
         CR_TRY(op_apply(h, precision, x, r, oc));
         residual_kernel<<<nb, 256, 0, h->stream>>>(n, b, r);
@@ -286,12 +291,13 @@ int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {
         for (int outer = 0; outer < 20; ++outer) {
             if (rnorm <= atol || s.iterations >= maxit) break;
             ++s.refinements;
-            // inner accuracy: enough to land below the target, not below the FP32 floor
-            const double inner_rel = std::min(0.5, std::max(0.3 * atol / rnorm, 1e-5));
+            // one inner cycle (up to `restart` FP32 iterations) aiming just below the
+            // target, never below what the FP32 operator can resolve
+            const double inner_rel = std::min(0.5, std::max(0.3 * atol / rnorm, 1e-6));
             CR_CUDA(h, cudaMemsetAsync(K.d, 0, n * sizeof(double), h->stream));
             double inner_norm = 0;
             int ist = fgmres(h, CR_FP32, K.d, K.rr, kResidualIsB, inner_rel * rnorm, maxit - s.iterations,
-                             &s.iterations, &s.restarts, &inner_norm, oc);
+                             &s.iterations, &s.restarts, &inner_norm, oc, true);
             if (ist != CR_OK && ist != CR_NOT_CONVERGED) return ist;
             axpy_kernel<<<nb, 256, 0, h->stream>>>(n, 1.0, K.d, x);
             CR_LAUNCH(h, "axpy_kernel");
