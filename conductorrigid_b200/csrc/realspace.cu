@@ -8,8 +8,8 @@
 //
 //  * clusters: beads sorted along a Morton curve of the box, cut into clusters of 32
 //    (the last one padded);
-//  * cluster pairs (I <= J) whose bounding boxes come within rc under any periodic
-//    image, found once per solve;
+//  * cluster pairs (I, J), both orders, whose bounding boxes come within rc under any
+//    periodic image, found once per solve;
 //  * per pair a 32x32 bit mask (row i, bit j) of the bead pairs with
 //    dr^2 <= d^2 < rc^2 under the minimum image (ConductorRigid.cu:536-540), and the
 //    values T(d_ij) of just those pairs, packed row by row, with the table index
@@ -17,12 +17,12 @@
 //    ConductorRigid.cu:549-554, evaluated in FP64 and stored in the operator
 //    precision (the 32x32 blocks of a 4 A cutoff are only 20-35% full, so the mask
 //    keeps the streamed bytes close to one value per interacting pair);
-//  * the product y_I += B x_J and, for I != J, y_J += B^T x_I (T(d_ij) = T(d_ji)), one
-//    warp per cluster I, lane i walking the set bits of its row, x_J and the
-//    transposed partial sums in shared memory.
+//  * the product y_I = sum_J B_IJ x_J, one warp per cluster I: each pair's packed values
+//    are staged in shared memory with coalesced loads, lane i walks the set bits of
+//    row i; the warp owns y_I, so there are no atomics and the sum order is fixed.
 //
 // The force pass (once per solve) evaluates the gradient table on the fly over the same
-// cluster pairs in FP64, with F_j -= f_ij for the mirrored half.
+// cluster pairs in FP64.
 #include <cub/cub.cuh>
 
 #include "cr_internal.cuh"
@@ -116,7 +116,7 @@ __device__ __forceinline__ double box_gap2(const double4 &ci, const double4 &ei,
     return g2;
 }
 
-// One warp per cluster I scans J >= I; FILL writes J in ascending order.
+// One warp per cluster I scans every J; FILL writes J in ascending order.
 template <bool FILL>
 __global__ void pair_search_kernel(int nclus, const double4 *__restrict__ centre, const double4 *__restrict__ extent,
                                    RSBuild c, int *count, const long long *__restrict__ head, int *pair_j) {
@@ -126,7 +126,7 @@ __global__ void pair_search_kernel(int nclus, const double4 *__restrict__ centre
     const double4 ci = centre[I], ei = extent[I];
     int n = 0;
     const long long h0 = FILL ? head[I] : 0;
-    for (int base = I; base < nclus; base += 32) {
+    for (int base = 0; base < nclus; base += 32) {
         const int J = base + lane;
         bool hit = false;
         if (J < nclus) hit = J == I || box_gap2(ci, ei, centre[J], extent[J], c) < c.rc2;
@@ -223,23 +223,25 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
     }
 }
 
-// acc[bead] += sum over the cluster pairs (both halves).  One warp per cluster I; lane
-// i walks the set bits of row i.
+// y_I = sum_J B_IJ x_J for cluster I (one warp), combined with the wave-space part and
+// the self term: out_i = Phi_body(i) - (phik_i + self q_i + y_i), or the bare sum when
+// phi_body is NULL.
 template <typename R>
 __global__ void __launch_bounds__(128) pair_spmv_kernel(int nclus, const long long *__restrict__ head,
                                                         const int *__restrict__ count, const int *__restrict__ pair_j,
                                                         const int *__restrict__ members,
                                                         const unsigned *__restrict__ masks,
                                                         const long long *__restrict__ voff,
-                                                        const R *__restrict__ vals, const R *__restrict__ q,
-                                                        R *__restrict__ acc) {
+                                                        const int *__restrict__ nnz_pair, const R *__restrict__ vals,
+                                                        const R *__restrict__ q, const R *__restrict__ phik,
+                                                        double selfc, const double *__restrict__ phi_body,
+                                                        const uint32_t *__restrict__ body, double *__restrict__ out) {
+    __shared__ R sv[4][CS * CS];
     __shared__ R xJs[4][CS];
-    __shared__ R tJ[4][CS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int I = blockIdx.x * 4 + w;
     if (I >= nclus) return;
     const int bi = members[I * CS + lane];
-    const R xI = bi >= 0 ? q[bi] : (R)0;
     R yI = 0;
     const long long h0 = head[I];
     const int n = count[I];
@@ -248,26 +250,24 @@ __global__ void __launch_bounds__(128) pair_spmv_kernel(int nclus, const long lo
         const int J = pair_j[p];
         const int bj = members[J * CS + lane];
         xJs[w][lane] = bj >= 0 ? q[bj] : (R)0;
-        tJ[w][lane] = (R)0;
-        unsigned m = masks[p * CS + lane];
-        const R *v = vals + voff[p] + warp_exclusive_scan(__popc(m), lane);
+        const unsigned m0 = masks[p * CS + lane];
+        const long long off = voff[p];
+        const int nv = nnz_pair[p];
+        for (int t = lane; t < nv; t += 32) sv[w][t] = __ldg(vals + off + t);
         __syncwarp();
-        const bool mirror = J != I;
+        unsigned m = m0;
+        int at = warp_exclusive_scan(__popc(m), lane);
         while (m) {
             const int j = __ffs(m) - 1;
             m &= m - 1;
-            const R t = __ldg(v++);
-            yI += t * xJs[w][j];
-            if (mirror) atomicAdd(&tJ[w][j], t * xI);
-        }
-        __syncwarp();
-        if (mirror && bj >= 0) {
-            const R t = tJ[w][lane];
-            if (t != (R)0) atomicAdd(acc + bj, t);
+            yI += sv[w][at++] * xJs[w][j];
         }
         __syncwarp();
     }
-    if (bi >= 0) atomicAdd(acc + bi, yI);
+    if (bi >= 0) {
+        const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)yI;
+        out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+    }
 }
 
 // out_i = Phi_body(i) - (phik_i + self q_i + acc_i)   or   phik_i + self q_i + acc_i
@@ -281,8 +281,8 @@ __global__ void combine_kernel(int N, const R *__restrict__ phik, const R *__res
     out[i] = phi_body ? phi_body[body[i]] - total : total;
 }
 
-// Real-space forces over the cluster pairs, on the fly in FP64: f_ij = -T'(d) q_i q_j
-// r_ij / d (ConductorRigid.cu:637-654), F_i += f_ij, F_j -= f_ij for I != J.
+// Real-space forces over the cluster pairs, on the fly in FP64: F_i += -T'(d) q_i q_j
+// r_ij / d (ConductorRigid.cu:637-654); every ordered pair (I, J) is in the list.
 __global__ void __launch_bounds__(128) pair_force_kernel(long long npairs, const int *__restrict__ pair_i,
                                                          const int *__restrict__ pair_j,
                                                          const int *__restrict__ members,
@@ -300,7 +300,6 @@ __global__ void __launch_bounds__(128) pair_force_kernel(long long npairs, const
     const double qi = bi >= 0 ? q[bi] : 0.0;
     const double qjl = bj >= 0 ? q[bj] : 0.0;
     double fi[3] = {0, 0, 0};
-    double fjmine[3] = {0, 0, 0};
     for (int j = 0; j < CS; ++j) {
         const int vj = __shfl_sync(0xffffffffu, bj, j);
         const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
@@ -322,18 +321,9 @@ __global__ void __launch_bounds__(128) pair_force_kernel(long long npairs, const
             }
         }
         for (int e = 0; e < 3; ++e) fi[e] += f[e];
-        if (J != I) {
-            double s[3] = {f[0], f[1], f[2]};
-            for (int e = 0; e < 3; ++e)
-                for (int o = 16; o > 0; o >>= 1) s[e] += __shfl_xor_sync(0xffffffffu, s[e], o);
-            if (lane == j)
-                for (int e = 0; e < 3; ++e) fjmine[e] = s[e];
-        }
     }
     if (bi >= 0)
         for (int e = 0; e < 3; ++e) atomicAdd(F + 3 * (size_t)bi + e, fi[e]);
-    if (J != I && bj >= 0)
-        for (int e = 0; e < 3; ++e) atomicAdd(F + 3 * (size_t)bj + e, -fjmine[e]);
 }
 
 // force_i = wave force_i + q_i E0 + real-space force_i
@@ -510,18 +500,11 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
         ProfScope pb(h, PROF_GEOMETRY);
         CR_TRY(realspace_blocks<R>(h));
     }
-    R *acc = acc_of<R>(r);
-    {
-        ProfScope ps(h, PROF_REAL);
-        CR_CUDA(h, cudaMemsetAsync(acc, 0, (size_t)N * sizeof(R), h->stream));
-        pair_spmv_kernel<R><<<(r.nclus + 3) / 4, 128, 0, h->stream>>>(r.nclus, r.head, r.count, r.pair_j, r.members,
-                                                                      r.masks, r.voff, blocks_of<R>(r), m.q, acc);
-        CR_LAUNCH(h, "pair_spmv_kernel");
-    }
-    ProfScope pc(h, PROF_BODY);
-    combine_kernel<R><<<blocks_for(N, 256), 256, 0, h->stream>>>(N, m.phi, m.q, acc, h->d.selfcoeff, phi_body,
-                                                                 h->d_body, out);
-    CR_LAUNCH(h, "combine_kernel");
+    ProfScope ps(h, PROF_REAL);
+    pair_spmv_kernel<R><<<(r.nclus + 3) / 4, 128, 0, h->stream>>>(
+        r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), m.q, m.phi,
+        h->d.selfcoeff, phi_body, h->d_body, out);
+    CR_LAUNCH(h, "pair_spmv_kernel");
     return CR_OK;
 }
 
