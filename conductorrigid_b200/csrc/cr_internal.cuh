@@ -95,7 +95,7 @@ struct RealSpace {
     double *vals64 = nullptr;
     long long blocks32_cap = 0, blocks64_cap = 0;
     bool valid32 = false, valid64 = false;
-    float *acc32 = nullptr;         // [N] product accumulators
+    float *acc32 = nullptr;         // [nclus*32] charges in cluster order
     double *acc64 = nullptr;
     double *freal = nullptr;        // [3N] real-space forces
 };

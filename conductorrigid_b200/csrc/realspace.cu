@@ -223,18 +223,32 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
     }
 }
 
+// Charges in cluster order (0 for padding), so that a warp reads a cluster's charges
+// with one coalesced load.
+template <typename R>
+__global__ void gather_cluster_kernel(int n, const int *__restrict__ members, const R *__restrict__ q,
+                                      R *__restrict__ qc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = members[k];
+    qc[k] = i >= 0 ? q[i] : (R)0;
+}
+
 // y_I = sum_J B_IJ x_J for cluster I (one warp), combined with the wave-space part and
 // the self term: out_i = Phi_body(i) - (phik_i + self q_i + y_i), or the bare sum when
-// phi_body is NULL.
-template <typename R>
+// phi_body is NULL.  Each pair's packed values are loaded U per lane at a time (all
+// independent, so they are in flight together) into shared memory; the metadata of
+// the next pair is fetched while the current one is summed.
+template <typename R, int U>
 __global__ void __launch_bounds__(128) pair_spmv_kernel(int nclus, const long long *__restrict__ head,
                                                         const int *__restrict__ count, const int *__restrict__ pair_j,
                                                         const int *__restrict__ members,
                                                         const unsigned *__restrict__ masks,
                                                         const long long *__restrict__ voff,
                                                         const int *__restrict__ nnz_pair, const R *__restrict__ vals,
-                                                        const R *__restrict__ q, const R *__restrict__ phik,
-                                                        double selfc, const double *__restrict__ phi_body,
+                                                        const R *__restrict__ qc, const R *__restrict__ q,
+                                                        const R *__restrict__ phik, double selfc,
+                                                        const double *__restrict__ phi_body,
                                                         const uint32_t *__restrict__ body, double *__restrict__ out) {
     __shared__ R sv[4][CS * CS];
     __shared__ R xJs[4][CS];
@@ -245,17 +259,45 @@ __global__ void __launch_bounds__(128) pair_spmv_kernel(int nclus, const long lo
     R yI = 0;
     const long long h0 = head[I];
     const int n = count[I];
+    // metadata of the current pair
+    int J = 0, nv = 0;
+    unsigned m0 = 0;
+    long long off = 0;
+    R xJ = 0;
+    if (n > 0) {
+        J = pair_j[h0];
+        m0 = masks[h0 * CS + lane];
+        off = voff[h0];
+        nv = nnz_pair[h0];
+        xJ = qc[J * CS + lane];
+    }
     for (int k = 0; k < n; ++k) {
-        const long long p = h0 + k;
-        const int J = pair_j[p];
-        const int bj = members[J * CS + lane];
-        xJs[w][lane] = bj >= 0 ? q[bj] : (R)0;
-        const unsigned m0 = masks[p * CS + lane];
-        const long long off = voff[p];
-        const int nv = nnz_pair[p];
-        for (int t = lane; t < nv; t += 32) sv[w][t] = __ldg(vals + off + t);
+        for (int base = 0; base < nv; base += 32 * U) {
+            R tmp[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int t = base + lane + 32 * u;
+                tmp[u] = t < nv ? __ldg(vals + off + t) : (R)0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int t = base + lane + 32 * u;
+                if (t < nv) sv[w][t] = tmp[u];
+            }
+        }
+        xJs[w][lane] = xJ;
+        const unsigned mcur = m0;
+        // prefetch the next pair's metadata
+        if (k + 1 < n) {
+            const long long p1 = h0 + k + 1;
+            J = pair_j[p1];
+            m0 = masks[p1 * CS + lane];
+            off = voff[p1];
+            nv = nnz_pair[p1];
+            xJ = qc[J * CS + lane];
+        }
         __syncwarp();
-        unsigned m = m0;
+        unsigned m = mcur;
         int at = warp_exclusive_scan(__popc(m), lane);
         while (m) {
             const int j = __ffs(m) - 1;
@@ -268,17 +310,6 @@ __global__ void __launch_bounds__(128) pair_spmv_kernel(int nclus, const long lo
         const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)yI;
         out[bi] = phi_body ? phi_body[body[bi]] - total : total;
     }
-}
-
-// out_i = Phi_body(i) - (phik_i + self q_i + acc_i)   or   phik_i + self q_i + acc_i
-template <typename R>
-__global__ void combine_kernel(int N, const R *__restrict__ phik, const R *__restrict__ q, const R *__restrict__ acc,
-                               double selfc, const double *__restrict__ phi_body, const uint32_t *__restrict__ body,
-                               double *__restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const double total = (double)phik[i] + selfc * (double)q[i] + (double)acc[i];
-    out[i] = phi_body ? phi_body[body[i]] - total : total;
 }
 
 // Real-space forces over the cluster pairs, on the fly in FP64: F_i += -T'(d) q_i q_j
@@ -421,8 +452,8 @@ int realspace_alloc(cr_handle *h) {
     CR_TRY(dalloc(h, &r.count, nc));
     CR_TRY(dalloc(h, &r.head, nc));
     CR_TRY(dalloc(h, &r.sorted, (size_t)std::max(h->N, 1)));
-    CR_TRY(dalloc(h, &r.acc32, (size_t)std::max(h->N, 1)));
-    CR_TRY(dalloc(h, &r.acc64, (size_t)std::max(h->N, 1)));
+    CR_TRY(dalloc(h, &r.acc32, nc * CS));
+    CR_TRY(dalloc(h, &r.acc64, nc * CS));
     CR_TRY(dalloc(h, &r.freal, 3 * (size_t)std::max(h->N, 1)));
     return CR_OK;
 }
@@ -501,8 +532,12 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
         CR_TRY(realspace_blocks<R>(h));
     }
     ProfScope ps(h, PROF_REAL);
-    pair_spmv_kernel<R><<<(r.nclus + 3) / 4, 128, 0, h->stream>>>(
-        r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), m.q, m.phi,
+    R *qc = acc_of<R>(r);
+    gather_cluster_kernel<R><<<blocks_for((long)r.nclus * CS, 256), 256, 0, h->stream>>>(r.nclus * CS, r.members,
+                                                                                         m.q, qc);
+    CR_LAUNCH(h, "gather_cluster_kernel");
+    pair_spmv_kernel<R, 8><<<(r.nclus + 3) / 4, 128, 0, h->stream>>>(
+        r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, m.phi,
         h->d.selfcoeff, phi_body, h->d_body, out);
     CR_LAUNCH(h, "pair_spmv_kernel");
     return CR_OK;
