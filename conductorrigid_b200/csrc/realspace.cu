@@ -234,44 +234,47 @@ __global__ void gather_cluster_kernel(int n, const int *__restrict__ members, co
     qc[k] = i >= 0 ? q[i] : (R)0;
 }
 
-// y_I = sum_J B_IJ x_J for cluster I (one warp), combined with the wave-space part and
-// the self term: out_i = Phi_body(i) - (phik_i + self q_i + y_i), or the bare sum when
-// phi_body is NULL.  Each pair's packed values are loaded U per lane at a time (all
-// independent, so they are in flight together) into shared memory; the metadata of
-// the next pair is fetched while the current one is summed.
-template <typename R, int U>
-__global__ void __launch_bounds__(128) pair_spmv_kernel(int nclus, const long long *__restrict__ head,
-                                                        const int *__restrict__ count, const int *__restrict__ pair_j,
-                                                        const int *__restrict__ members,
-                                                        const unsigned *__restrict__ masks,
-                                                        const long long *__restrict__ voff,
-                                                        const int *__restrict__ nnz_pair, const R *__restrict__ vals,
-                                                        const R *__restrict__ qc, const R *__restrict__ q,
-                                                        const R *__restrict__ phik, double selfc,
-                                                        const double *__restrict__ phi_body,
-                                                        const uint32_t *__restrict__ body, double *__restrict__ out) {
-    __shared__ R sv[4][CS * CS];
-    __shared__ R xJs[4][CS];
+// y_I = sum_J B_IJ x_J for cluster I (one CTA of W warps), combined with the wave-space
+// part and the self term: out_i = Phi_body(i) - (phik_i + self q_i + y_i), or the bare
+// sum when phi_body is NULL.  Warp w takes pairs w, w+W, ...: each pair's packed values
+// are loaded U per lane at a time (independent loads, in flight together) into the
+// warp's shared-memory slice, and the next pair's metadata is fetched while the current
+// one is summed.  The W partial sums are added in warp order, so the result does not
+// depend on scheduling.
+template <typename R, int W, int U>
+__global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long long *__restrict__ head,
+                                                           const int *__restrict__ count,
+                                                           const int *__restrict__ pair_j,
+                                                           const int *__restrict__ members,
+                                                           const unsigned *__restrict__ masks,
+                                                           const long long *__restrict__ voff,
+                                                           const int *__restrict__ nnz_pair,
+                                                           const R *__restrict__ vals, const R *__restrict__ qc,
+                                                           const R *__restrict__ q, const R *__restrict__ phik,
+                                                           double selfc, const double *__restrict__ phi_body,
+                                                           const uint32_t *__restrict__ body,
+                                                           double *__restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *sv = reinterpret_cast<R *>(smem_raw) + (threadIdx.x >> 5) * (CS * CS);
+    R *xJs = reinterpret_cast<R *>(smem_raw) + W * CS * CS + (threadIdx.x >> 5) * CS;
+    R *part = reinterpret_cast<R *>(smem_raw) + W * CS * CS + W * CS;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int I = blockIdx.x * 4 + w;
-    if (I >= nclus) return;
-    const int bi = members[I * CS + lane];
+    const int I = blockIdx.x;
     R yI = 0;
     const long long h0 = head[I];
     const int n = count[I];
-    // metadata of the current pair
     int J = 0, nv = 0;
     unsigned m0 = 0;
     long long off = 0;
     R xJ = 0;
-    if (n > 0) {
-        J = pair_j[h0];
-        m0 = masks[h0 * CS + lane];
-        off = voff[h0];
-        nv = nnz_pair[h0];
+    if (w < n) {
+        J = pair_j[h0 + w];
+        m0 = masks[(h0 + w) * CS + lane];
+        off = voff[h0 + w];
+        nv = nnz_pair[h0 + w];
         xJ = qc[J * CS + lane];
     }
-    for (int k = 0; k < n; ++k) {
+    for (int k = w; k < n; k += W) {
         for (int base = 0; base < nv; base += 32 * U) {
             R tmp[U];
 #pragma unroll
@@ -282,14 +285,13 @@ __global__ void __launch_bounds__(128) pair_spmv_kernel(int nclus, const long lo
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int t = base + lane + 32 * u;
-                if (t < nv) sv[w][t] = tmp[u];
+                if (t < nv) sv[t] = tmp[u];
             }
         }
-        xJs[w][lane] = xJ;
+        xJs[lane] = xJ;
         const unsigned mcur = m0;
-        // prefetch the next pair's metadata
-        if (k + 1 < n) {
-            const long long p1 = h0 + k + 1;
+        if (k + W < n) {
+            const long long p1 = h0 + k + W;
             J = pair_j[p1];
             m0 = masks[p1 * CS + lane];
             off = voff[p1];
@@ -302,15 +304,26 @@ __global__ void __launch_bounds__(128) pair_spmv_kernel(int nclus, const long lo
         while (m) {
             const int j = __ffs(m) - 1;
             m &= m - 1;
-            yI += sv[w][at++] * xJs[w][j];
+            yI += sv[at++] * xJs[j];
         }
         __syncwarp();
     }
-    if (bi >= 0) {
-        const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)yI;
-        out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+    part[w * CS + lane] = yI;
+    __syncthreads();
+    if (w == 0) {
+        R tot = 0;
+#pragma unroll
+        for (int v = 0; v < W; ++v) tot += part[v * CS + lane];
+        const int bi = members[I * CS + lane];
+        if (bi >= 0) {
+            const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)tot;
+            out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+        }
     }
 }
+
+template <typename R, int W> constexpr size_t spmv_smem() { return (size_t)(W * CS * CS + 2 * W * CS) * sizeof(R); }
+constexpr int kSpmvWarps = 8;
 
 // Real-space forces over the cluster pairs, on the fly in FP64: F_i += -T'(d) q_i q_j
 // r_ij / d (ConductorRigid.cu:637-654); every ordered pair (I, J) is in the list.
@@ -444,6 +457,12 @@ void realspace_free(cr_handle *h) {
 int realspace_alloc(cr_handle *h) {
     RealSpace &r = h->rs;
     realspace_free(h);
+    CR_CUDA(h, cudaFuncSetAttribute(pair_spmv_kernel<float, kSpmvWarps, 8>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)spmv_smem<float, kSpmvWarps>()));
+    CR_CUDA(h, cudaFuncSetAttribute(pair_spmv_kernel<double, kSpmvWarps, 8>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)spmv_smem<double, kSpmvWarps>()));
     r.nclus = (h->N + CS - 1) / CS;
     const size_t nc = (size_t)std::max(r.nclus, 1);
     CR_TRY(dalloc(h, &r.members, nc * CS));
@@ -536,7 +555,8 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
     gather_cluster_kernel<R><<<blocks_for((long)r.nclus * CS, 256), 256, 0, h->stream>>>(r.nclus * CS, r.members,
                                                                                          m.q, qc);
     CR_LAUNCH(h, "gather_cluster_kernel");
-    pair_spmv_kernel<R, 8><<<(r.nclus + 3) / 4, 128, 0, h->stream>>>(
+    constexpr int W = kSpmvWarps;
+    pair_spmv_kernel<R, W, 8><<<r.nclus, W * 32, spmv_smem<R, W>(), h->stream>>>(
         r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, m.phi,
         h->d.selfcoeff, phi_body, h->d_body, out);
     CR_LAUNCH(h, "pair_spmv_kernel");
