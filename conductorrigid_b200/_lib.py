@@ -148,6 +148,8 @@ _SIGS = {
     "cr_profile_read": ([_P, _I, C.POINTER(C.c_int), C.POINTER(C.c_double)], _I),
     "cr_counters": ([_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], _I),
     "cr_get_geometry_info": ([_P, C.POINTER(CrGeometryInfo)], _I),
+    "cr_spread_noalloc": ([C.POINTER(CrDerived), C.c_double, _D, _I, _P, _P, _P, _P], _I),
+    "cr_noalloc_last_error": ([], C.c_char_p),
     "cr_util_icosphere_count": ([_I], _I),
     "cr_util_icosphere": ([_I, _D], _I),
     "cr_util_place_spheres": ([_I, _D, _D, C.c_uint64, C.c_int64, _D], _I),

@@ -195,6 +195,29 @@ int cr_get_geometry_info(const cr_handle *h, cr_geometry_info *out);
 /* Kernels of this library launched through the handle, and cuFFT executions. */
 int cr_counters(const cr_handle *h, long long *kernel_launches, long long *fft_execs);
 
+/* ---- spreading without device allocation ----
+ * No counterpart in the reference.  For callers that cannot allocate device memory
+ * where they need the charge mesh: a host engine that owns all device memory through
+ * its own pool, or a time-step loop in which cudaMalloc/cudaFree would synchronise the
+ * device while other streams run.  Same result as cr_spread in FP64 (ConductorRigid.cu
+ * spreading rule) for derived parameters d (from cr_derive_params / cr_get_derived),
+ * Ewald parameter xi and box L; device arrays d_pos[n_beads*3], d_q[n_beads] in,
+ * d_grid[Nx*Ny*Nz] out (overwritten).  It allocates nothing: its scratch is one
+ * file-scope device array of CR_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library holds until exit, located per device with cudaGetSymbolAddress on the first
+ * call on that device (make that first call before any stream capture).  At most
+ * CR_NOALLOC_MAX_BEADS beads, CR_NOALLOC_MAX_TILES 8^3-node mesh tiles and support 16;
+ * larger inputs are rejected with CR_BAD_PARAM and a message in
+ * cr_noalloc_last_error().  All calls share the array, so calls that overlap on the GPU
+ * race and must be serialised by the caller.  Synchronises `stream` before returning. */
+#define CR_NOALLOC_MAX_BEADS 262144
+#define CR_NOALLOC_MAX_TILES 32768
+#define CR_NOALLOC_SCRATCH_BYTES 6291456
+int cr_spread_noalloc(const cr_derived *d, double xi, const double L[3], int n_beads, const double *d_pos,
+                      const double *d_q, double *d_grid, void *stream);
+/* Message of the last cr_spread_noalloc failure on the calling thread ("" if none). */
+const char *cr_noalloc_last_error(void);
+
 /* ---- synthetic systems (host utilities for the benchmark workloads) ---- */
 int cr_util_icosphere_count(int level);
 int cr_util_icosphere(int level, double *verts);
