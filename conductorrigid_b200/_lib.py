@@ -106,6 +106,7 @@ class CrGeometryInfo(C.Structure):
         ("n_beads", C.c_int),
         ("n_bodies", C.c_int),
         ("cluster_pairs", C.c_int64),
+        ("stored_values", C.c_int64),
     ]
 
 

@@ -423,6 +423,7 @@ int cr_get_geometry_info(const cr_handle *h, cr_geometry_info *out) {
     out->n_beads = h->N;
     out->n_bodies = h->B;
     out->cluster_pairs = h->geo.valid ? h->rs.npairs : 0;
+    out->stored_values = h->geo.valid ? h->rs.nnz : 0;
     return CR_OK;
 }
 

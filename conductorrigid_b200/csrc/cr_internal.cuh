@@ -90,7 +90,9 @@ struct RealSpace {
     unsigned *masks = nullptr;      // [npairs*32] row bit masks of in-range bead pairs
     int *nnz_pair = nullptr;        // [npairs] set bits per pair
     long long *voff = nullptr;      // [npairs] first packed value of each pair
-    long long nnz = 0;              // stored values
+    long long nnz = 0;              // stored value slots (rows padded to each pair's longest row)
+    long long npairs_beads = 0;     // interacting directed bead pairs (set mask bits)
+    unsigned long long *bits = nullptr;
     float *vals32 = nullptr;        // [nnz] packed T(d) values
     double *vals64 = nullptr;
     long long blocks32_cap = 0, blocks64_cap = 0;

@@ -12,14 +12,18 @@
 //    periodic image, found once per solve;
 //  * per pair a 32x32 bit mask (row i, bit j) of the bead pairs with
 //    dr^2 <= d^2 < rc^2 under the minimum image (ConductorRigid.cu:536-540), and the
-//    values T(d_ij) of just those pairs, packed row by row, with the table index
+//    values T(d_ij) of just those pairs with the table index
 //    floor(Ntable (d - dr)/(rc - dr)) and linear weight d/dr - index - 1 of
 //    ConductorRigid.cu:549-554, evaluated in FP64 and stored in the operator
-//    precision (the 32x32 blocks of a 4 A cutoff are only 20-35% full, so the mask
-//    keeps the streamed bytes close to one value per interacting pair);
-//  * the product y_I = sum_J B_IJ x_J, one warp per cluster I: each pair's packed values
-//    are staged in shared memory with coalesced loads, lane i walks the set bits of
-//    row i; the warp owns y_I, so there are no atomics and the sum order is fixed.
+//    precision (the 32x32 blocks of a 4-unit cutoff are only 20-35% full, so the mask
+//    keeps the streamed bytes near one value per interacting pair).  The values of a
+//    pair are stored lane-interleaved: the k-th value of row i at k*32 + i, rows padded
+//    with zeros to the pair's longest row, so that every load is one coalesced warp
+//    load;
+//  * the product y_I = sum_J B_IJ x_J, the pairs of cluster I split over the warps of
+//    one CTA: lane i takes the k-th set bit j of its row, multiplies the k-th value by
+//    x_J[j] fetched with a warp shuffle; the partial sums are added in warp order, so
+//    there are no atomics and the sum order is fixed.
 //
 // The force pass (once per solve) evaluates the gradient table on the fly over the same
 // cluster pairs in FP64.
@@ -153,10 +157,11 @@ __device__ __forceinline__ double table_lerp64(const double2 *__restrict__ tab, 
 }
 
 // Bit masks of the in-range bead pairs of every cluster pair (row i = bead i of I,
-// bit j = bead j of J) and the number of set bits per pair.
+// bit j = bead j of J) and the stored slots of the pair (32 x its longest row).
 __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
                                  const int *__restrict__ members, const double4 *__restrict__ pos, RSBuild c,
-                                 unsigned *__restrict__ masks, int *__restrict__ nnz) {
+                                 unsigned *__restrict__ masks, int *__restrict__ nnz,
+                                 unsigned long long *__restrict__ bits) {
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (p >= npairs) return;
@@ -180,9 +185,15 @@ __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_
         }
     }
     masks[p * CS + lane] = m;
-    int n = __popc(m);
-    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-    if (lane == 0) nnz[p] = n;
+    int n = __popc(m), tot = n;
+    for (int o = 16; o > 0; o >>= 1) {
+        n = max(n, __shfl_xor_sync(0xffffffffu, n, o));
+        tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    if (lane == 0) {
+        nnz[p] = n * CS;  // stored slots: longest row times 32 lanes
+        atomicAdd(bits, (unsigned long long)tot);
+    }
 }
 
 __device__ __forceinline__ int warp_exclusive_scan(int v, int lane) {
@@ -194,12 +205,14 @@ __device__ __forceinline__ int warp_exclusive_scan(int v, int lane) {
     return incl - v;
 }
 
-// Packed values T(d_ij) of the set mask bits, row by row, in the operator precision.
+// Values T(d_ij) of the set mask bits in the operator precision, lane-interleaved:
+// the k-th set bit of row i at voff + k*32 + i, zeros after the row's last bit.
 template <typename R>
 __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
                                    const int *__restrict__ members, const double4 *__restrict__ pos,
                                    const double2 *__restrict__ tab, RSBuild c, const unsigned *__restrict__ masks,
-                                   const long long *__restrict__ voff, R *__restrict__ vals) {
+                                   const long long *__restrict__ voff, const int *__restrict__ slots,
+                                   R *__restrict__ vals) {
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (p >= npairs) return;
@@ -209,7 +222,8 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
     const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
     const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
     const unsigned m = masks[p * CS + lane];
-    long long at = voff[p] + warp_exclusive_scan(__popc(m), lane);
+    R *out = vals + voff[p] + lane;
+    int k = 0;
     for (int j = 0; j < CS; ++j) {
         const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
         const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
@@ -218,9 +232,12 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
             const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
             const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
             const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
-            vals[at++] = (R)table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
+            out[(size_t)k * CS] = (R)table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
+            ++k;
         }
     }
+    const int rows = slots[p] / CS;
+    for (; k < rows; ++k) out[(size_t)k * CS] = (R)0;
 }
 
 // Charges in cluster order (0 for padding), so that a warp reads a cluster's charges
@@ -236,11 +253,11 @@ __global__ void gather_cluster_kernel(int n, const int *__restrict__ members, co
 
 // y_I = sum_J B_IJ x_J for cluster I (one CTA of W warps), combined with the wave-space
 // part and the self term: out_i = Phi_body(i) - (phik_i + self q_i + y_i), or the bare
-// sum when phi_body is NULL.  Warp w takes pairs w, w+W, ...: each pair's packed values
-// are loaded U per lane at a time (independent loads, in flight together) into the
-// warp's shared-memory slice, and the next pair's metadata is fetched while the current
-// one is summed.  The W partial sums are added in warp order, so the result does not
-// depend on scheduling.
+// sum when phi_body is NULL.  Warp w takes pairs w, w+W, ...; lane i consumes the set
+// bits of its mask row in order, the k-th against the coalesced load of slot k, with
+// x_J[j] from a shuffle.  Up to U slots are loaded before they are used; the next
+// pair's metadata is fetched while the current one is summed.  The W partial sums are
+// added in warp order, so the result does not depend on scheduling.
 template <typename R, int W, int U>
 __global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long long *__restrict__ head,
                                                            const int *__restrict__ count,
@@ -248,22 +265,19 @@ __global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long
                                                            const int *__restrict__ members,
                                                            const unsigned *__restrict__ masks,
                                                            const long long *__restrict__ voff,
-                                                           const int *__restrict__ nnz_pair,
+                                                           const int *__restrict__ slots,
                                                            const R *__restrict__ vals, const R *__restrict__ qc,
                                                            const R *__restrict__ q, const R *__restrict__ phik,
                                                            double selfc, const double *__restrict__ phi_body,
                                                            const uint32_t *__restrict__ body,
                                                            double *__restrict__ out) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R *sv = reinterpret_cast<R *>(smem_raw) + (threadIdx.x >> 5) * (CS * CS);
-    R *xJs = reinterpret_cast<R *>(smem_raw) + W * CS * CS + (threadIdx.x >> 5) * CS;
-    R *part = reinterpret_cast<R *>(smem_raw) + W * CS * CS + W * CS;
+    __shared__ R part[W][CS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int I = blockIdx.x;
     R yI = 0;
     const long long h0 = head[I];
     const int n = count[I];
-    int J = 0, nv = 0;
+    int J = 0, rows = 0;
     unsigned m0 = 0;
     long long off = 0;
     R xJ = 0;
@@ -271,49 +285,40 @@ __global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long
         J = pair_j[h0 + w];
         m0 = masks[(h0 + w) * CS + lane];
         off = voff[h0 + w];
-        nv = nnz_pair[h0 + w];
+        rows = slots[h0 + w] / CS;
         xJ = qc[J * CS + lane];
     }
     for (int k = w; k < n; k += W) {
-        for (int base = 0; base < nv; base += 32 * U) {
-            R tmp[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int t = base + lane + 32 * u;
-                tmp[u] = t < nv ? __ldg(vals + off + t) : (R)0;
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int t = base + lane + 32 * u;
-                if (t < nv) sv[t] = tmp[u];
-            }
-        }
-        xJs[lane] = xJ;
-        const unsigned mcur = m0;
+        const R *v = vals + off + lane;
+        unsigned m = m0;
+        const R xcur = xJ;
+        const int rcur = rows;
         if (k + W < n) {
             const long long p1 = h0 + k + W;
             J = pair_j[p1];
             m0 = masks[p1 * CS + lane];
             off = voff[p1];
-            nv = nnz_pair[p1];
+            rows = slots[p1] / CS;
             xJ = qc[J * CS + lane];
         }
-        __syncwarp();
-        unsigned m = mcur;
-        int at = warp_exclusive_scan(__popc(m), lane);
-        while (m) {
-            const int j = __ffs(m) - 1;
-            m &= m - 1;
-            yI += sv[at++] * xJs[j];
+        for (int base = 0; base < rcur; base += U) {
+            R t[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) t[u] = base + u < rcur ? __ldg(v + (size_t)(base + u) * CS) : (R)0;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = m ? __ffs(m) - 1 : 0;
+                m &= m - 1;
+                yI += t[u] * __shfl_sync(0xffffffffu, xcur, j);
+            }
         }
-        __syncwarp();
     }
-    part[w * CS + lane] = yI;
+    part[w][lane] = yI;
     __syncthreads();
     if (w == 0) {
         R tot = 0;
 #pragma unroll
-        for (int v = 0; v < W; ++v) tot += part[v * CS + lane];
+        for (int v = 0; v < W; ++v) tot += part[v][lane];
         const int bi = members[I * CS + lane];
         if (bi >= 0) {
             const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)tot;
@@ -322,7 +327,6 @@ __global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long
     }
 }
 
-template <typename R, int W> constexpr size_t spmv_smem() { return (size_t)(W * CS * CS + 2 * W * CS) * sizeof(R); }
 constexpr int kSpmvWarps = 8;
 
 // Real-space forces over the cluster pairs, on the fly in FP64: F_i += -T'(d) q_i q_j
@@ -421,7 +425,7 @@ template <typename R> int realspace_blocks(cr_handle *h) {
         cap_of<R>(r) = cap;
     }
     pair_values_kernel<R><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
-        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.voff,
+        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.voff, r.nnz_pair,
         blocks_of<R>(r));
     CR_LAUNCH(h, "pair_values_kernel");
     valid_of<R>(r) = true;
@@ -447,6 +451,7 @@ void realspace_free(cr_handle *h) {
     dfree(&r.acc32);
     dfree(&r.acc64);
     dfree(&r.freal);
+    dfree(&r.bits);
     r.pair_cap = 0;
     r.nnz = 0;
     r.blocks32_cap = r.blocks64_cap = 0;
@@ -457,12 +462,7 @@ void realspace_free(cr_handle *h) {
 int realspace_alloc(cr_handle *h) {
     RealSpace &r = h->rs;
     realspace_free(h);
-    CR_CUDA(h, cudaFuncSetAttribute(pair_spmv_kernel<float, kSpmvWarps, 8>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)spmv_smem<float, kSpmvWarps>()));
-    CR_CUDA(h, cudaFuncSetAttribute(pair_spmv_kernel<double, kSpmvWarps, 8>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)spmv_smem<double, kSpmvWarps>()));
+
     r.nclus = (h->N + CS - 1) / CS;
     const size_t nc = (size_t)std::max(r.nclus, 1);
     CR_TRY(dalloc(h, &r.members, nc * CS));
@@ -474,6 +474,7 @@ int realspace_alloc(cr_handle *h) {
     CR_TRY(dalloc(h, &r.acc32, nc * CS));
     CR_TRY(dalloc(h, &r.acc64, nc * CS));
     CR_TRY(dalloc(h, &r.freal, 3 * (size_t)std::max(h->N, 1)));
+    CR_TRY(dalloc(h, &r.bits, 1));
     return CR_OK;
 }
 
@@ -527,18 +528,23 @@ int realspace_build(cr_handle *h) {
     pair_owner_kernel<<<r.nclus, 128, 0, s>>>(r.nclus, r.head, r.count, r.pair_i);
     CR_LAUNCH(h, "pair_owner_kernel");
     const int pb = blocks_for(r.npairs * 32, 256);
-    pair_mask_kernel<<<pb, 256, 0, s>>>(r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, c, r.masks, r.nnz_pair);
+    CR_CUDA(h, cudaMemsetAsync(r.bits, 0, sizeof(unsigned long long), s));
+    pair_mask_kernel<<<pb, 256, 0, s>>>(r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, c, r.masks, r.nnz_pair,
+                                        r.bits);
     CR_LAUNCH(h, "pair_mask_kernel");
     bytes = h->sort_tmp_bytes;
     CR_CUDA(h, cub::DeviceScan::ExclusiveSum(h->d_sort_tmp, bytes, r.nnz_pair, r.voff, (int)r.npairs, s));
     long long last_off = 0;
     int last_nnz = 0;
+    unsigned long long nbits = 0;
+    CR_CUDA(h, cudaMemcpyAsync(&nbits, r.bits, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     CR_CUDA(h, cudaMemcpyAsync(&last_off, r.voff + r.npairs - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
     CR_CUDA(h, cudaMemcpyAsync(&last_nnz, r.nnz_pair + r.npairs - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     CR_CUDA(h, cudaStreamSynchronize(s));
     r.nnz = last_off + last_nnz;
-    // stored values the real-space product streams per application
-    h->geo.nl_total = r.nnz;
+    r.npairs_beads = (long long)nbits;
+    // interacting (directed) bead pairs of one real-space application
+    h->geo.nl_total = r.npairs_beads;
     return CR_OK;
 }
 
@@ -556,7 +562,7 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
                                                                                          m.q, qc);
     CR_LAUNCH(h, "gather_cluster_kernel");
     constexpr int W = kSpmvWarps;
-    pair_spmv_kernel<R, W, 8><<<r.nclus, W * 32, spmv_smem<R, W>(), h->stream>>>(
+    pair_spmv_kernel<R, W, 4><<<r.nclus, W * 32, 0, h->stream>>>(
         r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, m.phi,
         h->d.selfcoeff, phi_body, h->d_body, out);
     CR_LAUNCH(h, "pair_spmv_kernel");

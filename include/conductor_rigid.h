@@ -185,11 +185,12 @@ int cr_profile(cr_handle *h, int enable);   /* enable/disable; also resets the r
 int cr_profile_read(cr_handle *h, int kernel_class, int *launches, double *total_ms);
 /* Sizes of the current per-solve geometry (for traffic and roofline arithmetic). */
 typedef struct {
-    int64_t real_space_pairs;  /* bead-pair values the real-space product streams per application */
+    int64_t real_space_pairs;  /* interacting directed bead pairs of one real-space application */
     int tile_edge;             /* spread/contract tile edge in mesh nodes */
     int n_tiles;               /* mesh tiles */
     int n_beads, n_bodies;
     int64_t cluster_pairs;     /* 32-bead cluster pairs (each with a 128-byte bit mask) */
+    int64_t stored_values;     /* value slots stored for them (rows padded per pair) */
 } cr_geometry_info;
 int cr_get_geometry_info(const cr_handle *h, cr_geometry_info *out);
 /* Kernels of this library launched through the handle, and cuFFT executions. */
