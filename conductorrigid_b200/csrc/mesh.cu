@@ -17,6 +17,8 @@
 // ConductorRigid.cu:219-223), then sweep the P^2 (y,z) columns with the x loop inside.
 #include <cub/cub.cuh>
 
+#include <type_traits>
+
 #include "cr_internal.cuh"
 
 namespace cr {
@@ -68,14 +70,23 @@ __device__ __forceinline__ void window_factors(const WindowConst<R> &wc, int P, 
     }
 }
 
-template <typename R>
+// Index of mesh node g (tile origin + buffer offset, g >= 0) folded into [0, n).
+__device__ __forceinline__ int fold(int g, int n) {
+    while (g >= n) g -= n;
+    return g;
+}
+
+// PT > 0: support and tile fixed at compile time (T = 8); PT == 0: runtime values.
+template <typename R, int PT>
 __global__ void __launch_bounds__(256) spread_tiles_kernel(
     const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
     const int *__restrict__ tile_start, const int *__restrict__ tile_beads, MeshShape ms, WindowConst<R> wc,
     R prefac, R *__restrict__ grid) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *buf = reinterpret_cast<R *>(smem_raw);
-    const int Bd = ms.Bd, P = ms.P, T = ms.T;
+    const int P = PT ? PT : ms.P;
+    const int T = PT ? 8 : ms.T;
+    const int Bd = PT ? 8 + PT - 1 : ms.Bd;
     const int nbuf = Bd * Bd * Bd;
     const int tile = blockIdx.x;
     const int b0 = tile_start[tile], b1 = tile_start[tile + 1];
@@ -110,21 +121,23 @@ __global__ void __launch_bounds__(256) spread_tiles_kernel(
         const R v = buf[n];
         if (v == (R)0) continue;
         const int bz = n % Bd, by = (n / Bd) % Bd, bx = n / (Bd * Bd);
-        const int gx = (tx * T + bx) % ms.Ng[0];
-        const int gy = (ty * T + by) % ms.Ng[1];
-        const int gz = (tz * T + bz) % ms.Ng[2];
+        const int gx = fold(tx * T + bx, ms.Ng[0]);
+        const int gy = fold(ty * T + by, ms.Ng[1]);
+        const int gz = fold(tz * T + bz, ms.Ng[2]);
         atomicAdd(grid + ((size_t)gx * ms.Ng[1] + gy) * ms.Ng[2] + gz, v);
     }
 }
 
-template <typename R, bool FORCE>
+template <typename R, bool FORCE, int PT>
 __global__ void __launch_bounds__(256) contract_tiles_kernel(
     const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
     const int *__restrict__ tile_start, const int *__restrict__ tile_beads, MeshShape ms, WindowConst<R> wc,
     R coeff, const R *__restrict__ grid, R *__restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *buf = reinterpret_cast<R *>(smem_raw);
-    const int Bd = ms.Bd, P = ms.P, T = ms.T;
+    const int P = PT ? PT : ms.P;
+    const int T = PT ? 8 : ms.T;
+    const int Bd = PT ? 8 + PT - 1 : ms.Bd;
     const int nbuf = Bd * Bd * Bd;
     const int tile = blockIdx.x;
     const int b0 = tile_start[tile], b1 = tile_start[tile + 1];
@@ -135,9 +148,9 @@ __global__ void __launch_bounds__(256) contract_tiles_kernel(
     const int tz = tile % ms.ntd[2], ty = (tile / ms.ntd[2]) % ms.ntd[1], tx = tile / (ms.ntd[2] * ms.ntd[1]);
     for (int n = threadIdx.x; n < nbuf; n += blockDim.x) {
         const int bz = n % Bd, by = (n / Bd) % Bd, bx = n / (Bd * Bd);
-        const int gx = (tx * T + bx) % ms.Ng[0];
-        const int gy = (ty * T + by) % ms.Ng[1];
-        const int gz = (tz * T + bz) % ms.Ng[2];
+        const int gx = fold(tx * T + bx, ms.Ng[0]);
+        const int gy = fold(ty * T + by, ms.Ng[1]);
+        const int gz = fold(tz * T + bz, ms.Ng[2]);
         buf[n] = grid[((size_t)gx * ms.Ng[1] + gy) * ms.Ng[2] + gz];
     }
     __syncthreads();
@@ -264,6 +277,22 @@ template <typename R> size_t contract_smem(const cr_handle *h) {
     return ((size_t)Bd * Bd * Bd + 8 * 6 * (size_t)h->d.support) * sizeof(R);
 }
 
+template <typename R, int PT> int set_smem_attrs(cr_handle *h, size_t s1, size_t s2) {
+    CR_CUDA(h, cudaFuncSetAttribute(spread_tiles_kernel<R, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+    CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, false, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)s2));
+    CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, true, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)s2));
+    return CR_OK;
+}
+
+// Compile-time support for the common supports (tile edge 8), runtime otherwise.
+template <typename R, typename F> int with_support(const cr_handle *h, F f) {
+    if (h->tile == 8 && h->d.support == 9) return f(std::integral_constant<int, 9>());
+    if (h->tile == 8 && h->d.support == 11) return f(std::integral_constant<int, 11>());
+    return f(std::integral_constant<int, 0>());
+}
+
 }  // namespace
 
 template <typename R> int mesh_init(cr_handle *h, MeshBuffers<R> &m) {
@@ -301,11 +330,10 @@ template <typename R> int mesh_init(cr_handle *h, MeshBuffers<R> &m) {
     size_t s1 = spread_smem<R>(h), s2 = contract_smem<R>(h);
     if (s1 > 227 * 1024 || s2 > 227 * 1024)
         return fail(h, CR_BAD_PARAM, "support too large for the shared-memory tile buffer");
-    CR_CUDA(h, cudaFuncSetAttribute(spread_tiles_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
-    CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)s2));
-    CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)s2));
+    int st = set_smem_attrs<R, 0>(h, s1, s2);
+    if (st == CR_OK) st = set_smem_attrs<R, 9>(h, s1, s2);
+    if (st == CR_OK) st = set_smem_attrs<R, 11>(h, s1, s2);
+    if (st != CR_OK) return st;
     CR_CUDA(h, cudaDeviceSynchronize());
     m.ready = true;
     (void)sizeof(R4);
@@ -351,10 +379,13 @@ template <typename R> int spread_only(cr_handle *h, MeshBuffers<R> &m) {
     ProfScope ps(h, PROF_SPREAD);
     const long G = grid_size(h);
     CR_CUDA(h, cudaMemsetAsync(m.grid, 0, G * sizeof(R), h->stream));
-    spread_tiles_kernel<R><<<h->ntiles, 256, spread_smem<R>(h), h->stream>>>(
-        m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
-        (R)h->d.prefac, m.grid);
-    CR_LAUNCH(h, "spread_tiles_kernel");
+    CR_TRY(with_support<R>(h, [&](auto pt) -> int {
+        spread_tiles_kernel<R, decltype(pt)::value><<<h->ntiles, 256, spread_smem<R>(h), h->stream>>>(
+            m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
+            (R)h->d.prefac, m.grid);
+        CR_LAUNCH(h, "spread_tiles_kernel");
+        return CR_OK;
+    }));
     return CR_OK;
 }
 
@@ -384,20 +415,26 @@ template <typename R> static int wave_mesh(cr_handle *h, MeshBuffers<R> &m) {
 template <typename R> int wave_potential(cr_handle *h, MeshBuffers<R> &m) {
     CR_TRY(wave_mesh(h, m));
     ProfScope ps(h, PROF_CONTRACT);
-    contract_tiles_kernel<R, false><<<h->ntiles, 256, contract_smem<R>(h), h->stream>>>(
-        m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
-        (R)(h->d.quadW * h->d.prefac), m.grid, m.phi);
-    CR_LAUNCH(h, "contract_tiles_kernel");
+    CR_TRY(with_support<R>(h, [&](auto pt) -> int {
+        contract_tiles_kernel<R, false, decltype(pt)::value><<<h->ntiles, 256, contract_smem<R>(h), h->stream>>>(
+            m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
+            (R)(h->d.quadW * h->d.prefac), m.grid, m.phi);
+        CR_LAUNCH(h, "contract_tiles_kernel");
+        return CR_OK;
+    }));
     return CR_OK;
 }
 
 template <typename R> int wave_force(cr_handle *h, MeshBuffers<R> &m) {
     CR_TRY(wave_mesh(h, m));
     ProfScope ps(h, PROF_CONTRACT_FORCE);
-    contract_tiles_kernel<R, true><<<h->ntiles, 256, contract_smem<R>(h), h->stream>>>(
-        m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
-        (R)(2.0 * h->d.quadW * h->d.prefac * h->d.xiterm), m.grid, m.force);
-    CR_LAUNCH(h, "contract_force_tiles_kernel");
+    CR_TRY(with_support<R>(h, [&](auto pt) -> int {
+        contract_tiles_kernel<R, true, decltype(pt)::value><<<h->ntiles, 256, contract_smem<R>(h), h->stream>>>(
+            m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
+            (R)(2.0 * h->d.quadW * h->d.prefac * h->d.xiterm), m.grid, m.force);
+        CR_LAUNCH(h, "contract_force_tiles_kernel");
+        return CR_OK;
+    }));
     return CR_OK;
 }
 
