@@ -301,10 +301,11 @@ __global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long
             rows = slots[p1] / CS;
             xJ = qc[J * CS + lane];
         }
+        const int own = __popc(m);  // slots past the end of this lane's row hold zeros: skip them
         for (int base = 0; base < rcur; base += U) {
             R t[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) t[u] = base + u < rcur ? __ldg(v + (size_t)(base + u) * CS) : (R)0;
+            for (int u = 0; u < U; ++u) t[u] = base + u < own ? __ldg(v + (size_t)(base + u) * CS) : (R)0;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int j = m ? __ffs(m) - 1 : 0;
