@@ -86,6 +86,26 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     return LIB
 
 
+def build_module(force: bool = False) -> Path:
+    """The pybind11 module _ConductorRigid (C++ force compute, reference surface)."""
+    import sysconfig
+
+    import pybind11
+
+    src = PKG / "pybind" / "_ConductorRigid.cc"
+    out = PKG / ("_ConductorRigid" + sysconfig.get_config_var("EXT_SUFFIX"))
+    deps = [src, LIB, ROOT / "include" / "ConductorRigid.hpp"]
+    if not force and out.exists() and out.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return out
+    cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", str(ROOT / "include"), "-I", pybind11.get_include(),
+           "-I", sysconfig.get_paths()["include"], str(src), "-L", str(PKG), "-lconductor_rigid",
+           "-Wl,-rpath,$ORIGIN", "-o", str(out)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"pybind11 module build failed:\n{r.stdout}\n{r.stderr}")
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
@@ -93,6 +113,7 @@ def main() -> None:
     ap.add_argument("-v", action="store_true")
     a = ap.parse_args()
     print(build(force=a.force, jobs=a.j, verbose=a.v))
+    print(build_module(force=a.force))
 
 
 if __name__ == "__main__":
