@@ -128,6 +128,86 @@ __global__ void __launch_bounds__(256) spread_tiles_kernel(
     }
 }
 
+// Spread for a compile-time support PT (tile edge 8, halo buffer edge BD = 8 + PT - 1):
+// thread t < BD*BD owns the buffer column (y, z) = (t / BD, t % BD) in registers.  Beads
+// of the tile are taken 32 at a time: lane l of warp 0 computes the Gaussian factors of
+// bead l of the batch into shared memory (x factors already shifted to the column's
+// x index and scaled by prefac q), then every thread adds the beads whose window covers
+// its column.  No shared-memory atomics; within a tile the summation order is fixed.
+// The columns are added to the mesh once at the end.
+template <typename R, int PT>
+__global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32) spread_columns_kernel(
+    const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
+    const int *__restrict__ tile_start, const int *__restrict__ tile_beads, MeshShape ms, WindowConst<R> wc,
+    R prefac, R *__restrict__ grid) {
+    constexpr int P = PT, T = 8, BD = T + PT - 1;
+    __shared__ R sx[32][BD];     // shifted, scaled x factors
+    __shared__ R sy[32][P], sz[32][P];
+    __shared__ int soy[32], soz[32];
+    const int tile = blockIdx.x;
+    const int b0 = tile_start[tile], b1 = tile_start[tile + 1];
+    if (b0 == b1) return;
+    const int t = threadIdx.x;
+    const int cy = t / BD, cz = t - (t / BD) * BD;
+    const bool owner = t < BD * BD;
+    const int tz = tile % ms.ntd[2], ty = (tile / ms.ntd[2]) % ms.ntd[1], tx = tile / (ms.ntd[2] * ms.ntd[1]);
+    R col[BD];
+#pragma unroll
+    for (int x = 0; x < BD; ++x) col[x] = (R)0;
+    for (int base = b0; base < b1; base += 32) {
+        const int nb = min(32, b1 - base);
+        if (t < 32) {
+            const int l = t;
+            if (l < nb) {
+                const int i = tile_beads[base + l];
+                const typename Prec<R>::R4 p = pos[i];
+                const int4 st = wstart[i];
+                const int ox = wrapmod(st.x, ms.Ng[0]) - tx * T;
+                const int oy = wrapmod(st.y, ms.Ng[1]) - ty * T;
+                const int oz = wrapmod(st.z, ms.Ng[2]) - tz * T;
+                const bool ok = ox >= 0 && ox < T && oy >= 0 && oy < T && oz >= 0 && oz < T;
+                const R c = ok ? prefac * q[i] : (R)0;
+#pragma unroll
+                for (int x = 0; x < BD; ++x) sx[l][x] = (R)0;
+#pragma unroll
+                for (int a = 0; a < P; ++a) {
+                    const R rx = wc.h[0] * (R)(st.x + a) - wc.halfL[0] - p.x;
+                    const R ry = wc.h[1] * (R)(st.y + a) - wc.halfL[1] - p.y;
+                    const R rz = wc.h[2] * (R)(st.z + a) - wc.halfL[2] - p.z;
+                    if (ok) sx[l][ox + a] = c * dexp(-wc.xiterm * rx * rx * wc.inv_eta[0]);
+                    sy[l][a] = dexp(-wc.xiterm * ry * ry * wc.inv_eta[1]);
+                    sz[l][a] = dexp(-wc.xiterm * rz * rz * wc.inv_eta[2]);
+                }
+                soy[l] = ok ? oy : -BD;  // a bead outside its tile touches no column
+                soz[l] = oz;
+            }
+        }
+        __syncthreads();
+        if (owner) {
+            for (int b = 0; b < nb; ++b) {
+                const int ay = cy - soy[b], az = cz - soz[b];
+                if ((unsigned)ay < (unsigned)P && (unsigned)az < (unsigned)P) {
+                    const R wyz = sy[b][ay] * sz[b][az];
+#pragma unroll
+                    for (int x = 0; x < BD; ++x) col[x] += wyz * sx[b][x];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (owner) {
+        const int gy = fold(ty * T + cy, ms.Ng[1]);
+        const int gz = fold(tz * T + cz, ms.Ng[2]);
+#pragma unroll
+        for (int x = 0; x < BD; ++x) {
+            if (col[x] != (R)0) {
+                const int gx = fold(tx * T + x, ms.Ng[0]);
+                atomicAdd(grid + ((size_t)gx * ms.Ng[1] + gy) * ms.Ng[2] + gz, col[x]);
+            }
+        }
+    }
+}
+
 template <typename R, bool FORCE, int PT>
 __global__ void __launch_bounds__(256) contract_tiles_kernel(
     const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
@@ -380,10 +460,18 @@ template <typename R> int spread_only(cr_handle *h, MeshBuffers<R> &m) {
     const long G = grid_size(h);
     CR_CUDA(h, cudaMemsetAsync(m.grid, 0, G * sizeof(R), h->stream));
     CR_TRY(with_support<R>(h, [&](auto pt) -> int {
-        spread_tiles_kernel<R, decltype(pt)::value><<<h->ntiles, 256, spread_smem<R>(h), h->stream>>>(
-            m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h), window_const<R>(h),
-            (R)h->d.prefac, m.grid);
-        CR_LAUNCH(h, "spread_tiles_kernel");
+        constexpr int PT = decltype(pt)::value;
+        if (PT == 0) {
+            spread_tiles_kernel<R, 0><<<h->ntiles, 256, spread_smem<R>(h), h->stream>>>(
+                m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h),
+                window_const<R>(h), (R)h->d.prefac, m.grid);
+        } else {
+            constexpr int BD = 8 + (PT ? PT : 1) - 1;
+            spread_columns_kernel<R, (PT ? PT : 9)><<<h->ntiles, (BD * BD + 31) / 32 * 32, 0, h->stream>>>(
+                m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h),
+                window_const<R>(h), (R)h->d.prefac, m.grid);
+        }
+        CR_LAUNCH(h, "spread kernel");
         return CR_OK;
     }));
     return CR_OK;

@@ -563,7 +563,7 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
                                                                                          m.q, qc);
     CR_LAUNCH(h, "gather_cluster_kernel");
     constexpr int W = kSpmvWarps;
-    pair_spmv_kernel<R, W, 4><<<r.nclus, W * 32, 0, h->stream>>>(
+    pair_spmv_kernel<R, W, 16><<<r.nclus, W * 32, 0, h->stream>>>(
         r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, m.phi,
         h->d.selfcoeff, phi_body, h->d_body, out);
     CR_LAUNCH(h, "pair_spmv_kernel");

@@ -246,3 +246,23 @@ def test_conductor_preconditioned_solve_matches_oracle(cuda, product_lib, oracle
           f"err q={eq:.2e} phi={ep:.2e} F={ef:.2e}")
     assert st["converged"] == 1 and st["final_residual"] <= 1e-6
     assert eq < 1e-3 and ep < 1e-3 and ef < 1e-3
+
+
+@pytest.mark.parametrize("support", [7, 11])
+def test_operator_matches_oracle_other_supports(cuda, product_lib, oracle_lib, support):
+    """P=11 runs the compile-time spread/contract kernels, P=7 the runtime-P ones."""
+    from conductorrigid_b200 import systems
+
+    w = systems.workload("plain_small", scale=0.3)
+    s, p = w.system, w.params
+    base = {k: p[k] for k in ("xi", "errortol", "grid", "rcut")}
+    h = make_handle(product_lib, s, dict(base, support=support))
+    orc = oracle_lib.Oracle(s, p["xi"], p["errortol"], p["grid"], support, p["rcut"])
+    x = np.random.default_rng(13).standard_normal(s.n_beads + s.n_bodies)
+    q = x[: s.n_beads]
+    assert rel(h.spread(q), oracle_lib.spread(orc.p, s.pos, q)) < 1e-12
+    assert rel(h.spread(q, product_lib.CR_FP32), oracle_lib.spread(orc.p, s.pos, q)) < 2e-6
+    assert rel(h.apply_operator(x), orc.matvec(x)) < 1e-11
+    assert rel(h.apply_operator(x, product_lib.CR_FP32), orc.matvec(x)) < 2e-5
+    assert rel(h.forces(q), orc.forces(q, s.field)) < 1e-11
+    h.close()
