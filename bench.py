@@ -191,6 +191,29 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_op_case(args) -> None:
+    """Operator applications on the scaled workload (the case the ncu captures use)."""
+    import torch
+
+    from conductorrigid_b200 import _lib, systems
+    from conductorrigid_b200.device import Handle
+
+    w = systems.workload(WORKLOAD, scale=args.op_case)
+    s, p = w.system, w.params
+    full_L = systems.workload(WORKLOAD).system.L[0]
+    grid = systems.smooth_at_least(int(np.ceil(p["grid"] * s.L[0] / full_L)), 4096)  # same mesh spacing
+    base = dict(xi=p["xi"], errortol=p["errortol"], grid=grid, support=p["support"], rcut=p["rcut"])
+    h = Handle(_lib.make_params(field=tuple(s.field), precond="conductor", **base), s.L)
+    h.set_topology(s.body, s.rigid, s.body_charge)
+    h.set_positions(s.pos, s.body_pos)
+    x = torch.randn(s.n_beads + s.n_bodies, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup + args.steps):
+        h.apply_operator(x, _lib.CR_FP32)
+    torch.cuda.synchronize()
+    print(json.dumps({"op_case": args.op_case, "charges": s.n_beads, "mesh": grid, **h.geometry_info()}))
+    h.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -199,10 +222,16 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--learned", type=int, default=0)
+    ap.add_argument("--op-case", type=float, default=0.0,
+                    help="profiling case: the workload scaled to this body fraction, --steps operator "
+                         "applications in FP32 (small enough for a full ncu capture)")
     ap.add_argument("--arms", default="fast,plain,f64c",
                     help="arms to run: fast (headline), plain (reference preconditioner), f64c (FP64 ablation)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.op_case > 0:
+        run_op_case(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
