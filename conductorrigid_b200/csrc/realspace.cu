@@ -314,19 +314,14 @@ __global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long
         }
         const int len = __popc(m);
         const int kmax = __reduce_max_sync(0xffffffffu, len);
-        const R *vbase = vals + o;
-        int orel = 0;  // offset of slot base within the pair (at most 1024 values)
         for (int base = 0; base < kmax; base += U) {
-            // slot offsets first (ballots only), then every load, then the sums
-            int at[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                at[u] = orel + rank;
-                orel += __popc(__ballot_sync(0xffffffffu, len > base + u));
-            }
             R t[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) t[u] = base + u < len ? __ldg(vbase + at[u]) : (R)0;
+            for (int u = 0; u < U; ++u) {
+                const int kk = base + u;
+                t[u] = kk < len ? __ldg(vals + o + rank) : (R)0;
+                o += __popc(__ballot_sync(0xffffffffu, len > kk));
+            }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int j = m ? __ffs(m) - 1 : 0;
