@@ -88,10 +88,9 @@ struct RealSpace {
     int *pair_i = nullptr, *pair_j = nullptr;
     long long npairs = 0, pair_cap = 0;
     unsigned *masks = nullptr;      // [npairs*32] row bit masks of in-range bead pairs
-    unsigned char *ranks = nullptr; // [npairs*32] rank of each row by length (longest first)
     int *nnz_pair = nullptr;        // [npairs] set bits per pair
     long long *voff = nullptr;      // [npairs] first packed value of each pair
-    long long nnz = 0;              // stored values (one per interacting directed bead pair)
+    long long nnz = 0;              // stored value slots (rows padded to each pair's longest row)
     long long npairs_beads = 0;     // interacting directed bead pairs (set mask bits)
     unsigned long long *bits = nullptr;
     float *vals32 = nullptr;        // [nnz] packed T(d) values

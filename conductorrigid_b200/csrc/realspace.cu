@@ -16,10 +16,10 @@
 //    floor(Ntable (d - dr)/(rc - dr)) and linear weight d/dr - index - 1 of
 //    ConductorRigid.cu:549-554, evaluated in FP64 and stored in the operator
 //    precision (the 32x32 blocks of a 4-unit cutoff are only 20-35% full, so the mask
-//    keeps the streamed bytes at one value per interacting pair).  The rows of a pair
-//    are ranked by length (longest first, ties by row index); slot k holds the k-th
-//    value of every row longer than k, in rank order, so that slot k of all lanes is
-//    one contiguous, coalesced warp load and nothing is padded;
+//    keeps the streamed bytes near one value per interacting pair).  The values of a
+//    pair are stored lane-interleaved: the k-th value of row i at k*32 + i, rows padded
+//    with zeros to the pair's longest row, so that every load is one coalesced warp
+//    load;
 //  * the product y_I = sum_J B_IJ x_J, the pairs of cluster I split over the warps of
 //    one CTA: lane i takes the k-th set bit j of its row, multiplies the k-th value by
 //    x_J[j] fetched with a warp shuffle; the partial sums are added in warp order, so
@@ -157,11 +157,11 @@ __device__ __forceinline__ double table_lerp64(const double2 *__restrict__ tab, 
 }
 
 // Bit masks of the in-range bead pairs of every cluster pair (row i = bead i of I,
-// bit j = bead j of J), the rank of every row by length, and the set bits per pair.
+// bit j = bead j of J) and the stored slots of the pair (32 x its longest row).
 __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
                                  const int *__restrict__ members, const double4 *__restrict__ pos, RSBuild c,
-                                 unsigned *__restrict__ masks, unsigned char *__restrict__ ranks,
-                                 int *__restrict__ nnz, unsigned long long *__restrict__ bits) {
+                                 unsigned *__restrict__ masks, int *__restrict__ nnz,
+                                 unsigned long long *__restrict__ bits) {
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (p >= npairs) return;
@@ -185,17 +185,13 @@ __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_
         }
     }
     masks[p * CS + lane] = m;
-    const int len = __popc(m);
-    int rank = 0;  // rows before this one: longer, or as long with a smaller index
-    for (int j = 0; j < CS; ++j) {
-        const int lj = __shfl_sync(0xffffffffu, len, j);
-        rank += (lj > len || (lj == len && j < lane)) ? 1 : 0;
+    int n = __popc(m), tot = n;
+    for (int o = 16; o > 0; o >>= 1) {
+        n = max(n, __shfl_xor_sync(0xffffffffu, n, o));
+        tot += __shfl_xor_sync(0xffffffffu, tot, o);
     }
-    ranks[p * CS + lane] = (unsigned char)rank;
-    int tot = len;
-    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
     if (lane == 0) {
-        nnz[p] = tot;
+        nnz[p] = n * CS;  // stored slots: longest row times 32 lanes
         atomicAdd(bits, (unsigned long long)tot);
     }
 }
@@ -209,13 +205,13 @@ __device__ __forceinline__ int warp_exclusive_scan(int v, int lane) {
     return incl - v;
 }
 
-// Values T(d_ij) of the set mask bits in the operator precision: the k-th set bit of row
-// i at voff + (rows longer than 0..k-1, summed) + rank_i.
+// Values T(d_ij) of the set mask bits in the operator precision, lane-interleaved:
+// the k-th set bit of row i at voff + k*32 + i, zeros after the row's last bit.
 template <typename R>
 __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
                                    const int *__restrict__ members, const double4 *__restrict__ pos,
                                    const double2 *__restrict__ tab, RSBuild c, const unsigned *__restrict__ masks,
-                                   const unsigned char *__restrict__ ranks, const long long *__restrict__ voff,
+                                   const long long *__restrict__ voff, const int *__restrict__ slots,
                                    R *__restrict__ vals) {
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -226,15 +222,7 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
     const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
     const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
     const unsigned m = masks[p * CS + lane];
-    const int len = __popc(m), rank = ranks[p * CS + lane];
-    const int kmax = __reduce_max_sync(0xffffffffu, len);
-    // slot offsets (uniform across the warp)
-    long long o = voff[p];
-    long long myoff[CS];
-    for (int k = 0; k < kmax; ++k) {
-        myoff[k] = o + rank;
-        o += __popc(__ballot_sync(0xffffffffu, len > k));
-    }
+    R *out = vals + voff[p] + lane;
     int k = 0;
     for (int j = 0; j < CS; ++j) {
         const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
@@ -244,10 +232,12 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
             const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
             const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
             const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
-            vals[myoff[k]] = (R)table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
+            out[(size_t)k * CS] = (R)table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
             ++k;
         }
     }
+    const int rows = slots[p] / CS;
+    for (; k < rows; ++k) out[(size_t)k * CS] = (R)0;
 }
 
 // Charges in cluster order (0 for padding), so that a warp reads a cluster's charges
@@ -264,19 +254,18 @@ __global__ void gather_cluster_kernel(int n, const int *__restrict__ members, co
 // y_I = sum_J B_IJ x_J for cluster I (one CTA of W warps), combined with the wave-space
 // part and the self term: out_i = Phi_body(i) - (phik_i + self q_i + y_i), or the bare
 // sum when phi_body is NULL.  Warp w takes pairs w, w+W, ...; lane i consumes the set
-// bits of its mask row in order, the k-th against slot k at offset
-// (rows longer than 0..k-1) + rank_i, with x_J[j] from a shuffle.  Up to U slots are
-// loaded before they are used; the next pair's metadata is fetched while the current
-// one is summed.  The W partial sums are added in warp order, so the result does not
-// depend on scheduling.
+// bits of its mask row in order, the k-th against the coalesced load of slot k, with
+// x_J[j] from a shuffle.  Up to U slots are loaded before they are used; the next
+// pair's metadata is fetched while the current one is summed.  The W partial sums are
+// added in warp order, so the result does not depend on scheduling.
 template <typename R, int W, int U>
 __global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long long *__restrict__ head,
                                                            const int *__restrict__ count,
                                                            const int *__restrict__ pair_j,
                                                            const int *__restrict__ members,
                                                            const unsigned *__restrict__ masks,
-                                                           const unsigned char *__restrict__ ranks,
                                                            const long long *__restrict__ voff,
+                                                           const int *__restrict__ slots,
                                                            const R *__restrict__ vals, const R *__restrict__ qc,
                                                            const R *__restrict__ q, const R *__restrict__ phik,
                                                            double selfc, const double *__restrict__ phi_body,
@@ -288,40 +277,35 @@ __global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long
     R yI = 0;
     const long long h0 = head[I];
     const int n = count[I];
-    int J = 0, rk = 0;
+    int J = 0, rows = 0;
     unsigned m0 = 0;
     long long off = 0;
     R xJ = 0;
     if (w < n) {
         J = pair_j[h0 + w];
         m0 = masks[(h0 + w) * CS + lane];
-        rk = ranks[(h0 + w) * CS + lane];
         off = voff[h0 + w];
+        rows = slots[h0 + w] / CS;
         xJ = qc[J * CS + lane];
     }
     for (int k = w; k < n; k += W) {
+        const R *v = vals + off + lane;
         unsigned m = m0;
         const R xcur = xJ;
-        const int rank = rk;
-        long long o = off;
+        const int rcur = rows;
         if (k + W < n) {
             const long long p1 = h0 + k + W;
             J = pair_j[p1];
             m0 = masks[p1 * CS + lane];
-            rk = ranks[p1 * CS + lane];
             off = voff[p1];
+            rows = slots[p1] / CS;
             xJ = qc[J * CS + lane];
         }
-        const int len = __popc(m);
-        const int kmax = __reduce_max_sync(0xffffffffu, len);
-        for (int base = 0; base < kmax; base += U) {
+        const int own = __popc(m);  // slots past the end of this lane's row hold zeros: skip them
+        for (int base = 0; base < rcur; base += U) {
             R t[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int kk = base + u;
-                t[u] = kk < len ? __ldg(vals + o + rank) : (R)0;
-                o += __popc(__ballot_sync(0xffffffffu, len > kk));
-            }
+            for (int u = 0; u < U; ++u) t[u] = base + u < own ? __ldg(v + (size_t)(base + u) * CS) : (R)0;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int j = m ? __ffs(m) - 1 : 0;
@@ -442,7 +426,7 @@ template <typename R> int realspace_blocks(cr_handle *h) {
         cap_of<R>(r) = cap;
     }
     pair_values_kernel<R><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
-        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.ranks, r.voff,
+        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.voff, r.nnz_pair,
         blocks_of<R>(r));
     CR_LAUNCH(h, "pair_values_kernel");
     valid_of<R>(r) = true;
@@ -463,7 +447,6 @@ void realspace_free(cr_handle *h) {
     dfree(&r.vals32);
     dfree(&r.vals64);
     dfree(&r.masks);
-    dfree(&r.ranks);
     dfree(&r.nnz_pair);
     dfree(&r.voff);
     dfree(&r.acc32);
@@ -529,7 +512,6 @@ int realspace_build(cr_handle *h) {
         CR_TRY(dalloc(h, &r.pair_i, (size_t)cap));
         CR_TRY(dalloc(h, &r.pair_j, (size_t)cap));
         CR_TRY(dalloc(h, &r.masks, (size_t)cap * CS));
-        CR_TRY(dalloc(h, &r.ranks, (size_t)cap * CS));
         CR_TRY(dalloc(h, &r.nnz_pair, (size_t)cap));
         CR_TRY(dalloc(h, &r.voff, (size_t)cap));
         r.pair_cap = cap;
@@ -548,8 +530,8 @@ int realspace_build(cr_handle *h) {
     CR_LAUNCH(h, "pair_owner_kernel");
     const int pb = blocks_for(r.npairs * 32, 256);
     CR_CUDA(h, cudaMemsetAsync(r.bits, 0, sizeof(unsigned long long), s));
-    pair_mask_kernel<<<pb, 256, 0, s>>>(r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, c, r.masks, r.ranks,
-                                        r.nnz_pair, r.bits);
+    pair_mask_kernel<<<pb, 256, 0, s>>>(r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, c, r.masks, r.nnz_pair,
+                                        r.bits);
     CR_LAUNCH(h, "pair_mask_kernel");
     bytes = h->sort_tmp_bytes;
     CR_CUDA(h, cub::DeviceScan::ExclusiveSum(h->d_sort_tmp, bytes, r.nnz_pair, r.voff, (int)r.npairs, s));
@@ -582,7 +564,7 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
     CR_LAUNCH(h, "gather_cluster_kernel");
     constexpr int W = kSpmvWarps;
     pair_spmv_kernel<R, W, 16><<<r.nclus, W * 32, 0, h->stream>>>(
-        r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.ranks, r.voff, blocks_of<R>(r), qc, m.q, m.phi,
+        r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, m.phi,
         h->d.selfcoeff, phi_body, h->d_body, out);
     CR_LAUNCH(h, "pair_spmv_kernel");
     return CR_OK;
