@@ -110,6 +110,10 @@ class CrGeometryInfo(C.Structure):
     ]
 
 
+class CrBrownianParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("kT", C.c_double), ("viscosity", C.c_double), ("seed", C.c_uint64)]
+
+
 class CrError(RuntimeError):
     def __init__(self, status: int, where: str, msg: str = ""):
         self.status = status
@@ -149,6 +153,18 @@ _SIGS = {
     "cr_profile_read": ([_P, _I, C.POINTER(C.c_int), C.POINTER(C.c_double)], _I),
     "cr_counters": ([_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], _I),
     "cr_get_geometry_info": ([_P, C.POINTER(CrGeometryInfo)], _I),
+    "cr_body_force_torque": ([_P, _P, _P, _P, _P, _P], _I),
+    "cr_brownian_step": ([_P, C.POINTER(CrBrownianParams), C.c_int64, _P, _P, _P, _P], _I),
+    "cr_mlp_create": ([C.c_uint64, C.POINTER(_P)], _I),
+    "cr_mlp_destroy": ([_P], _I),
+    "cr_mlp_last_error": ([_P], C.c_char_p),
+    "cr_mlp_get_params": ([_P, C.POINTER(C.c_float)], _I),
+    "cr_mlp_set_params": ([_P, C.POINTER(C.c_float)], _I),
+    "cr_mlp_get_grads": ([_P, C.POINTER(C.c_float)], _I),
+    "cr_mlp_forward": ([_P, _I, _P, _P, _P], _I),
+    "cr_mlp_accumulate_grad": ([_P, _I, _P, _P, C.POINTER(C.c_double), _P], _I),
+    "cr_mlp_adam": ([_P, C.c_double, C.c_double, _P], _I),
+    "cr_mlp_counters": ([_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], _I),
     "cr_spread_noalloc": ([C.POINTER(CrDerived), C.c_double, _D, _I, _P, _P, _P, _P], _I),
     "cr_noalloc_last_error": ([], C.c_char_p),
     "cr_util_icosphere_count": ([_I], _I),

@@ -79,6 +79,9 @@ void free_all(cr_handle *h) {
     dfree(&h->d_io_q);
     dfree(&h->d_io_phi);
     dfree(&h->d_io_force);
+    dfree(&h->d_bf);
+    dfree(&h->d_bt);
+    dfree(&h->d_moves);
 }
 
 int derive(cr_handle *h, const cr_params *p, const double L[3]) {
@@ -513,5 +516,25 @@ int cr_compute_host(cr_handle *h, const double *pos, const double *body_pos, dou
     return st;
 }
 
-}  // extern "C"
+int cr_body_force_torque(cr_handle *h, const double *d_pos, const double *d_body_pos, const double *d_force,
+                         double *d_body_force, double *d_body_torque) {
+    CR_TRY(need_ready(h));
+    if (h->B > 0 && (!d_pos || !d_body_pos || !d_force || !d_body_force || !d_body_torque))
+        return fail(h, CR_BAD_PARAM, "null array");
+    return body_force_torque(h, d_pos, d_body_pos, d_force, d_body_force, d_body_torque);
+}
 
+int cr_brownian_step(cr_handle *h, const cr_brownian_params *p, int64_t step, const double *d_radius,
+                     const double *d_force, double *d_pos, double *d_body_pos) {
+    CR_TRY(need_ready(h));
+    if (!p) return fail(h, CR_BAD_PARAM, "null parameters");
+    if (!(p->dt >= 0.0) || !(p->kT >= 0.0) || !(p->viscosity > 0.0) || !std::isfinite(p->dt) ||
+        !std::isfinite(p->kT) || !std::isfinite(p->viscosity))
+        return fail(h, CR_BAD_PARAM, "dt and kT must be finite and >= 0, viscosity > 0");
+    if (h->B > 0 && (!d_radius || !d_force || !d_pos || !d_body_pos)) return fail(h, CR_BAD_PARAM, "null array");
+    const int st = brownian_step(h, p, (long long)step, d_radius, d_force, d_pos, d_body_pos);
+    h->geo.valid = false;  // positions moved: the next solve rebuilds the geometry
+    return st;
+}
+
+}  // extern "C"

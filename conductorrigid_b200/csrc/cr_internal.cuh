@@ -207,6 +207,8 @@ struct cr_handle {
     long long fft_execs = 0;          // cuFFT executions
     // staging for cr_compute_host
     double *d_io_pos = nullptr, *d_io_bpos = nullptr, *d_io_q = nullptr, *d_io_phi = nullptr, *d_io_force = nullptr;
+    // rigid-body stepper: body force and torque, per-body move sizes
+    double *d_bf = nullptr, *d_bt = nullptr, *d_moves = nullptr;
 };
 
 namespace cr {
@@ -303,6 +305,10 @@ void conductor_free(cr_handle *h);
 int apply_operator(cr_handle *h, const double *x, double *y, int precision);
 // Solve A x = b (x holds the warm start).
 int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st);
+int body_force_torque(cr_handle *h, const double *pos, const double *bpos, const double *force, double *bf,
+                      double *bt);
+int brownian_step(cr_handle *h, const cr_brownian_params *bp, long long step, const double *radius,
+                  const double *force, double *pos, double *bpos);
 int krylov_alloc(cr_handle *h);
 void krylov_free(cr_handle *h);
 

@@ -166,6 +166,31 @@ class Handle:
         self._check(_lib.lib().cr_counters(self.h, C.byref(a), C.byref(b)), "cr_counters")
         return {"kernel_launches": a.value, "fft_execs": b.value}
 
+    # -- rigid-body dynamics ---------------------------------------------------
+    def body_force_torque(self, pos, body_pos, force):
+        """Body forces and torques [B, 3] about the centres from bead forces [N, 3]."""
+        pos = self.dev(pos).reshape(-1, 3)
+        bpos = self.dev(body_pos).reshape(-1, 3)
+        force = self.dev(force).reshape(-1, 3)
+        bf = self.empty(self.B, 3)
+        bt = self.empty(self.B, 3)
+        self._check(_lib.lib().cr_body_force_torque(self.h, _ptr(pos), _ptr(bpos), _ptr(force), _ptr(bf),
+                                                    _ptr(bt)), "cr_body_force_torque")
+        return bf, bt
+
+    def brownian_step(self, step, radius, force, pos, body_pos, dt=1e-3, kT=1.0, viscosity=1.0, seed=1):
+        """One overdamped rigid-body Brownian step; pos [N, 3] and body_pos [B, 3] (device
+        float64 tensors) are moved in place."""
+        t = self.torch
+        for a in (pos, body_pos):
+            if not (isinstance(a, t.Tensor) and a.is_cuda and a.dtype == t.float64 and a.is_contiguous()):
+                raise TypeError("pos and body_pos must be contiguous float64 CUDA tensors (moved in place)")
+        p = _lib.CrBrownianParams(dt, kT, viscosity, seed)
+        radius = self.dev(radius)
+        force = self.dev(force).reshape(-1, 3)
+        self._check(_lib.lib().cr_brownian_step(self.h, C.byref(p), int(step), _ptr(radius), _ptr(force),
+                                                _ptr(pos), _ptr(body_pos)), "cr_brownian_step")
+
     # -- the step --------------------------------------------------------------
     def compute(self, pos, body_pos, q, phi, allow_not_converged=False):
         """Device arrays in, solve + forces; q and phi are updated in place."""

@@ -196,6 +196,54 @@ int cr_get_geometry_info(const cr_handle *h, cr_geometry_info *out);
 /* Kernels of this library launched through the handle, and cuFFT executions. */
 int cr_counters(const cr_handle *h, long long *kernel_launches, long long *fft_execs);
 
+/* ---- rigid-body dynamics ----
+ * No counterpart in the reference, which leaves time integration to HOOMD's rigid-body
+ * integrator.  cr_body_force_torque sums bead forces d_force[N*3] (from cr_compute)
+ * into body forces d_body_force[B*3] and torques d_body_torque[B*3] about the body
+ * centres d_body_pos[B*3] (minimum-image bead offsets, FP64).
+ * cr_brownian_step takes one overdamped Brownian step of every body in place:
+ * translation mu_t F dt + sqrt(2 kT mu_t dt) g, mu_t = 1/(6 pi viscosity a_b);
+ * rotation (rigid bodies only) by the angle vector mu_r T dt + sqrt(2 kT mu_r dt) g',
+ * mu_r = 1/(8 pi viscosity a_b^3), about the body centre; d_radius[B] holds a_b.  Bead
+ * and body positions are wrapped into [-L/2, L/2).  The Gaussian numbers g, g' are a
+ * pure function of (seed, step, body): SplitMix64 counters and the Box-Muller
+ * transform, so a trajectory does not depend on launch shape or device. */
+typedef struct {
+    double dt;          /* time step */
+    double kT;          /* thermal energy */
+    double viscosity;   /* solvent viscosity */
+    uint64_t seed;      /* noise stream */
+} cr_brownian_params;
+int cr_body_force_torque(cr_handle *h, const double *d_pos, const double *d_body_pos, const double *d_force,
+                         double *d_body_force, double *d_body_torque);
+int cr_brownian_step(cr_handle *h, const cr_brownian_params *p, int64_t step, const double *d_radius,
+                     const double *d_force, double *d_pos, double *d_body_pos);
+
+/* ---- the learned initial guess: per-bead network on the tensor cores ----
+ * No counterpart in the reference.  A 48 -> 128 -> 128 -> 1 GELU network with BF16
+ * operands and FP32 accumulation on the sm_100 tensor cores (tcgen05, accumulators in
+ * tensor memory).  Parameters are one FP32 vector of CR_MLP_PARAMS values:
+ * W1[128][48], b1[128], W2[128][128], b2[128], w3[128], b3.  Features are BF16 rows of
+ * 48 values (16-byte aligned).  cr_mlp_forward writes y[n]; cr_mlp_accumulate_grad adds
+ * the gradient of (1/n) sum (y - t)^2 to the network's gradient buffer and returns the
+ * loss; cr_mlp_adam applies one Adam step (gradients clipped to +-clip) and clears the
+ * buffer.  Device waits are bounded: a wait that runs out returns CR_TIMEOUT.
+ * Needs an sm_100 GPU (CR_BAD_PARAM otherwise). */
+#define CR_MLP_FEATURES 48
+#define CR_MLP_HIDDEN 128
+#define CR_MLP_PARAMS 22913
+typedef struct cr_mlp cr_mlp;
+int cr_mlp_create(uint64_t seed, cr_mlp **out);
+int cr_mlp_destroy(cr_mlp *net);
+const char *cr_mlp_last_error(const cr_mlp *net);
+int cr_mlp_get_params(cr_mlp *net, float *params);
+int cr_mlp_set_params(cr_mlp *net, const float *params);
+int cr_mlp_get_grads(cr_mlp *net, float *grads);
+int cr_mlp_forward(cr_mlp *net, int n, const uint16_t *d_x, float *d_y, void *stream);
+int cr_mlp_accumulate_grad(cr_mlp *net, int n, const uint16_t *d_x, const float *d_t, double *loss, void *stream);
+int cr_mlp_adam(cr_mlp *net, double lr, double clip, void *stream);
+int cr_mlp_counters(const cr_mlp *net, long long *kernel_launches, long long *adam_steps);
+
 /* ---- spreading without device allocation ----
  * No counterpart in the reference.  For callers that cannot allocate device memory
  * where they need the charge mesh: a host engine that owns all device memory through
