@@ -92,6 +92,7 @@ class CrSolveStats(C.Structure):
         ("initial_residual", C.c_double),
         ("final_residual", C.c_double),
         ("solve_ms", C.c_double),
+        ("learned_residual", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -111,7 +112,8 @@ class CrGeometryInfo(C.Structure):
 
 
 class CrBrownianParams(C.Structure):
-    _fields_ = [("dt", C.c_double), ("kT", C.c_double), ("viscosity", C.c_double), ("seed", C.c_uint64)]
+    _fields_ = [("dt", C.c_double), ("kT", C.c_double), ("viscosity", C.c_double), ("seed", C.c_uint64),
+                ("repulsion", C.c_double), ("contact_gap", C.c_double)]
 
 
 class CrError(RuntimeError):
@@ -165,6 +167,14 @@ _SIGS = {
     "cr_mlp_accumulate_grad": ([_P, _I, _P, _P, C.POINTER(C.c_double), _P], _I),
     "cr_mlp_adam": ([_P, C.c_double, C.c_double, _P], _I),
     "cr_mlp_counters": ([_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], _I),
+    "cr_set_guess_directions": ([_P, _I, _P], _I),
+    "cr_bead_neighbors": ([_P, _P, _P], _I),
+    "cr_body_neighbors": ([_P, _P, _P], _I),
+    "cr_guess_features": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
+    "cr_feature_stats": ([_P, _I, _P, _P], _I),
+    "cr_feature_pack": ([_P, _I, _P, _P, _P, _P], _I),
+    "cr_guess_target": ([_P, _P, _P, C.c_double, _P], _I),
+    "cr_neutral_direction": ([_P, _P, _I, C.c_double, _P], _I),
     "cr_spread_noalloc": ([C.POINTER(CrDerived), C.c_double, _D, _I, _P, _P, _P, _P], _I),
     "cr_noalloc_last_error": ([], C.c_char_p),
     "cr_util_icosphere_count": ([_I], _I),

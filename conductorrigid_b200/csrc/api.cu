@@ -82,6 +82,8 @@ void free_all(cr_handle *h) {
     dfree(&h->d_bf);
     dfree(&h->d_bt);
     dfree(&h->d_moves);
+    dfree(&h->d_guess);
+    h->n_guess = 0;
 }
 
 int derive(cr_handle *h, const cr_params *p, const double L[3]) {
@@ -531,6 +533,8 @@ int cr_brownian_step(cr_handle *h, const cr_brownian_params *p, int64_t step, co
     if (!(p->dt >= 0.0) || !(p->kT >= 0.0) || !(p->viscosity > 0.0) || !std::isfinite(p->dt) ||
         !std::isfinite(p->kT) || !std::isfinite(p->viscosity))
         return fail(h, CR_BAD_PARAM, "dt and kT must be finite and >= 0, viscosity > 0");
+    if (!(p->repulsion >= 0.0) || !std::isfinite(p->repulsion) || !std::isfinite(p->contact_gap))
+        return fail(h, CR_BAD_PARAM, "repulsion must be finite and >= 0");
     if (h->B > 0 && (!d_radius || !d_force || !d_pos || !d_body_pos)) return fail(h, CR_BAD_PARAM, "null array");
     const int st = brownian_step(h, p, (long long)step, d_radius, d_force, d_pos, d_body_pos);
     h->geo.valid = false;  // positions moved: the next solve rebuilds the geometry

@@ -209,6 +209,9 @@ struct cr_handle {
     double *d_io_pos = nullptr, *d_io_bpos = nullptr, *d_io_q = nullptr, *d_io_phi = nullptr, *d_io_force = nullptr;
     // rigid-body stepper: body force and torque, per-body move sizes
     double *d_bf = nullptr, *d_bt = nullptr, *d_moves = nullptr;
+    // learned guess: caller directions for the next solve [CR_MAX_GUESS_DIRECTIONS][N+B]
+    double *d_guess = nullptr;
+    int n_guess = 0;
 };
 
 namespace cr {

@@ -8,7 +8,8 @@
 //   dth = mu_r tau_b dt + sqrt(2 kT mu_r dt) xi_r, mu_r = 1/(8 pi eta a_b^3)
 //   R_b <- R_b + dR,  r_i <- R_b + dR + Rot(dth) (r_i - R_b)   (Rodrigues rotation)
 // and every position is wrapped back into the box.  Free beads (rigid = 0) translate
-// only.  The Gaussian numbers come from a counter-based generator (SplitMix64 of seed,
+// only.  An optional harmonic steric repulsion between body surfaces is added to F_b
+// (the reference's users run one in HOOMD beside the plugin).  The Gaussian numbers come from a counter-based generator (SplitMix64 of seed,
 // step, body, component; Box-Muller), so a step is reproducible anywhere.
 #include <cmath>
 
@@ -75,6 +76,39 @@ __global__ void body_force_torque_kernel(int B, const int *__restrict__ start, c
             bf[3 * (size_t)b + d] = f[d];
             bt[3 * (size_t)b + d] = t[d];
         }
+}
+
+// Harmonic steric repulsion between body surfaces, added to bf: all pairs, minimum
+// image, centres staged through shared memory in tiles.
+__global__ void repulsion_kernel(int B, const double *__restrict__ bpos, const double *__restrict__ radius,
+                                 double k, double gap, double Lx, double Ly, double Lz, double *__restrict__ bf) {
+    __shared__ double4 tile[256];
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    double4 c = make_double4(0, 0, 0, 0);
+    if (b < B) c = make_double4(bpos[3 * (size_t)b], bpos[3 * (size_t)b + 1], bpos[3 * (size_t)b + 2], radius[b]);
+    double f[3] = {0, 0, 0};
+    for (int t0 = 0; t0 < B; t0 += 256) {
+        const int j = t0 + threadIdx.x;
+        if (j < B) tile[threadIdx.x] = make_double4(bpos[3 * (size_t)j], bpos[3 * (size_t)j + 1], bpos[3 * (size_t)j + 2], radius[j]);
+        __syncthreads();
+        const int cnt = min(256, B - t0);
+        if (b < B)
+            for (int u = 0; u < cnt; ++u) {
+                if (t0 + u == b) continue;
+                const double dx = mimg(tile[u].x - c.x, Lx), dy = mimg(tile[u].y - c.y, Ly), dz = mimg(tile[u].z - c.z, Lz);
+                const double reach = c.w + tile[u].w + gap;
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 >= reach * reach || d2 == 0.0) continue;
+                const double d = sqrt(d2);
+                const double mag = k * (reach - d) / d;
+                f[0] -= mag * dx;
+                f[1] -= mag * dy;
+                f[2] -= mag * dz;
+            }
+        __syncthreads();
+    }
+    if (b < B)
+        for (int e = 0; e < 3; ++e) bf[3 * (size_t)b + e] += f[e];
 }
 
 struct StepArgs {
@@ -159,6 +193,12 @@ int brownian_step(cr_handle *h, const cr_brownian_params *bp, long long step, co
         CR_TRY(dalloc(h, &h->d_moves, 2 * (size_t)h->B));
     }
     CR_TRY(body_force_torque(h, pos, bpos, force, h->d_bf, h->d_bt));
+    if (bp->repulsion > 0.0) {
+        repulsion_kernel<<<blocks_for(h->B, 256), 256, 0, h->stream>>>(h->B, bpos, radius, bp->repulsion,
+                                                                       bp->contact_gap, h->L[0], h->L[1], h->L[2],
+                                                                       h->d_bf);
+        CR_LAUNCH(h, "repulsion_kernel");
+    }
     StepArgs a;
     a.dt = bp->dt;
     a.kT = bp->kT;

@@ -89,6 +89,23 @@ __global__ void axpy_kernel(int n, double a, const double *__restrict__ x, doubl
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
 }
 
+// Learned-guess refit of the body potentials: Phi_b += mean of the bead residuals of
+// body b, which zeroes that mean (a bead row is Phi_b - (M q)_i = b_i; the charge rows
+// do not involve Phi).  Exact, no operator application.
+__global__ void phi_refit_kernel(int N, int B, const int *__restrict__ start, const int *__restrict__ members,
+                                 double *__restrict__ x, double *__restrict__ r) {
+    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (b >= B) return;
+    const int k0 = start[b], k1 = start[b + 1];
+    double s = 0.0;
+    for (int k = k0 + lane; k < k1; k += 32) s += r[members[k]];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double mean = s / (double)(k1 - k0);
+    for (int k = k0 + lane; k < k1; k += 32) r[members[k]] -= mean;
+    if (lane == 0) x[N + b] += mean;
+}
+
 int vec_blocks(int n) { return std::max(1, std::min(4 * 148, blocks_for(n, 256))); }
 
 // hcol[0..k) = V[0..k)^T w   (device result)
@@ -219,6 +236,80 @@ int fgmres(cr_handle *h, int precision, double *x, const double *b, int r_mode, 
     return beta <= atol ? CR_OK : CR_NOT_CONVERGED;
 }
 
+// Learned start: x += sum_j c_j D_j with c minimising ||r - sum_j c_j A D_j|| over the
+// caller's guess directions D (h->d_guess, k of them), then the potential refit; r is
+// recomputed with the FP64 operator.  The k x k normal equations are solved in FP64 on
+// the host (Gaussian elimination with partial pivoting on a slightly shifted Gram matrix;
+// a direction whose pivot vanishes gets weight 0).
+int learned_start(cr_handle *h, int precision, double *x, const double *b, OpCount &oc, double *rnorm) {
+    Krylov &K = h->kry;
+    const int n = K.n, nb = vec_blocks(n);
+    const int k = std::min(h->n_guess, K.m + 1);
+    if (k > 0) {
+        double *W = K.V;  // A D_j in the basis storage (free before the solve)
+        for (int j = 0; j < k; ++j) CR_TRY(op_apply(h, precision, h->d_guess + (size_t)j * n, W + (size_t)j * n, oc));
+        std::vector<double> G((size_t)k * k), rhs(k);
+        for (int l = 0; l < k; ++l) {
+            CR_TRY(dots(h, k, W, W + (size_t)l * n, K.hcol));
+            CR_CUDA(h, cudaMemcpyAsync(K.h_pinned, K.hcol, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CR_CUDA(h, cudaStreamSynchronize(h->stream));
+            for (int j = 0; j < k; ++j) G[(size_t)j * k + l] = K.h_pinned[j];
+        }
+        CR_TRY(dots(h, k, W, K.r, K.hcol));
+        CR_CUDA(h, cudaMemcpyAsync(K.h_pinned, K.hcol, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CR_CUDA(h, cudaStreamSynchronize(h->stream));
+        for (int j = 0; j < k; ++j) rhs[j] = K.h_pinned[j];
+        double tr = 0;
+        for (int j = 0; j < k; ++j) tr += G[(size_t)j * k + j];
+        for (int j = 0; j < k; ++j) G[(size_t)j * k + j] += 1e-13 * tr + 1e-300;
+        std::vector<int> piv(k);
+        std::vector<double> c(k, 0.0);
+        std::vector<bool> dead(k, false);
+        for (int j = 0; j < k; ++j) piv[j] = j;
+        for (int col = 0; col < k; ++col) {
+            int best = col;
+            for (int r = col + 1; r < k; ++r)
+                if (std::fabs(G[(size_t)r * k + col]) > std::fabs(G[(size_t)best * k + col])) best = r;
+            if (!(std::fabs(G[(size_t)best * k + col]) > 1e-14 * tr)) {
+                dead[col] = true;
+                continue;
+            }
+            if (best != col) {
+                for (int q = 0; q < k; ++q) std::swap(G[(size_t)best * k + q], G[(size_t)col * k + q]);
+                std::swap(rhs[best], rhs[col]);
+            }
+            for (int r = col + 1; r < k; ++r) {
+                const double f = G[(size_t)r * k + col] / G[(size_t)col * k + col];
+                for (int q = col; q < k; ++q) G[(size_t)r * k + q] -= f * G[(size_t)col * k + q];
+                rhs[r] -= f * rhs[col];
+            }
+        }
+        for (int r = k - 1; r >= 0; --r) {
+            if (dead[r]) continue;
+            double acc = rhs[r];
+            for (int q = r + 1; q < k; ++q) acc -= G[(size_t)r * k + q] * c[q];
+            c[r] = acc / G[(size_t)r * k + r];
+            if (!std::isfinite(c[r])) c[r] = 0.0;
+        }
+        for (int j = 0; j < k; ++j)
+            if (c[j] != 0.0) {
+                axpy_kernel<<<nb, 256, 0, h->stream>>>(n, c[j], h->d_guess + (size_t)j * n, x);
+                CR_LAUNCH(h, "axpy_kernel");
+            }
+        CR_TRY(op_apply(h, CR_FP64, x, K.r, oc));
+        residual_kernel<<<nb, 256, 0, h->stream>>>(n, b, K.r);
+        CR_LAUNCH(h, "residual_kernel");
+    }
+    if (h->B > 0) {
+        phi_refit_kernel<<<blocks_for((long)h->B * 32, 256), 256, 0, h->stream>>>(h->N, h->B, h->d_body_start,
+                                                                                 h->d_body_members, x, K.r);
+        CR_LAUNCH(h, "phi_refit_kernel");
+    }
+    CR_TRY(norm(h, K.r, rnorm));
+    if (!std::isfinite(*rnorm)) return fail(h, CR_NUMERICAL, "non-finite residual");
+    return CR_OK;
+}
+
 }  // namespace
 
 int krylov_alloc(cr_handle *h) {
@@ -279,6 +370,13 @@ int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {
     CR_TRY(norm(h, K.r, &rnorm));
     if (!std::isfinite(rnorm)) return fail(h, CR_NUMERICAL, "non-finite residual");
     s.initial_residual = bnorm > 0 ? rnorm / bnorm : rnorm;
+    const bool learned = h->user.learned != 0;
+    if (learned) {
+        CR_TRY(learned_start(h, h->user.precision == CR_FP64 ? CR_FP64 : CR_FP32, x, b, oc, &rnorm));
+        s.learned_residual = bnorm > 0 ? rnorm / bnorm : rnorm;
+        // the guess counts as used when it lowered the initial residual
+        s.used_learned_guess = s.learned_residual < 0.999 * s.initial_residual ? 1 : 0;
+    }
     int status = CR_OK;
     if (h->user.precision != CR_MIXED) {
         status = fgmres(h, h->user.precision == CR_FP32 ? CR_FP32 : CR_FP64, x, b, kResidualReady, atol, maxit,
@@ -317,6 +415,7 @@ int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {
         CR_TRY(norm(h, K.w, &rnorm));
     }
     s.final_residual = bnorm > 0 ? rnorm / bnorm : rnorm;
+    h->n_guess = 0;  // directions apply to one solve
     s.converged = rnorm <= atol ? 1 : 0;
     s.matvecs_fp64 = oc.fp64;
     s.matvecs_fp32 = oc.fp32;

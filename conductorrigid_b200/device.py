@@ -178,14 +178,15 @@ class Handle:
                                                     _ptr(bt)), "cr_body_force_torque")
         return bf, bt
 
-    def brownian_step(self, step, radius, force, pos, body_pos, dt=1e-3, kT=1.0, viscosity=1.0, seed=1):
+    def brownian_step(self, step, radius, force, pos, body_pos, dt=1e-3, kT=1.0, viscosity=1.0, seed=1,
+                      repulsion=0.0, contact_gap=0.0):
         """One overdamped rigid-body Brownian step; pos [N, 3] and body_pos [B, 3] (device
         float64 tensors) are moved in place."""
         t = self.torch
         for a in (pos, body_pos):
             if not (isinstance(a, t.Tensor) and a.is_cuda and a.dtype == t.float64 and a.is_contiguous()):
                 raise TypeError("pos and body_pos must be contiguous float64 CUDA tensors (moved in place)")
-        p = _lib.CrBrownianParams(dt, kT, viscosity, seed)
+        p = _lib.CrBrownianParams(dt, kT, viscosity, seed, repulsion, contact_gap)
         radius = self.dev(radius)
         force = self.dev(force).reshape(-1, 3)
         self._check(_lib.lib().cr_brownian_step(self.h, C.byref(p), int(step), _ptr(radius), _ptr(force),

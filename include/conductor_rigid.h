@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define CR_ABI_VERSION 1
+#define CR_ABI_VERSION 2
 
 typedef enum {
     CR_OK = 0,
@@ -102,6 +102,8 @@ typedef struct {
     double initial_residual;  /* ||b - A x0|| / ||b|| */
     double final_residual;    /* true FP64 relative residual ||b - A x|| / ||b|| */
     double solve_ms;          /* device time of the solve (CUDA events) */
+    double learned_residual;  /* with learned = 1: relative residual of the start after the
+                                 guess directions and the potential refit */
 } cr_solve_stats;
 
 typedef struct cr_handle cr_handle;
@@ -207,12 +209,17 @@ int cr_counters(const cr_handle *h, long long *kernel_launches, long long *fft_e
  * mu_r = 1/(8 pi viscosity a_b^3), about the body centre; d_radius[B] holds a_b.  Bead
  * and body positions are wrapped into [-L/2, L/2).  The Gaussian numbers g, g' are a
  * pure function of (seed, step, body): SplitMix64 counters and the Box-Muller
- * transform, so a trajectory does not depend on launch shape or device. */
+ * transform, so a trajectory does not depend on launch shape or device.  The steric
+ * repulsion is added to the body forces (all pairs, minimum image). */
 typedef struct {
     double dt;          /* time step */
     double kT;          /* thermal energy */
     double viscosity;   /* solvent viscosity */
     uint64_t seed;      /* noise stream */
+    double repulsion;   /* stiffness k of the steric body-body repulsion (0: none): a pair
+                           whose centre distance d is below a_i + a_j + contact_gap is pushed
+                           apart along the centre line by k (a_i + a_j + contact_gap - d) */
+    double contact_gap; /* surface gap at which the repulsion starts */
 } cr_brownian_params;
 int cr_body_force_torque(cr_handle *h, const double *d_pos, const double *d_body_pos, const double *d_force,
                          double *d_body_force, double *d_body_torque);
@@ -243,6 +250,43 @@ int cr_mlp_forward(cr_mlp *net, int n, const uint16_t *d_x, float *d_y, void *st
 int cr_mlp_accumulate_grad(cr_mlp *net, int n, const uint16_t *d_x, const float *d_t, double *loss, void *stream);
 int cr_mlp_adam(cr_mlp *net, double lr, double clip, void *stream);
 int cr_mlp_counters(const cr_mlp *net, long long *kernel_launches, long long *adam_steps);
+
+/* ---- learned guess for time stepping ----
+ * No counterpart in the reference (its solve starts from the previous step's charges,
+ * ConductorRigid.cu:1118-1128).  With cr_params.learned = 1 a solve first (1) adds to
+ * its start x0 the combination sum_j c_j D_j of the directions D set by
+ * cr_set_guess_directions that minimises ||b - A x0|| (one operator application per
+ * direction, FP32 in CR_MIXED, then the FP64 residual; a direction that does not help
+ * gets c_j = 0), then (2) refits every body potential to the mean of its bead residuals
+ * (exact, no operator application), and runs the usual solve from there.
+ * cr_solve_stats reports the residual this start reaches and whether it lowered the
+ * initial one.  Directions are [n_dir][N+B] device vectors, used by the next solve
+ * only; passing the previous solution as one of them keeps both it and the zero vector
+ * in reach, so the start is never worse than either.
+ * The helpers build the two directions of the learned guess between time steps from the
+ * previous solution q' at positions (r', R') and the new positions (r, R):
+ *   cr_bead_neighbors   the CR_GUESS_BEAD_NEIGHBORS nearest same-body beads of each bead;
+ *   cr_body_neighbors   the CR_GUESS_BODY_NEIGHBORS nearest bodies of each body (centres);
+ *   cr_guess_features   FP32 features [N][CR_MLP_FEATURES] and the transport term
+ *                       s_i = grad_s q'(r'_i) . (rotation displacement of bead i);
+ *   cr_feature_stats    per-feature sums and sums of squares [2][48] (FP64);
+ *   cr_feature_pack     standardised BF16 rows for the network;
+ *   cr_guess_target     network target (q - q') / scale;
+ *   cr_neutral_direction scale * v minus per-body means (charge rows unchanged), Phi 0. */
+#define CR_GUESS_BEAD_NEIGHBORS 6
+#define CR_GUESS_BODY_NEIGHBORS 8
+#define CR_MAX_GUESS_DIRECTIONS 4
+int cr_set_guess_directions(cr_handle *h, int n_dir, const double *d_dirs);
+int cr_bead_neighbors(cr_handle *h, const double *d_pos, int *d_nbr);
+int cr_body_neighbors(cr_handle *h, const double *d_body_pos, int *d_nbr);
+int cr_guess_features(cr_handle *h, const double *d_radius, const int *d_bead_nbr, const int *d_body_nbr,
+                      const double *d_q_prev, const double *d_pos_prev, const double *d_body_pos_prev,
+                      const double *d_pos, const double *d_body_pos, float *d_feat, double *d_transport);
+int cr_feature_stats(cr_handle *h, int n, const float *d_feat, double *d_sums);
+int cr_feature_pack(cr_handle *h, int n, const float *d_feat, const float *d_mu, const float *d_inv_sigma,
+                    uint16_t *d_x);
+int cr_guess_target(cr_handle *h, const double *d_q, const double *d_q_prev, double scale, float *d_t);
+int cr_neutral_direction(cr_handle *h, const void *d_v, int v_is_fp32, double scale, double *d_dir);
 
 /* ---- spreading without device allocation ----
  * No counterpart in the reference.  For callers that cannot allocate device memory

@@ -65,10 +65,23 @@ def rotation(th):
     return np.eye(3) + np.sin(ang) * K + (1.0 - np.cos(ang)) * (K @ K), ang
 
 
-def brownian_step(pos, body, rigid, body_pos, radius, force, L, step, dt=1e-3, kT=1.0, viscosity=1.0, seed=1):
+def repulsion(body_pos, radius, L, k, gap):
+    """Harmonic steric repulsion force on every body (all pairs, minimum image)."""
+    D = _mimg(body_pos[None, :, :] - body_pos[:, None, :], L)   # D[b, j] = R_j - R_b
+    d = np.linalg.norm(D, axis=-1)
+    reach = radius[:, None] + radius[None, :] + gap
+    on = (d < reach) & (d > 0)
+    mag = np.where(on, k * (reach - d) / np.where(on, d, 1.0), 0.0)
+    return -(mag[..., None] * D).sum(1)
+
+
+def brownian_step(pos, body, rigid, body_pos, radius, force, L, step, dt=1e-3, kT=1.0, viscosity=1.0, seed=1,
+                  k_rep=0.0, gap=0.0):
     """Returns new (pos, body_pos, moves[B, 2] = (|dR|, |dtheta|))."""
     L = np.asarray(L, dtype=np.float64)
     bf, bt = body_force_torque(pos, body, body_pos, force, L)
+    if k_rep > 0:
+        bf = bf + repulsion(body_pos, np.asarray(radius, dtype=np.float64), L, k_rep, gap)
     new_pos = np.empty_like(pos)
     new_bpos = np.empty_like(body_pos)
     moves = np.zeros((len(body_pos), 2))

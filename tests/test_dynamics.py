@@ -25,6 +25,22 @@ def test_counter_normals_statistics():
     assert not np.array_equal(br.normals6(7, 3, 11), br.normals6(8, 3, 11))
 
 
+def test_repulsion_is_pairwise_and_opens_gaps():
+    s = _system()
+    B = s.n_bodies
+    Fr = br.repulsion(s.body_pos, np.ones(B), s.L, 100.0, 0.3)
+    assert np.abs(Fr.sum(0)).max() < 1e-9  # equal and opposite
+    bpos = s.body_pos.copy()
+    pos = s.pos.copy()
+    for step in range(200):
+        pos, bpos, _ = br.brownian_step(pos, s.body, s.rigid, bpos, np.ones(B), np.zeros_like(pos), s.L, step, kT=0.0,
+                                        dt=0.05, k_rep=100.0, gap=0.3)
+    D = _mimg(bpos[None] - bpos[:, None], s.L)
+    d = np.linalg.norm(D, axis=-1) + np.eye(B) * 1e9
+    d0 = np.linalg.norm(_mimg(s.body_pos[None] - s.body_pos[:, None], s.L), axis=-1) + np.eye(B) * 1e9
+    assert d.min() > d0.min()
+
+
 def test_restatement_keeps_bodies_rigid_and_drifts_with_force():
     s = _system()
     B = s.n_bodies
@@ -78,9 +94,11 @@ def test_brownian_steps_match_restatement(cuda, product_lib):
     bpos = torch.tensor(s.body_pos, device="cuda", dtype=torch.float64).contiguous()
     rp, rb = s.pos.copy(), s.body_pos.copy()
     for step in range(4):
-        h.brownian_step(step, radius, F, pos, bpos, dt=2e-3, kT=1.5, viscosity=0.8, seed=11)
+        kr = 300.0 if step % 2 else 0.0  # steric repulsion on every other step
+        h.brownian_step(step, radius, F, pos, bpos, dt=2e-3, kT=1.5, viscosity=0.8, seed=11, repulsion=kr,
+                        contact_gap=0.5)
         rp, rb, _ = br.brownian_step(rp, s.body, s.rigid, rb, radius, F, s.L, step, dt=2e-3, kT=1.5, viscosity=0.8,
-                                     seed=11)
+                                     seed=11, k_rep=kr, gap=0.5)
     assert np.abs(_mimg(pos.cpu().numpy() - rp, s.L)).max() < 1e-11
     assert np.abs(_mimg(bpos.cpu().numpy() - rb, s.L)).max() < 1e-11
     # moved noticeably, stayed rigid
