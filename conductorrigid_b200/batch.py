@@ -1,0 +1,97 @@
+"""Many independent periodic systems of uneven size, solved side by side.
+
+Each replica is a full system with its own handle: box, mesh (2 nodes per unit length,
+rounded up to a 5-smooth size of at most 128), Ewald parameter and topology.  The
+real-space sum takes one image per pair, as the reference's does, so it needs
+rc <= L/2; for boxes smaller than 2 rc the replica's Ewald parameter is raised to
+xi = sqrt(-ln tol)/rc with rc = L/2, which keeps the real-space truncation error at the
+tolerance and moves the rest of the sum to the mesh.
+
+solve_batched() runs all replicas through cr_batch_compute (concurrent streams);
+solve_looped() solves them one after another through cr_compute, the single-system path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib, systems
+from .device import Handle
+
+
+def replica_params(system, tol=1e-5, support=9, gmres_tol=1e-6, restart=50, maxiter=4000, precision="mixed",
+                   precond="conductor", rc_max=4.0):
+    L = float(min(system.L))
+    rc = min(rc_max, 0.5 * L * (1.0 - 1e-12))
+    xi = math.sqrt(-math.log(tol)) / rc
+    grid = tuple(systems.smooth_at_least(int(math.ceil(2.0 * Ld))) for Ld in system.L)
+    return _lib.make_params(field=tuple(system.field), xi=xi, errortol=tol, grid=grid, support=support, rcut=rc,
+                            gmres_tol=gmres_tol, restart=restart, maxiter=maxiter, precision=precision,
+                            precond=precond)
+
+
+class Replicas:
+    def __init__(self, specs, **param_kw):
+        import torch
+
+        self.torch = torch
+        self.systems = []
+        self.handles = []
+        self.arrays = []
+        for sp in specs:
+            s = systems.spheres(np.ones(sp["n_bodies"]), 1, sp["phi"], sp["field"], seed=sp["seed"])
+            h = Handle(replica_params(s, **param_kw), s.L)
+            h.set_topology(s.body, s.rigid, s.body_charge)
+            pos = h.dev(s.pos).reshape(-1, 3).contiguous()
+            bpos = h.dev(s.body_pos).reshape(-1, 3).contiguous()
+            q = torch.zeros(s.n_beads, dtype=torch.float64, device="cuda")
+            phi = torch.zeros(s.n_bodies, dtype=torch.float64, device="cuda")
+            force = torch.zeros(s.n_beads, 3, dtype=torch.float64, device="cuda")
+            self.systems.append(s)
+            self.handles.append(h)
+            self.arrays.append((pos, bpos, q, phi, force))
+        self.n = len(self.handles)
+        self.n_charges = sum(s.n_beads for s in self.systems)
+
+    def reset(self):
+        for (_, _, q, phi, _) in self.arrays:
+            q.zero_()
+            phi.zero_()
+
+    def warm(self):
+        """One solve per replica: allocates every handle's per-solve buffers."""
+        self.reset()
+        self.solve_looped()
+        self.reset()
+
+    def solve_looped(self):
+        stats = []
+        for h, (pos, bpos, q, phi, force) in zip(self.handles, self.arrays):
+            st = _lib.CrSolveStats()
+            code = _lib.lib().cr_compute(h.h, C.c_void_p(pos.data_ptr()), C.c_void_p(bpos.data_ptr()),
+                                         C.c_void_p(q.data_ptr()), C.c_void_p(phi.data_ptr()),
+                                         C.c_void_p(force.data_ptr()), C.byref(st))
+            h._check(code, "cr_compute")
+            stats.append(st.as_dict())
+        self.torch.cuda.synchronize()
+        return stats
+
+    def solve_batched(self, n_threads=16):
+        n = self.n
+        P = C.c_void_p * n
+        hs = P(*[h.h.value for h in self.handles])
+        cols = [P(*[a[k].data_ptr() for a in self.arrays]) for k in range(5)]
+        st = (_lib.CrSolveStats * n)()
+        status = (C.c_int * n)()
+        code = _lib.lib().cr_batch_compute(n, hs, *cols, st, status, int(n_threads))
+        if code != _lib.CR_OK:
+            bad = [i for i in range(n) if status[i] != _lib.CR_OK]
+            raise _lib.CrError(code, "cr_batch_compute", f"replicas {bad[:8]} failed")
+        return [st[i].as_dict() for i in range(n)]
+
+    def close(self):
+        for h in self.handles:
+            h.close()
+        self.handles = []

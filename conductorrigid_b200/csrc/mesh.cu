@@ -19,6 +19,8 @@
 
 #include <type_traits>
 
+#include <mutex>
+
 #include "cr_internal.cuh"
 
 namespace cr {
@@ -357,12 +359,25 @@ template <typename R> size_t contract_smem(const cr_handle *h) {
     return ((size_t)Bd * Bd * Bd + 8 * 6 * (size_t)h->d.support) * sizeof(R);
 }
 
+// The dynamic shared-memory limit is a process-wide attribute of each kernel: it only
+// ever grows (under a lock), so handles with different supports can launch concurrently.
+std::mutex g_smem_mu;
+
 template <typename R, int PT> int set_smem_attrs(cr_handle *h, size_t s1, size_t s2) {
-    CR_CUDA(h, cudaFuncSetAttribute(spread_tiles_kernel<R, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
-    CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, false, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)s2));
-    CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, true, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)s2));
+    static size_t set1 = 0, set2 = 0;
+    std::lock_guard<std::mutex> lk(g_smem_mu);
+    if (s1 > set1) {
+        CR_CUDA(h, cudaFuncSetAttribute(spread_tiles_kernel<R, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)s1));
+        set1 = s1;
+    }
+    if (s2 > set2) {
+        CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, false, PT>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
+        CR_CUDA(h, cudaFuncSetAttribute(contract_tiles_kernel<R, true, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)s2));
+        set2 = s2;
+    }
     return CR_OK;
 }
 

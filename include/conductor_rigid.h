@@ -288,6 +288,19 @@ int cr_feature_pack(cr_handle *h, int n, const float *d_feat, const float *d_mu,
 int cr_guess_target(cr_handle *h, const double *d_q, const double *d_q_prev, double scale, float *d_t);
 int cr_neutral_direction(cr_handle *h, const void *d_v, int v_is_fp32, double scale, double *d_dir);
 
+/* ---- batched independent systems ----
+ * No counterpart in the reference (one system per force compute).  Solves n independent
+ * systems, each through its own handle (its own parameters, box, mesh and topology), as
+ * cr_compute would one by one, but side by side: a pool of n_threads host threads
+ * (<= 0: 16), each with its own non-blocking stream, takes the systems largest first.
+ * status[i] receives each cr_compute status, stats (may be NULL) each solve's
+ * statistics; the return value is the worst status.  Each handle's own stream setting
+ * is restored afterwards.  Call every handle once with cr_compute before batching: its
+ * first solve allocates device memory, which synchronises the device. */
+int cr_batch_compute(int n, cr_handle *const *handles, const double *const *d_pos, const double *const *d_body_pos,
+                     double *const *d_q, double *const *d_phi, double *const *d_force, cr_solve_stats *stats,
+                     int *status, int n_threads);
+
 /* ---- spreading without device allocation ----
  * No counterpart in the reference.  For callers that cannot allocate device memory
  * where they need the charge mesh: a host engine that owns all device memory through
