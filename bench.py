@@ -214,6 +214,91 @@ def run_op_case(args) -> None:
     h.close()
 
 
+def run_replicas(args) -> None:
+    """256 uneven independent replicas: solves/s through cr_batch_compute against looping
+    the single-system solver.  The batch runs on its own streams, so each timed region is
+    bracketed by device synchronisation and CUDA events on the default stream."""
+    import torch
+
+    from conductorrigid_b200 import systems
+    from conductorrigid_b200.batch import Replicas
+
+    R = Replicas(systems.replica_specs(256, seed=1))
+    R.warm()
+
+    def timed(fn):
+        R.reset()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1), st
+
+    for _ in range(args.warmup):
+        timed(lambda: R.solve_batched(16))
+    ms = [timed(lambda: R.solve_batched(16)) for _ in range(args.steps)]
+    ms_loop, st_loop = timed(R.solve_looped)
+    t_batch = statistics.median(m for m, _ in ms)
+    st = ms[-1][1]
+    line = {
+        "metric": "replica solves/s at 1e-6 residual, 256 uneven replicas in one batch",
+        "value": round(R.n / (t_batch / 1e3), 2), "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t_batch, 2), "higher_is_better": True,
+        "looped_solves_per_s": round(R.n / (ms_loop / 1e3), 2),
+        "iterations_mean": round(float(np.mean([s["iterations"] for s in st])), 1),
+        "iterations_max": int(max(s["iterations"] for s in st)),
+        "converged": int(sum(s["converged"] for s in st)), "replicas": R.n, "charges": R.n_charges,
+        "dtype": "f32 operator, f64 Krylov", "data": "synthetic (seeded replica generator)",
+        "config": {"workload": "replicas_256: N_body~U[20,400], phi~U[0.05,0.35], |E0|=1, 2 nodes/unit, P=9"},
+    }
+    R.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_dynamics(args) -> None:
+    """Rigid-body Brownian steps of the 420k-charge suspension: the plain solver warm-started
+    from the previous step against the learned start (network trained online on the first
+    half of the steps), both on one trajectory; per-step device time includes, for the
+    learned arm, the features, network inference and training."""
+    import torch
+
+    from conductorrigid_b200 import _lib, systems
+    from conductorrigid_b200.dynamics import paired_run
+
+    w = systems.workload("dynamics_420k", scale=args.scale)
+    s, p = w.system, w.params
+    grid = p["grid"] if args.scale == 1.0 else systems.smooth_at_least(int(np.ceil(256 * s.L[0] / 49.28)), 4096)
+    common = dict(field=tuple(s.field), xi=p["xi"], errortol=p["errortol"], grid=grid, support=p["support"],
+                  rcut=p["rcut"], gmres_tol=TOL, restart=RESTART, maxiter=20000, precision="mixed",
+                  precond="conductor")
+    steps = args.warmup + args.steps
+    train = min(200, max(1, steps // 2))
+    out, guess = paired_run(_lib.make_params(**common), _lib.make_params(learned=True, **common), s,
+                            np.ones(s.n_bodies), steps, train_solves=train, seed=1)
+    tail = out[max(train + 1, args.warmup):]
+
+    def arm(name):
+        ms = float(np.mean([o[name]["step_ms"] for o in tail]))
+        return {"iterations": round(float(np.mean([o[name]["iterations"] for o in tail])), 1),
+                "ms_per_step": round(ms, 2), "solves_per_s": round(1e3 / ms, 3),
+                "ns_per_day": round(1e3 / ms * 86400 * 1e-3, 1)}
+
+    line = {
+        "metric": "dynamics: GMRES iterations per step and solves/s, learned start vs plain warm start",
+        "value": arm("learned")["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": len(tail),
+        "warmup": len(out) - len(tail), "higher_is_better": True,
+        "learned": arm("learned"), "plain_warm_start": arm("plain"), "trained_solves": guess.trained,
+        "heldout_explained": round(float(np.mean(guess.heldout[-len(tail):])) if guess.heldout else 0.0, 3),
+        "dtype": "f32 operator, f64 Krylov; bf16 network", "data": "synthetic (seeded placement, relaxed)",
+        "config": {"workload": f"dynamics_420k scale {args.scale}: {s.n_bodies} spheres x 42, phi 0.35, "
+                               f"mesh {grid}^3, P=9, dt 1e-3, kT 1, steric repulsion k=1000 gap 0.1",
+                   "ns_per_day_unit": "reduced time units per day (dt = 1e-3)"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -227,8 +312,18 @@ def main() -> None:
                          "applications in FP32 (small enough for a full ncu capture)")
     ap.add_argument("--arms", default="fast,plain,f64c",
                     help="arms to run: fast (headline), plain (reference preconditioner), f64c (FP64 ablation)")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=[WORKLOAD, "replicas_256", "dynamics_420k"],
+                    help="headline solve (default), 256 batched replicas, or Brownian dynamics")
+    ap.add_argument("--scale", type=float, default=1.0, help="dynamics workload: body-count fraction")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.impl == "ours" and args.workload == "replicas_256":
+        run_replicas(args)
+        return
+    if args.impl == "ours" and args.workload == "dynamics_420k":
+        run_dynamics(args)
+        return
     if args.op_case > 0:
         run_op_case(args)
         return

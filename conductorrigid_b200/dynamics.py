@@ -182,11 +182,16 @@ class BrownianRun:
                   contact_gap=contact_gap or 0.1, dt=dt, kT=kT, viscosity=viscosity, seed=seed)
 
     def step(self) -> dict:
+        e0, e1 = self.torch.cuda.Event(enable_timing=True), self.torch.cuda.Event(enable_timing=True)
+        e0.record()
         if self.guess is not None and self.prev is not None:
             self.guess.prepare(self.prev[2], self.prev[0], self.prev[1], self.pos, self.bpos, self.prev[3])
         F, st = self.h.compute(self.pos, self.bpos, self.q, self.phi)
         if self.guess is not None:
             st["train_loss"] = self.guess.learn(self.q)
+        e1.record()
+        e1.synchronize()
+        st["step_ms"] = e0.elapsed_time(e1)  # guess, solve, forces and training (device time)
         self.prev = (self.pos.clone(), self.bpos.clone(), self.q.clone(), self.phi.clone())
         self.h.brownian_step(self.t, self.radius, F, self.pos, self.bpos, dt=self.dt, kT=self.kT,
                              viscosity=self.visc, seed=self.seed, repulsion=self.repulsion,
@@ -219,6 +224,8 @@ def paired_run(params_plain, params_learned, system, radius, steps, *, train_sol
     prev = None
     for k in range(steps):
         pos, bpos = run.pos.clone(), run.bpos.clone()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         if prev is not None:
             k = guess.prepare(prev[2], prev[0], prev[1], pos, bpos, None if mode == "add" else prev[3])
             if mode == "add":
@@ -228,6 +235,9 @@ def paired_run(params_plain, params_learned, system, radius, steps, *, train_sol
                 _lib.lib().cr_set_guess_directions(hl.h, 0, None)
         _, stl = hl.compute(pos, bpos, ql, pl)
         stl["train_loss"] = guess.learn(ql)
+        e1.record()
+        e1.synchronize()
+        stl["step_ms"] = e0.elapsed_time(e1)
         prev = (pos, bpos, ql.clone(), pl.clone())
         stp = run.step()
         out.append({"plain": stp, "learned": stl})
