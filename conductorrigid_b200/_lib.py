@@ -150,6 +150,7 @@ _SIGS = {
     "cr_spread": ([_P, _P, _P, _I], _I),
     "cr_apply_M": ([_P, _P, _P, _I], _I),
     "cr_forces": ([_P, _P, _P, _I], _I),
+    "cr_energy": ([_P, _P, C.POINTER(C.c_double)], _I),
     "cr_neighbor_list": ([_P, C.c_double, _P, _P, _P, C.c_int64, C.POINTER(C.c_int64)], _I),
     "cr_profile": ([_P, _I], _I),
     "cr_profile_read": ([_P, _I, C.POINTER(C.c_int), C.POINTER(C.c_double)], _I),

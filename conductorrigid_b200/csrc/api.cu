@@ -160,6 +160,23 @@ template <typename R> int wave_out(cr_handle *h, MeshBuffers<R> &m, const double
 
 using namespace cr;
 
+namespace cr {
+// out += sum_i a_i b_i / 2 (FP64; one atomic per block)
+__global__ void half_dot_kernel(int n, const double *__restrict__ a, const double *__restrict__ b, double *out) {
+    __shared__ double red[8];
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        atomicAdd(out, 0.5 * t);
+    }
+}
+}  // namespace cr
+
 extern "C" {
 
 int cr_abi_version(void) { return CR_ABI_VERSION; }
@@ -356,6 +373,24 @@ int cr_spread(cr_handle *h, const double *d_q, double *d_grid, int precision) {
         CR_TRY(cast_to_double(h, h->m32.grid, d_grid, G));
     }
     return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_spread");
+}
+
+
+// Electrostatic energy of the bead charges, U = 1/2 q.(M q), with M the periodic
+// (Ewald-split) shell interaction of the current positions, FP64.
+int cr_energy(cr_handle *h, const double *d_q, double *energy) {
+    CR_TRY(need_geometry(h));
+    if (!energy) return fail(h, CR_BAD_PARAM, "null output");
+    *energy = 0.0;
+    if (h->N == 0) return CR_OK;
+    if (!d_q) return fail(h, CR_BAD_PARAM, "null vector");
+    CR_TRY(cr_apply_M(h, d_q, h->d_tmp_n, CR_FP64));
+    CR_CUDA(h, cudaMemsetAsync(h->d_tmp_n2, 0, sizeof(double), h->stream));
+    cr::half_dot_kernel<<<std::min(4 * 148, blocks_for(h->N, 256)), 256, 0, h->stream>>>(h->N, d_q, h->d_tmp_n,
+                                                                                     h->d_tmp_n2);
+    CR_LAUNCH(h, "half_dot_kernel");
+    CR_CUDA(h, cudaMemcpyAsync(energy, h->d_tmp_n2, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_energy");
 }
 
 int cr_apply_M(cr_handle *h, const double *d_q, double *d_Mq, int precision) {

@@ -132,6 +132,13 @@ class Handle:
         self._check(_lib.lib().cr_forces(self.h, _ptr(q), _ptr(f), int(precision)), "cr_forces")
         return f
 
+    def energy(self, q) -> float:
+        """1/2 q.(M q) at the current positions (FP64)."""
+        q = self.dev(q)
+        u = C.c_double(0.0)
+        self._check(_lib.lib().cr_energy(self.h, _ptr(q), C.byref(u)), "cr_energy")
+        return u.value
+
     def neighbor_list(self, r_list: float):
         t = self.torch
         count = t.empty(self.N, dtype=t.int32, device="cuda")

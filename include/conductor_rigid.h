@@ -166,6 +166,10 @@ int cr_spread(cr_handle *h, const double *d_q, double *d_grid, int precision);
 /* M q = wave + self + real-space potential (PotentialChargeMultiply without the
  * Phi_b subtraction, ConductorRigid.cu:862-946). */
 int cr_apply_M(cr_handle *h, const double *d_q, double *d_Mq, int precision);
+/* Electrostatic energy U = 1/2 q.(M q) of bead charges d_q[N] at the positions of the
+ * last cr_set_positions / cr_compute (FP64).  Not computed by the reference, whose force
+ * pass leaves the energy slot at zero (ConductorRigid.cu:464,661). */
+int cr_energy(cr_handle *h, const double *d_q, double *energy);
 /* Bead forces for charges q (force pass, ConductorRigid.cu:1256-1278). */
 int cr_forces(cr_handle *h, const double *d_q, double *d_force, int precision);
 /* Full neighbour list within r_list of the current positions (the pair set of the
