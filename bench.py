@@ -299,6 +299,61 @@ def run_dynamics(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_mlp(args) -> None:
+    """The learned part's tensor-core kernels at the dynamics size (one row per bead,
+    420,000 rows): inference and one training step (forward, backward, weight gradients;
+    the Adam update is timed with it).  FLOPs per row: 2 * (48*128 + 128*128 + 128) in the
+    forward, and 2 * (128*128) + 2 * (128*128 + 128) + 2 * (48*128 + 48) more in the
+    backward (dH1, dW2 with db2, dW1 with db1), the MMA work the kernels issue."""
+    import torch
+
+    from conductorrigid_b200.learned import FEATURES, Network
+
+    n = 420_000
+    net = Network(seed=1)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.randn(n, FEATURES, device="cuda", generator=g).to(torch.bfloat16).view(torch.int16).contiguous()
+    t = torch.randn(n, device="cuda", generator=g)
+    f_fwd = 2.0 * (48 * 128 + 128 * 128 + 128)
+    f_bwd = 2.0 * (128 * 128) + 2.0 * (128 * 128 + 128) + 2.0 * (48 * 128 + 48)
+    pf = ROOT / "MEASURED_PEAKS.json"
+    peak, peak_src = (float(json.loads(pf.read_text())["bf16_tflops"]), "measured bf16 burst") if pf.exists() \
+        else (1590.0, "fallback bf16 burst")
+
+    def timed(fn, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(k):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    for _ in range(args.warmup):
+        net.forward(x)
+        net.train_step(x, t)
+    c0 = net.counters()["kernel_launches"]
+    ms_f = timed(lambda: net.forward(x), args.steps)
+    ms_t = timed(lambda: net.train_step(x, t), args.steps)
+    launches = net.counters()["kernel_launches"] - c0
+    tf_f = n * f_fwd / (ms_f * 1e-3) / 1e12
+    tf_t = n * (f_fwd + f_bwd) / (ms_t * 1e-3) / 1e12
+    line = {
+        "metric": "per-bead network on tcgen05: rows/s and TFLOP/s (inference, training step)",
+        "value": round(n / (ms_t * 1e-3), 1), "unit": "training rows/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "dtype": "bf16 operands, f32 accumulate",
+        "data": "synthetic normal features", "rows": n,
+        "inference": {"ms": round(ms_f, 4), "tflops": round(tf_f, 2)},
+        "training_step": {"ms": round(ms_t, 4), "tflops": round(tf_t, 2)},
+        "roofline": {"bound": "tensor", "achieved": round(tf_t, 2), "peak": peak, "unit": "TFLOP/s",
+                     "frac": round(tf_t / peak, 4), "peak_source": peak_src},
+        "gpu_launches": launches,
+        "config": {"workload": "mlp_420k: 48-128-128-1 GELU network, one row per bead of the 420k-charge system"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -313,7 +368,7 @@ def main() -> None:
     ap.add_argument("--arms", default="fast,plain,f64c",
                     help="arms to run: fast (headline), plain (reference preconditioner), f64c (FP64 ablation)")
     ap.add_argument("--workload", default=WORKLOAD,
-                    choices=[WORKLOAD, "replicas_256", "dynamics_420k"],
+                    choices=[WORKLOAD, "replicas_256", "dynamics_420k", "mlp"],
                     help="headline solve (default), 256 batched replicas, or Brownian dynamics")
     ap.add_argument("--scale", type=float, default=1.0, help="dynamics workload: body-count fraction")
     args = ap.parse_args()
@@ -323,6 +378,9 @@ def main() -> None:
         return
     if args.impl == "ours" and args.workload == "dynamics_420k":
         run_dynamics(args)
+        return
+    if args.impl == "ours" and args.workload == "mlp":
+        run_mlp(args)
         return
     if args.op_case > 0:
         run_op_case(args)
