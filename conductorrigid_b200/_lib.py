@@ -140,6 +140,10 @@ _SIGS = {
     "cr_set_params": ([_P, C.POINTER(CrParams), _D], _I),
     "cr_set_topology": ([_P, _I, C.POINTER(C.c_uint32), _I, C.POINTER(C.c_uint8), _D], _I),
     "cr_set_stream": ([_P, _P], _I),
+    "cr_set_graphs": ([_P, _I], _I),
+    "cr_set_tiling": ([_P, _I, _I], _I),
+    "cr_autotune": ([_P, _P, _P, _I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)], _I),
+    "cr_graph_launches": ([_P, C.POINTER(C.c_longlong)], _I),
     "cr_compute": ([_P, _P, _P, _P, _P, _P, C.POINTER(CrSolveStats)], _I),
     "cr_compute_host": ([_P, _D, _D, _D, _D, _D, C.POINTER(CrSolveStats)], _I),
     "cr_set_positions": ([_P, _P, _P], _I),

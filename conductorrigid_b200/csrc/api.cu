@@ -101,8 +101,9 @@ int derive(cr_handle *h, const cr_params *p, const double L[3]) {
     h->h_phiq.assign(2 * (size_t)nt, 0.0);
     h->h_gradphiq.assign(2 * (size_t)nt, 0.0);
     cr_build_tables(&d, p->xi, h->h_phiq.data(), h->h_gradphiq.data());
-    // tiles of 8^3 nodes (fewer along short dimensions)
+    // tiles of 8^3 nodes (fewer along short dimensions); cr_autotune may change this
     h->tile = 8;
+    h->spread_mode = 0;
     h->ntiles = 1;
     for (int k = 0; k < 3; ++k) {
         h->ntiles_dim[k] = (d.grid[k] + h->tile - 1) / h->tile;
@@ -269,6 +270,72 @@ int cr_set_params(cr_handle *h, const cr_params *p, const double L[3]) {
 int cr_set_stream(cr_handle *h, void *stream) {
     if (!h) return CR_BAD_PARAM;
     h->stream = (cudaStream_t)stream;
+    return CR_OK;
+}
+
+int cr_set_tiling(cr_handle *h, int tile_edge, int spread_mode) {
+    CR_TRY(need_ready(h));
+    if (spread_mode < 0 || spread_mode > 1) return fail(h, CR_BAD_PARAM, "spread mode must be 0 or 1");
+    if (h->stream) CR_CUDA(h, cudaStreamSynchronize(h->stream));
+    CR_TRY(mesh_set_tile(h, tile_edge));
+    h->spread_mode = spread_mode;
+    return CR_OK;
+}
+
+// Time the FP32 mesh path (spread, FFT, influence function, FFT, contract) of the given
+// positions for every valid tiling and keep the fastest.
+int cr_autotune(cr_handle *h, const double *d_pos, const double *d_body_pos, int reps, int *tile_edge,
+                int *spread_mode, float *best_ms) {
+    CR_TRY(need_ready(h));
+    if (h->N > 0 && !d_pos) return fail(h, CR_BAD_PARAM, "null positions");
+    if (h->B > 0 && !d_body_pos) return fail(h, CR_BAD_PARAM, "null body positions");
+    reps = std::max(1, reps);
+    const bool compiled = h->d.support == 9 || h->d.support == 11;
+    const int edges[] = {4, 6, 8, 12, 16};
+    int best_t = h->tile, best_m = h->spread_mode;
+    float best = 3.4e38f;
+    if (h->N > 0) {
+        for (int t : edges) {
+            for (int mode = 0; mode < 2; ++mode) {
+                if (mode == 0 && !(t == 8 && compiled)) continue;  // register columns exist for T = 8 only
+                if (mesh_set_tile(h, t) != CR_OK) continue;             // too large for shared memory
+                h->spread_mode = mode;
+                CR_TRY(geometry_update(h, d_pos, d_body_pos));
+                CR_TRY(cast_charges(h, h->m32, d_pos));                 // any charges will do for timing
+                CR_TRY(wave_potential(h, h->m32));
+                CR_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+                for (int r = 0; r < reps; ++r) CR_TRY(wave_potential(h, h->m32));
+                CR_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+                CR_CUDA(h, cudaEventSynchronize(h->ev1));
+                float ms = 0.f;
+                CR_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+                ms /= reps;
+                if (ms < best) {
+                    best = ms;
+                    best_t = t;
+                    best_m = mode;
+                }
+            }
+        }
+    }
+    CR_TRY(mesh_set_tile(h, best_t));
+    h->spread_mode = best_m;
+    CR_TRY(geometry_update(h, d_pos, d_body_pos));
+    if (tile_edge) *tile_edge = best_t;
+    if (spread_mode) *spread_mode = best_m;
+    if (best_ms) *best_ms = h->N > 0 ? best : 0.f;
+    return CR_OK;
+}
+
+int cr_set_graphs(cr_handle *h, int enable) {
+    if (!h) return CR_BAD_PARAM;
+    h->use_graphs = enable ? 1 : 0;
+    return CR_OK;
+}
+
+int cr_graph_launches(const cr_handle *h, long long *launches) {
+    if (!h || !launches) return CR_BAD_PARAM;
+    *launches = h->graph_launches;
     return CR_OK;
 }
 

@@ -118,6 +118,17 @@ struct Krylov {
     double *yvec = nullptr;     // [m] least-squares coefficients
     double *h_pinned = nullptr; // pinned host mirror of hcol
     int nblocks = 0;
+    // captured Arnoldi step (CUDA graph): device-side Hessenberg bookkeeping
+    double *H = nullptr;        // [(m+1) * m] row-major Hessenberg, rotated in place
+    double *cs = nullptr, *sn = nullptr;  // [m] Givens rotations
+    double *g = nullptr;        // [m+1] rotated right-hand side
+    double *sin = nullptr, *sz = nullptr; // [n] staging of V_j and Z_j (fixed addresses for the graph)
+    int *state = nullptr;       // device ArnoldiState
+    void *h_state = nullptr;    // pinned mirror of ArnoldiState
+    double *h_hg = nullptr;     // pinned [(m+1)*m + (m+1)]: H and g at the end of a cycle
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};  // per operator precision (FP64, FP32)
+    long long exec_gen[2] = {-1, -1};              // geometry generation captured
+    long long exec_kernels[2] = {0, 0}, exec_ffts[2] = {0, 0};  // work per launch
 };
 
 // Conductor-response preconditioner: one K^-1 per distinct body shape.
@@ -184,6 +195,7 @@ struct cr_handle {
 
     // mesh tiling
     int tile = 8;                     // tile edge in nodes
+    int spread_mode = 0;              // 0: register columns where compiled (T = 8, P = 9/11); 1: shared atomics
     int ntiles_dim[3] = {0, 0, 0};
     int ntiles = 0;
 
@@ -209,6 +221,10 @@ struct cr_handle {
     double *d_io_pos = nullptr, *d_io_bpos = nullptr, *d_io_q = nullptr, *d_io_phi = nullptr, *d_io_force = nullptr;
     // rigid-body stepper: body force and torque, per-body move sizes
     double *d_bf = nullptr, *d_bt = nullptr, *d_moves = nullptr;
+    // solver graphs: capture one Arnoldi step per geometry when a stream is set
+    int use_graphs = 1;
+    long long geo_gen = 0;
+    long long graph_launches = 0;
     // learned guess: caller directions for the next solve [CR_MAX_GUESS_DIRECTIONS][N+B]
     double *d_guess = nullptr;
     int n_guess = 0;
@@ -292,6 +308,8 @@ int realspace_alloc(cr_handle *h);
 void realspace_free(cr_handle *h);
 // Clusters and cluster pairs of the current positions.
 int realspace_build(cr_handle *h);
+int realspace_prepare(cr_handle *h, int precision);
+int mesh_set_tile(cr_handle *h, int T);
 int neighbor_list_build(cr_handle *h, double r_list, int *d_count, int64_t *d_head, int *d_list,
                         int64_t capacity, int64_t *total);
 // Body rows y[N+b] = sum_{i in b} x_i (FP64).

@@ -360,6 +360,7 @@ int geometry_update(cr_handle *h, const double *d_pos, const double *d_body_pos)
     Geometry &g = h->geo;
     const int N = h->N;
     g.valid = false;
+    ++h->geo_gen;  // captured solver graphs refer to this geometry's sizes
     CellGrid cg = make_cell_grid(h, h->d.rcut);
     PrepArgs a;
     a.N = N;

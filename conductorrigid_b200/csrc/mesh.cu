@@ -19,6 +19,7 @@
 
 #include <type_traits>
 
+#include <algorithm>
 #include <mutex>
 
 #include "cr_internal.cuh"
@@ -476,8 +477,8 @@ template <typename R> int spread_only(cr_handle *h, MeshBuffers<R> &m) {
     CR_CUDA(h, cudaMemsetAsync(m.grid, 0, G * sizeof(R), h->stream));
     CR_TRY(with_support<R>(h, [&](auto pt) -> int {
         constexpr int PT = decltype(pt)::value;
-        if (PT == 0) {
-            spread_tiles_kernel<R, 0><<<h->ntiles, 256, spread_smem<R>(h), h->stream>>>(
+        if (PT == 0 || h->spread_mode == 1) {
+            spread_tiles_kernel<R, PT><<<h->ntiles, 256, spread_smem<R>(h), h->stream>>>(
                 m.pos, m.q, h->geo.wstart, h->geo.tile_start, h->geo.tile_beads, mesh_shape<R>(h),
                 window_const<R>(h), (R)h->d.prefac, m.grid);
         } else {
@@ -538,6 +539,30 @@ template <typename R> int wave_force(cr_handle *h, MeshBuffers<R> &m) {
         CR_LAUNCH(h, "contract_force_tiles_kernel");
         return CR_OK;
     }));
+    return CR_OK;
+}
+
+// Tile edge T for both precisions: tile counts, the shared-memory limits of the tile
+// kernels, and the tile-sized geometry buffers (the geometry must be rebuilt after).
+int mesh_set_tile(cr_handle *h, int T) {
+    if (T < 2 || T > 32) return fail(h, CR_BAD_PARAM, "tile edge out of range");
+    const int saved = h->tile;
+    h->tile = T;
+    const size_t s1f = spread_smem<float>(h), s2f = contract_smem<float>(h);
+    const size_t s1d = spread_smem<double>(h), s2d = contract_smem<double>(h);
+    if (std::max(std::max(s1f, s2f), std::max(s1d, s2d)) > 227 * 1024) {
+        h->tile = saved;
+        return fail(h, CR_BAD_PARAM, "tile edge too large for the shared-memory tile buffer");
+    }
+    h->ntiles = 1;
+    for (int k = 0; k < 3; ++k) {
+        h->ntiles_dim[k] = (h->d.grid[k] + T - 1) / T;
+        h->ntiles *= h->ntiles_dim[k];
+    }
+    CR_TRY((set_smem_attrs<float, 0>(h, s1f, s2f)));
+    CR_TRY((set_smem_attrs<double, 0>(h, s1d, s2d)));
+    h->geo.valid = false;
+    if (h->have_topology) CR_TRY(geometry_alloc(h));
     return CR_OK;
 }
 

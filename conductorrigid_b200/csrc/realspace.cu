@@ -435,6 +435,12 @@ template <typename R> int realspace_blocks(cr_handle *h) {
 
 }  // namespace
 
+// Build the stored values of the given operator precision for the current geometry now
+// (the operator otherwise builds them on its first application).
+int realspace_prepare(cr_handle *h, int precision) {
+    return precision == CR_FP64 ? realspace_blocks<double>(h) : realspace_blocks<float>(h);
+}
+
 void realspace_free(cr_handle *h) {
     RealSpace &r = h->rs;
     dfree(&r.members);

@@ -14,7 +14,10 @@
 //     FP64 iterative refinement: r = b - A64 x, solve A32 d ~= r, x += d.
 // All vectors stay on the device; each Arnoldi step copies its j+2 Hessenberg
 // entries to pinned host memory for the Givens update (one small copy per step).
+#include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <vector>
 
 #include "cr_internal.cuh"
 
@@ -89,6 +92,150 @@ __global__ void axpy_kernel(int n, double a, const double *__restrict__ x, doubl
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
 }
 
+// ---- captured Arnoldi step --------------------------------------------------------
+// With a stream set and the profiler off, one Arnoldi step is captured once per geometry
+// as a CUDA graph and launched once per iteration.  Everything that depends on the
+// column index lives in device memory (ArnoldiState), so one graph serves every step:
+// V_j and Z_j pass through fixed staging vectors, the dot/projection kernels read their
+// length from the state, and the Hessenberg column, the Givens rotations and the
+// stopping test run in a one-thread kernel.  The last node copies the state to pinned
+// host memory, which the host reads after each launch to stop exactly where the eager
+// loop would.
+struct ArnoldiState {
+    int j;          // columns completed in this cycle
+    int stop;       // 1: the last column met the tolerance or broke down; 2: non-finite norm
+    int frozen;     // set once a stopping column is counted: later launches change nothing
+    int pad;
+    double res;     // |g[j]| after the last counted column
+    double inv_hn;  // 1 / ||w|| of the column being added
+    double atol;    // absolute tolerance of this cycle
+};
+
+__global__ void init_cycle_kernel(int m, double beta, double atol, ArnoldiState *st, double *__restrict__ g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= m) g[i] = i == 0 ? beta : 0.0;
+    if (i == 0) {
+        st->j = 0;
+        st->stop = 0;
+        st->frozen = 0;
+        st->pad = 0;
+        st->res = beta;
+        st->inv_hn = 0.0;
+        st->atol = atol;
+    }
+}
+
+__global__ void gather_col_kernel(int n, const double *__restrict__ base, const ArnoldiState *st,
+                                  double *__restrict__ dst) {
+    const size_t off = (size_t)st->j * n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = base[off + i];
+}
+
+__global__ void scatter_col_kernel(int n, int m, const double *__restrict__ src, const ArnoldiState *st,
+                                   double *__restrict__ base) {
+    const int j = st->j;
+    if (j >= m) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        base[(size_t)j * n + i] = src[i];
+}
+
+// multi_dot_kernel with k = j + 1 read from the state (at most kmax)
+__global__ void __launch_bounds__(kDotThreads) multi_dot_dev_kernel(int n, int kmax, const ArnoldiState *st,
+                                                                    const double *__restrict__ V,
+                                                                    const double *__restrict__ w,
+                                                                    double *__restrict__ partial) {
+    __shared__ double red[kDotThreads / 32];
+    const int k = min(st->j + 1, kmax);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = 0; j < k; ++j) {
+        const double *v = V + (size_t)j * n;
+        double s = 0.0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += v[i] * w[i];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) red[warp] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int q = 0; q < kDotThreads / 32; ++q) t += red[q];
+            partial[(size_t)blockIdx.x * kmax + j] = t;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void reduce_partials_dev_kernel(int nblk, int kmax, const ArnoldiState *st,
+                                           const double *__restrict__ partial, double *__restrict__ out) {
+    const int j = blockIdx.x;
+    if (j >= min(st->j + 1, kmax)) return;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += 32) s += partial[(size_t)b * kmax + j];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) out[j] = s;
+}
+
+__global__ void project_dev_kernel(int n, int kmax, const ArnoldiState *st, const double *__restrict__ V,
+                                   const double *__restrict__ hv, double *__restrict__ w) {
+    const int k = min(st->j + 1, kmax);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = w[i];
+        for (int j = 0; j < k; ++j) s -= hv[j] * V[(size_t)j * n + i];
+        w[i] = s;
+    }
+}
+
+// The host loop's Hessenberg update for column j, on the device (one thread).
+__global__ void arnoldi_column_kernel(int m, ArnoldiState *st, const double *__restrict__ hcol, double *__restrict__ H,
+                                      double *__restrict__ cs, double *__restrict__ sn, double *__restrict__ g) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    st->inv_hn = 0.0;
+    if (st->frozen) return;
+    const int j = st->j;
+    if (j >= m) return;
+    const double *h1 = hcol, *h2 = hcol + (m + 1);
+    const double hn = sqrt(fmax(0.0, hcol[2 * (m + 1)]));
+    if (!isfinite(hn)) {
+        st->stop = 2;
+        return;
+    }
+    for (int k = 0; k <= j; ++k) H[(size_t)k * m + j] = h1[k] + h2[k];
+    H[(size_t)(j + 1) * m + j] = hn;
+    for (int k = 0; k < j; ++k) {
+        const double a = H[(size_t)k * m + j], c = H[(size_t)(k + 1) * m + j];
+        H[(size_t)k * m + j] = cs[k] * a + sn[k] * c;
+        H[(size_t)(k + 1) * m + j] = -sn[k] * a + cs[k] * c;
+    }
+    const double a = H[(size_t)j * m + j], c = H[(size_t)(j + 1) * m + j];
+    const double den = hypot(a, c);
+    cs[j] = den > 0 ? a / den : 1.0;
+    sn[j] = den > 0 ? c / den : 0.0;
+    H[(size_t)j * m + j] = den;
+    H[(size_t)(j + 1) * m + j] = 0.0;
+    g[j + 1] = -sn[j] * g[j];
+    g[j] = cs[j] * g[j];
+    st->res = fabs(g[j + 1]);
+    st->inv_hn = hn > 0 ? 1.0 / hn : 0.0;
+    if (fabs(g[j + 1]) <= st->atol || hn == 0.0) st->stop = 1;
+}
+
+__global__ void scale_next_kernel(int n, int m, const ArnoldiState *st, const double *__restrict__ w,
+                                  double *__restrict__ V) {
+    const int j = st->j;
+    const double a = st->inv_hn;
+    if (st->frozen || j >= m || a == 0.0) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        V[(size_t)(j + 1) * n + i] = a * w[i];
+}
+
+__global__ void advance_kernel(int m, ArnoldiState *st) {
+    if (blockIdx.x != 0 || threadIdx.x != 0 || st->frozen) return;
+    if (st->stop == 2) {
+        st->frozen = 1;
+        return;
+    }
+    st->j += 1;
+    if (st->stop || st->j >= m) st->frozen = 1;
+}
+
 // Learned-guess refit of the body potentials: Phi_b += mean of the bead residuals of
 // body b, which zeroes that mean (a bead row is Phi_b - (M q)_i = b_i; the charge rows
 // do not involve Phi).  Exact, no operator application.
@@ -138,6 +285,122 @@ int op_apply(cr_handle *h, int precision, const double *x, double *y, OpCount &o
     return apply_operator(h, x, y, precision);
 }
 
+bool graph_mode(const cr_handle *h) { return h->use_graphs && h->stream != nullptr && !h->prof.on; }
+
+// The kernels of one Arnoldi step on the device state (recorded into a graph).
+int record_step(cr_handle *h, int precision) {
+    Krylov &K = h->kry;
+    const int n = K.n, m = K.m, nb = vec_blocks(n);
+    cudaStream_t s = h->stream;
+    ArnoldiState *st = reinterpret_cast<ArnoldiState *>(K.state);
+    OpCount none;
+    gather_col_kernel<<<nb, 256, 0, s>>>(n, K.V, st, K.sin);
+    CR_LAUNCH(h, "gather_col_kernel");
+    CR_TRY(precondition(h, K.sin, K.sz));
+    scatter_col_kernel<<<nb, 256, 0, s>>>(n, m, K.sz, st, K.Z);
+    CR_LAUNCH(h, "scatter_col_kernel");
+    CR_TRY(op_apply(h, precision, K.sz, K.w, none));
+    for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+        double *hv = K.hcol + (size_t)pass * (m + 1);
+        multi_dot_dev_kernel<<<K.nblocks, kDotThreads, 0, s>>>(n, m + 1, st, K.V, K.w, K.partial);
+        CR_LAUNCH(h, "multi_dot_dev_kernel");
+        reduce_partials_dev_kernel<<<m + 1, 32, 0, s>>>(K.nblocks, m + 1, st, K.partial, hv);
+        CR_LAUNCH(h, "reduce_partials_dev_kernel");
+        project_dev_kernel<<<nb, 256, 0, s>>>(n, m + 1, st, K.V, hv, K.w);
+        CR_LAUNCH(h, "project_dev_kernel");
+    }
+    CR_TRY(dots(h, 1, K.w, K.w, K.hcol + 2 * (m + 1)));
+    arnoldi_column_kernel<<<1, 32, 0, s>>>(m, st, K.hcol, K.H, K.cs, K.sn, K.g);
+    CR_LAUNCH(h, "arnoldi_column_kernel");
+    scale_next_kernel<<<nb, 256, 0, s>>>(n, m, st, K.w, K.V);
+    CR_LAUNCH(h, "scale_next_kernel");
+    advance_kernel<<<1, 32, 0, s>>>(m, st);
+    CR_LAUNCH(h, "advance_kernel");
+    CR_CUDA(h, cudaMemcpyAsync(K.h_state, K.state, sizeof(ArnoldiState), cudaMemcpyDeviceToHost, s));
+    return CR_OK;
+}
+
+// Capture the step for this geometry and operator precision (once per geometry; an
+// existing executable graph is updated in place when the topology allows).
+int capture_step(cr_handle *h, int precision) {
+    Krylov &K = h->kry;
+    const int slot = precision == CR_FP64 ? 0 : 1;
+    if (K.exec[slot] && K.exec_gen[slot] == h->geo_gen) return CR_OK;
+    CR_TRY(realspace_prepare(h, precision));  // allocations and one-off work stay outside the graph
+    const long long l0 = h->launches, f0 = h->fft_execs;
+    CR_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = record_step(h, precision);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    K.exec_kernels[slot] = h->launches - l0;
+    K.exec_ffts[slot] = h->fft_execs - f0;
+    h->launches = l0;  // nothing ran yet
+    h->fft_execs = f0;
+    if (st != CR_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return st != CR_OK ? st : fail(h, CR_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
+    }
+    if (K.exec[slot]) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(K.exec[slot], graph, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(K.exec[slot]);
+            K.exec[slot] = nullptr;
+        }
+    }
+    if (!K.exec[slot]) {
+        const cudaError_t ei = cudaGraphInstantiate(&K.exec[slot], graph, 0);
+        if (ei != cudaSuccess) {
+            K.exec[slot] = nullptr;
+            cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return fail(h, CR_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        }
+    }
+    cudaGraphDestroy(graph);
+    K.exec_gen[slot] = h->geo_gen;
+    return CR_OK;
+}
+
+// One Arnoldi cycle by graph launches: at most min(m, budget) steps, stopping where the
+// host loop would.  On return H and g hold the cycle's rotated Hessenberg and
+// right-hand side, *cols the columns completed.
+int cycle_graph(cr_handle *h, int precision, double beta, double atol, int budget, OpCount &oc, int *cols,
+                std::vector<double> &H, std::vector<double> &g) {
+    Krylov &K = h->kry;
+    const int m = K.m;
+    const int slot = precision == CR_FP64 ? 0 : 1;
+    CR_TRY(capture_step(h, precision));
+    init_cycle_kernel<<<blocks_for(m + 1, 128), 128, 0, h->stream>>>(m, beta, atol,
+                                                                     reinterpret_cast<ArnoldiState *>(K.state), K.g);
+    CR_LAUNCH(h, "init_cycle_kernel");
+    const ArnoldiState *hs = reinterpret_cast<const ArnoldiState *>(K.h_state);
+    int launched = 0;
+    while (launched < m && launched < budget) {
+        CR_CUDA(h, cudaGraphLaunch(K.exec[slot], h->stream));
+        ++launched;
+        ++h->graph_launches;
+        h->launches += K.exec_kernels[slot];
+        h->fft_execs += K.exec_ffts[slot];
+        if (precision == CR_FP64) ++oc.fp64;
+        else ++oc.fp32;
+        CR_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (hs->frozen) break;
+    }
+    if (hs->stop == 2) return fail(h, CR_NUMERICAL, "non-finite Arnoldi norm");
+    const int j = hs->j;
+    CR_CUDA(h, cudaMemcpyAsync(K.h_hg, K.H, (size_t)(m + 1) * m * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->stream));
+    CR_CUDA(h, cudaMemcpyAsync(K.h_hg + (size_t)(m + 1) * m, K.g, (m + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->stream));
+    CR_CUDA(h, cudaStreamSynchronize(h->stream));
+    std::copy(K.h_hg, K.h_hg + (size_t)(m + 1) * m, H.begin());
+    std::copy(K.h_hg + (size_t)(m + 1) * m, K.h_hg + (size_t)(m + 1) * m + (m + 1), g.begin());
+    *cols = j;
+    return CR_OK;
+}
+
 // Restarted right-preconditioned FGMRES(m) on A_prec x = b with absolute tolerance
 // `atol` on ||b - A_prec x||.  x holds the initial guess.  Returns CR_OK or
 // CR_NOT_CONVERGED; *iters accumulates iterations, *restarts restart cycles.
@@ -168,6 +431,11 @@ int fgmres(cr_handle *h, int precision, double *x, const double *b, int r_mode, 
         g[0] = beta;
         int j = 0;
         bool stop = false;
+        if (graph_mode(h)) {
+            CR_TRY(cycle_graph(h, precision, beta, atol, maxit - it, oc, &j, H, g));
+            it += j;
+            stop = true;  // the eager loop below is skipped
+        }
         for (; j < m && it < maxit && !stop; ++j) {
             double *vj = K.V + (size_t)j * n;
             double *zj = K.Z + (size_t)j * n;
@@ -331,6 +599,16 @@ int krylov_alloc(cr_handle *h) {
     CR_TRY(dalloc(h, &K.hcol, 3 * (m + 1)));
     CR_TRY(dalloc(h, &K.yvec, m));
     CR_CUDA(h, cudaMallocHost((void **)&K.h_pinned, 3 * (m + 1) * sizeof(double)));
+    CR_TRY(dalloc(h, &K.H, (m + 1) * m));
+    CR_TRY(dalloc(h, &K.cs, m));
+    CR_TRY(dalloc(h, &K.sn, m));
+    CR_TRY(dalloc(h, &K.g, m + 1));
+    CR_TRY(dalloc(h, &K.sin, n));
+    CR_TRY(dalloc(h, &K.sz, n));
+    CR_TRY(dalloc(h, &K.state, (sizeof(ArnoldiState) + sizeof(int) - 1) / sizeof(int)));
+    CR_CUDA(h, cudaMallocHost(&K.h_state, sizeof(ArnoldiState)));
+    CR_CUDA(h, cudaMallocHost((void **)&K.h_hg, ((m + 1) * m + (m + 1)) * sizeof(double)));
+    std::memset(K.h_state, 0, sizeof(ArnoldiState));
     return CR_OK;
 }
 
@@ -349,6 +627,22 @@ void krylov_free(cr_handle *h) {
     dfree(&K.yvec);
     if (K.h_pinned) cudaFreeHost(K.h_pinned);
     K.h_pinned = nullptr;
+    dfree(&K.H);
+    dfree(&K.cs);
+    dfree(&K.sn);
+    dfree(&K.g);
+    dfree(&K.sin);
+    dfree(&K.sz);
+    dfree(&K.state);
+    if (K.h_state) cudaFreeHost(K.h_state);
+    if (K.h_hg) cudaFreeHost(K.h_hg);
+    K.h_state = nullptr;
+    K.h_hg = nullptr;
+    for (int s = 0; s < 2; ++s) {
+        if (K.exec[s]) cudaGraphExecDestroy(K.exec[s]);
+        K.exec[s] = nullptr;
+        K.exec_gen[s] = -1;
+    }
 }
 
 int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {

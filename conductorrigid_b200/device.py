@@ -50,6 +50,26 @@ class Handle:
     def set_stream(self, stream):
         self._check(_lib.lib().cr_set_stream(self.h, C.c_void_p(stream.cuda_stream)), "cr_set_stream")
 
+    def set_tiling(self, tile_edge: int, spread_mode: int = 1):
+        self._check(_lib.lib().cr_set_tiling(self.h, int(tile_edge), int(spread_mode)), "cr_set_tiling")
+
+    def autotune(self, pos, body_pos, reps: int = 5) -> dict:
+        """Pick the fastest mesh tiling for these positions (leaves them set)."""
+        self._pos = self.dev(pos).reshape(-1, 3)
+        self._bpos = self.dev(body_pos).reshape(-1, 3)
+        t, m, ms = C.c_int(0), C.c_int(0), C.c_float(0)
+        self._check(_lib.lib().cr_autotune(self.h, _ptr(self._pos), _ptr(self._bpos), int(reps), C.byref(t),
+                                           C.byref(m), C.byref(ms)), "cr_autotune")
+        return {"tile_edge": t.value, "spread_mode": m.value, "mesh_ms": ms.value}
+
+    def set_graphs(self, enable: bool):
+        self._check(_lib.lib().cr_set_graphs(self.h, int(bool(enable))), "cr_set_graphs")
+
+    def graph_launches(self) -> int:
+        v = C.c_longlong(0)
+        self._check(_lib.lib().cr_graph_launches(self.h, C.byref(v)), "cr_graph_launches")
+        return v.value
+
     def derived(self) -> _lib.CrDerived:
         d = _lib.CrDerived()
         self._check(_lib.lib().cr_get_derived(self.h, C.byref(d)), "cr_get_derived")

@@ -135,6 +135,26 @@ int cr_set_topology(cr_handle *h, int n_beads, const uint32_t *body, int n_bodie
                     const uint8_t *rigid, const double *body_charge);
 /* Stream for all later work on this handle (a cudaStream_t; NULL = legacy default). */
 int cr_set_stream(cr_handle *h, void *stream);
+/* Captured Arnoldi steps (on by default).  When a stream is set (cr_set_stream, not the
+ * legacy default stream) and the profiler is off, a solve captures one Arnoldi step of
+ * GMRES (preconditioner, operator, Gram-Schmidt, Hessenberg/Givens update on the
+ * device) as a CUDA graph once per geometry and launches it once per iteration, instead
+ * of ~25 kernel launches; the iterates are those of the uncaptured loop.  enable = 0
+ * keeps every step uncaptured.  cr_graph_launches counts the graph launches. */
+/* Mesh tiling of spreading and contraction.  tile_edge T: the mesh is processed in T^3
+ * tiles with a (T+P-1)^3 shared-memory halo (T in 2..32, within 227 KB in FP64);
+ * spread_mode 0 spreads with per-thread register columns where compiled (T = 8, P = 9
+ * or 11), 1 with shared-memory atomics.  cr_set_tiling sets one explicitly; cr_autotune
+ * times the FP32 mesh path (spread, FFT, influence function, FFT, contract; reps times)
+ * at the given positions for T in {4, 6, 8, 12, 16} and both spread modes where they
+ * exist, keeps the fastest and reports it.  Results do not depend on the tiling beyond
+ * the summation order of the spreading atomics.  The default is T = 8, mode 0;
+ * cr_set_params restores it. */
+int cr_set_tiling(cr_handle *h, int tile_edge, int spread_mode);
+int cr_autotune(cr_handle *h, const double *d_pos, const double *d_body_pos, int reps, int *tile_edge,
+                int *spread_mode, float *best_ms);
+int cr_set_graphs(cr_handle *h, int enable);
+int cr_graph_launches(const cr_handle *h, long long *launches);
 
 /* ---- the step (gpu_ComputeForce, ConductorRigid.cu:1153-1286) ----
  * Solves for the bead charges and body potentials (warm start from d_q / d_phi,
