@@ -7,8 +7,11 @@ rc <= L/2; for boxes smaller than 2 rc the replica's Ewald parameter is raised t
 xi = sqrt(-ln tol)/rc with rc = L/2, which keeps the real-space truncation error at the
 tolerance and moves the rest of the sum to the mesh.
 
-solve_batched() runs all replicas through cr_batch_compute (concurrent streams);
-solve_looped() solves them one after another through cr_compute, the single-system path.
+solve_batched() runs all replicas through cr_batch_compute (concurrent streams, each
+Arnoldi step a captured graph); solve_looped() solves them one after another through
+cr_compute, the single-system path.  With autotune=True every replica's mesh tiling is
+chosen by cr_autotune at construction (each system timed alone); tune_batch() instead
+chooses the tiling policy by the batch's own throughput.
 """
 from __future__ import annotations
 
@@ -33,7 +36,7 @@ def replica_params(system, tol=1e-5, support=9, gmres_tol=1e-6, restart=50, maxi
 
 
 class Replicas:
-    def __init__(self, specs, **param_kw):
+    def __init__(self, specs, autotune=False, **param_kw):
         import torch
 
         self.torch = torch
@@ -53,6 +56,7 @@ class Replicas:
             self.handles.append(h)
             self.arrays.append((pos, bpos, q, phi, force))
         self.n = len(self.handles)
+        self.tilings = [h.autotune(a[0], a[1], reps=3) for h, a in zip(self.handles, self.arrays)] if autotune else []
         self.n_charges = sum(s.n_beads for s in self.systems)
 
     def reset(self):
@@ -90,6 +94,46 @@ class Replicas:
             bad = [i for i in range(n) if status[i] != _lib.CR_OK]
             raise _lib.CrError(code, "cr_batch_compute", f"replicas {bad[:8]} failed")
         return [st[i].as_dict() for i in range(n)]
+
+    def set_tilings(self, tilings):
+        for h, t in zip(self.handles, tilings):
+            h.set_tiling(t["tile_edge"], t["spread_mode"])
+
+    def tune_batch(self, n_threads=16, policies=((8, 0), (4, 1), (6, 1), "isolated")):
+        """Pick the mesh tiling by the throughput of the batch itself.  Per-replica tuning
+        (cr_autotune) times each system alone, where small tiles win by occupying more of
+        the GPU; in a batch the GPU is already full and the extra halo work of small tiles
+        costs throughput, so the policy is chosen by timing one batched solve under each.
+        Returns {policy: solves/s}; the fastest policy stays set."""
+        import time
+
+        if "isolated" in policies and not self.tilings:
+            self.tilings = [h.autotune(a[0], a[1], reps=3) for h, a in zip(self.handles, self.arrays)]
+        rates = {}
+        for pol in policies:
+            if pol == "isolated":
+                self.set_tilings(self.tilings)
+            else:
+                for h in self.handles:
+                    h.set_tiling(*pol)
+            self.warm()
+            self.solve_batched(n_threads)  # captures this policy's graphs
+            self.reset()
+            self.torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            self.solve_batched(n_threads)
+            self.torch.cuda.synchronize()
+            rates[str(pol)] = self.n / (time.perf_counter() - t0)
+            self.reset()
+        best = max(policies, key=lambda p: rates[str(p)])
+        if best == "isolated":
+            self.set_tilings(self.tilings)
+        else:
+            for h in self.handles:
+                h.set_tiling(*best)
+        self.best_policy = str(best)
+        self.warm()
+        return rates
 
     def close(self):
         for h in self.handles:
