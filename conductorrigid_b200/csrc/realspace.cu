@@ -29,6 +29,8 @@
 // cluster pairs in FP64.
 #include <cub/cub.cuh>
 
+#include <type_traits>
+
 #include "cr_internal.cuh"
 
 namespace cr {
@@ -207,12 +209,14 @@ __device__ __forceinline__ int warp_exclusive_scan(int v, int lane) {
 
 // Values T(d_ij) of the set mask bits in the operator precision, lane-interleaved:
 // the k-th set bit of row i at voff + k*32 + i, zeros after the row's last bit.
-template <typename R>
+// With R2 = double (and R = float) one pass writes both precisions' values.
+template <typename R, typename R2 = void>
 __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
                                    const int *__restrict__ members, const double4 *__restrict__ pos,
                                    const double2 *__restrict__ tab, RSBuild c, const unsigned *__restrict__ masks,
                                    const long long *__restrict__ voff, const int *__restrict__ slots,
-                                   R *__restrict__ vals) {
+                                   R *__restrict__ vals, double *__restrict__ vals2 = nullptr) {
+    constexpr bool BOTH = std::is_same<R2, double>::value;
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (p >= npairs) return;
@@ -223,6 +227,7 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
     const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
     const unsigned m = masks[p * CS + lane];
     R *out = vals + voff[p] + lane;
+    double *out2 = BOTH ? vals2 + voff[p] + lane : nullptr;
     int k = 0;
     for (int j = 0; j < CS; ++j) {
         const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
@@ -232,12 +237,17 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
             const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
             const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
             const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
-            out[(size_t)k * CS] = (R)table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
+            const double t = table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
+            out[(size_t)k * CS] = (R)t;
+            if (BOTH) out2[(size_t)k * CS] = t;
             ++k;
         }
     }
     const int rows = slots[p] / CS;
-    for (; k < rows; ++k) out[(size_t)k * CS] = (R)0;
+    for (; k < rows; ++k) {
+        out[(size_t)k * CS] = (R)0;
+        if (BOTH) out2[(size_t)k * CS] = 0.0;
+    }
 }
 
 // Charges in cluster order (0 for padding), so that a warp reads a cluster's charges
@@ -415,16 +425,34 @@ template <typename R> long long &cap_of(RealSpace &r);
 template <> long long &cap_of<float>(RealSpace &r) { return r.blocks32_cap; }
 template <> long long &cap_of<double>(RealSpace &r) { return r.blocks64_cap; }
 
-// Packed values of precision R for the current cluster pairs (once per solve).
-template <typename R> int realspace_blocks(cr_handle *h) {
+template <typename R> int realspace_reserve(cr_handle *h) {
     RealSpace &r = h->rs;
-    if (valid_of<R>(r) || h->N == 0) return CR_OK;
     const long long need = std::max(r.nnz, 1LL);
     if (need > cap_of<R>(r)) {
         const long long cap = need + need / 8;
         CR_TRY(dalloc(h, &blocks_of<R>(r), (size_t)cap));
         cap_of<R>(r) = cap;
     }
+    return CR_OK;
+}
+
+// Packed values of precision R for the current cluster pairs (once per solve).  A solve
+// that runs an FP32 operator also needs FP64 values (its true residuals), so in those
+// modes the first request builds both in one pass.
+template <typename R> int realspace_blocks(cr_handle *h) {
+    RealSpace &r = h->rs;
+    if (valid_of<R>(r) || h->N == 0) return CR_OK;
+    if (h->user.precision != CR_FP64 && !r.valid32 && !r.valid64) {
+        CR_TRY(realspace_reserve<float>(h));
+        CR_TRY(realspace_reserve<double>(h));
+        pair_values_kernel<float, double><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
+            r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.voff,
+            r.nnz_pair, r.vals32, r.vals64);
+        CR_LAUNCH(h, "pair_values_kernel");
+        r.valid32 = r.valid64 = true;
+        return CR_OK;
+    }
+    CR_TRY(realspace_reserve<R>(h));
     pair_values_kernel<R><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
         r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.voff, r.nnz_pair,
         blocks_of<R>(r));

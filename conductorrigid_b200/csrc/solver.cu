@@ -27,26 +27,43 @@ namespace {
 
 constexpr int kDotThreads = 256;
 
-// partial[blk * k + j] = sum over this block's rows of V_j[i] * w[i]   (j < k)
-__global__ void __launch_bounds__(kDotThreads) multi_dot_kernel(int n, int k, const double *__restrict__ V,
-                                                                const double *__restrict__ w,
-                                                                double *__restrict__ partial) {
-    __shared__ double red[kDotThreads / 32];
+// partial[blk * kmax + j] = sum over this block's rows of V_j[i] * w[i]   (j < k):
+// eight vectors per pass, so w is read once and the block reduces once per eight.
+constexpr int kDotChunk = 8;
+__device__ __forceinline__ void multi_dot_body(int n, int k, int kmax, const double *__restrict__ V,
+                                               const double *__restrict__ w, double *__restrict__ partial) {
+    __shared__ double red[kDotThreads / 32][kDotChunk];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int j = 0; j < k; ++j) {
-        const double *v = V + (size_t)j * n;
-        double s = 0.0;
-        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += v[i] * w[i];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) red[warp] = s;
+    for (int j0 = 0; j0 < k; j0 += kDotChunk) {
+        double acc[kDotChunk];
+#pragma unroll
+        for (int c = 0; c < kDotChunk; ++c) acc[c] = 0.0;
+        const int kc = min(kDotChunk, k - j0);
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+            const double wi = w[i];
+#pragma unroll
+            for (int c = 0; c < kDotChunk; ++c)
+                if (c < kc) acc[c] += V[(size_t)(j0 + c) * n + i] * wi;
+        }
+#pragma unroll
+        for (int c = 0; c < kDotChunk; ++c) {
+            for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+            if (lane == 0) red[warp][c] = acc[c];
+        }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < kc) {
             double t = 0.0;
-            for (int q = 0; q < kDotThreads / 32; ++q) t += red[q];
-            partial[(size_t)blockIdx.x * k + j] = t;
+            for (int q = 0; q < kDotThreads / 32; ++q) t += red[q][threadIdx.x];
+            partial[(size_t)blockIdx.x * kmax + j0 + threadIdx.x] = t;
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(kDotThreads) multi_dot_kernel(int n, int k, const double *__restrict__ V,
+                                                                const double *__restrict__ w,
+                                                                double *__restrict__ partial) {
+    multi_dot_body(n, k, k, V, w, partial);
 }
 
 // out[j] = sum_blk partial[blk * k + j], in block order (deterministic).
@@ -64,6 +81,7 @@ __global__ void project_kernel(int n, int k, const double *__restrict__ V, const
                                double *__restrict__ w) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = w[i];
+#pragma unroll 8
         for (int j = 0; j < k; ++j) s -= hv[j] * V[(size_t)j * n + i];
         w[i] = s;
     }
@@ -144,23 +162,7 @@ __global__ void __launch_bounds__(kDotThreads) multi_dot_dev_kernel(int n, int k
                                                                     const double *__restrict__ V,
                                                                     const double *__restrict__ w,
                                                                     double *__restrict__ partial) {
-    __shared__ double red[kDotThreads / 32];
-    const int k = min(st->j + 1, kmax);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int j = 0; j < k; ++j) {
-        const double *v = V + (size_t)j * n;
-        double s = 0.0;
-        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += v[i] * w[i];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) red[warp] = s;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (int q = 0; q < kDotThreads / 32; ++q) t += red[q];
-            partial[(size_t)blockIdx.x * kmax + j] = t;
-        }
-        __syncthreads();
-    }
+    multi_dot_body(n, min(st->j + 1, kmax), kmax, V, w, partial);
 }
 
 __global__ void reduce_partials_dev_kernel(int nblk, int kmax, const ArnoldiState *st,
@@ -178,6 +180,7 @@ __global__ void project_dev_kernel(int n, int kmax, const ArnoldiState *st, cons
     const int k = min(st->j + 1, kmax);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = w[i];
+#pragma unroll 8
         for (int j = 0; j < k; ++j) s -= hv[j] * V[(size_t)j * n + i];
         w[i] = s;
     }
