@@ -479,9 +479,9 @@ def main() -> None:
     from conductorrigid_b200 import _lib, systems
     from conductorrigid_b200.device import Handle
 
-    world = env_int("WORLD_SIZE", 1)
-    rank = env_int("RANK", 0)
-    local = env_int("LOCAL_RANK", 0)
+    from conductorrigid_b200 import ranks
+
+    rank, local, world = ranks.rank_info()
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
@@ -489,17 +489,12 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        ranks.barrier(world)
 
     def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ranks.max_over_ranks(v, world, device="cuda")
 
-    w = systems.workload(WORKLOAD, seed=1 + rank)
+    w = systems.workload(WORKLOAD, seed=ranks.replica_seed(1, rank))
     s, p = w.system, w.params
     base = {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")}
     common = dict(field=tuple(s.field), gmres_tol=TOL, maxiter=20000, **base)
@@ -625,8 +620,8 @@ def main() -> None:
     total_prof_ms = sum(v["ms"] for v in prof.values())
     shares = {k: round(v["ms"] / total_prof_ms, 4) for k, v in prof.items() if total_prof_ms > 0}
 
-    value = world * 1e3 / ms_fast
-    plain_value = world * 1e3 / ms_plain
+    value = ranks.job_throughput(1.0, ms_fast, world)
+    plain_value = ranks.job_throughput(1.0, ms_plain, world)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_fast, "higher_is_better": True, "scaling": "weak",
