@@ -341,48 +341,63 @@ __global__ void __launch_bounds__(W * 32) pair_spmv_kernel(int nclus, const long
 constexpr int kSpmvWarps = 8;
 
 // Real-space forces over the cluster pairs, on the fly in FP64: F_i += -T'(d) q_i q_j
-// r_ij / d (ConductorRigid.cu:637-654); every ordered pair (I, J) is in the list.
-__global__ void __launch_bounds__(128) pair_force_kernel(long long npairs, const int *__restrict__ pair_i,
-                                                         const int *__restrict__ pair_j,
-                                                         const int *__restrict__ members,
-                                                         const double4 *__restrict__ pos, const double *__restrict__ q,
-                                                         const double2 *__restrict__ tab, RSBuild c,
-                                                         double *__restrict__ F) {
-    const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (p >= npairs) return;
-    const int I = pair_i[p], J = pair_j[p];
+// r_ij / d (ConductorRigid.cu:637-654); every ordered pair (I, J) is in the list.  One
+// CTA per cluster I: warp w takes I's pairs w, w+W, ..., lane i accumulates bead i's
+// force over the set bits of its mask rows, and the W partial forces are added in warp
+// order and written once (no atomics, the same result on every run).
+template <int W>
+__global__ void __launch_bounds__(W * 32) pair_force_kernel(const long long *__restrict__ head,
+                                                            const int *__restrict__ count,
+                                                            const int *__restrict__ pair_j,
+                                                            const int *__restrict__ members,
+                                                            const unsigned *__restrict__ masks,
+                                                            const double4 *__restrict__ pos,
+                                                            const double *__restrict__ q,
+                                                            const double2 *__restrict__ tab, RSBuild c,
+                                                            double *__restrict__ F) {
+    __shared__ double part[W][3][CS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int I = blockIdx.x;
     const int bi = members[I * CS + lane];
-    const int bj = members[J * CS + lane];
     const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
-    const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
     const double qi = bi >= 0 ? q[bi] : 0.0;
-    const double qjl = bj >= 0 ? q[bj] : 0.0;
     double fi[3] = {0, 0, 0};
-    for (int j = 0; j < CS; ++j) {
-        const int vj = __shfl_sync(0xffffffffu, bj, j);
-        const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
-        const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
-        const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
-        const double qj = __shfl_sync(0xffffffffu, qjl, j);
-        double f[3] = {0, 0, 0};
-        if (bi >= 0 && vj >= 0) {
-            const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
-            const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
-            const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
-            const double d2 = dx * dx + dy * dy + dz * dz;
-            if (d2 < c.rc2 && d2 >= c.rmin2) {
-                const double d = sqrt(d2);
+    const long long h0 = head[I];
+    const int n = count[I];
+    for (int k = w; k < n; k += W) {
+        const long long p = h0 + k;
+        const int J = pair_j[p];
+        const unsigned m = masks[p * CS + lane];
+        const int bj = members[J * CS + lane];
+        const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
+        const double qjl = bj >= 0 ? q[bj] : 0.0;
+        for (int j = 0; j < CS; ++j) {
+            const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
+            const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
+            const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
+            const double qj = __shfl_sync(0xffffffffu, qjl, j);
+            if (m & (1u << j)) {  // the in-range test of pair_mask_kernel
+                const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
+                const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
+                const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
+                const double d = sqrt(dx * dx + dy * dy + dz * dz);
                 const double a = -table_lerp64(tab, c, d) * qi * qj / d;
-                f[0] = a * dx;
-                f[1] = a * dy;
-                f[2] = a * dz;
+                fi[0] += a * dx;
+                fi[1] += a * dy;
+                fi[2] += a * dz;
             }
         }
-        for (int e = 0; e < 3; ++e) fi[e] += f[e];
     }
-    if (bi >= 0)
-        for (int e = 0; e < 3; ++e) atomicAdd(F + 3 * (size_t)bi + e, fi[e]);
+    for (int e = 0; e < 3; ++e) part[w][e][lane] = fi[e];
+    __syncthreads();
+    if (w == 0 && bi >= 0) {
+        for (int e = 0; e < 3; ++e) {
+            double t = 0.0;
+#pragma unroll
+            for (int v = 0; v < W; ++v) t += part[v][e][lane];
+            F[3 * (size_t)bi + e] = t;
+        }
+    }
 }
 
 // force_i = wave force_i + q_i E0 + real-space force_i
@@ -609,9 +624,9 @@ template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, cons
     if (N == 0) return CR_OK;
     RealSpace &r = h->rs;
     ProfScope ps(h, PROF_REAL_FORCE);
-    CR_CUDA(h, cudaMemsetAsync(r.freal, 0, 3 * (size_t)N * sizeof(double), h->stream));
-    pair_force_kernel<<<blocks_for(r.npairs * 32, 128), 128, 0, h->stream>>>(
-        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, q64, h->m64.gradphiq, rs_build(h), r.freal);
+    CR_CUDA(h, cudaMemsetAsync(r.freal, 0, 3 * (size_t)N * sizeof(double), h->stream));  // beads without pairs
+    pair_force_kernel<kSpmvWarps><<<r.nclus, kSpmvWarps * 32, 0, h->stream>>>(
+        r.head, r.count, r.pair_j, r.members, r.masks, h->m64.pos, q64, h->m64.gradphiq, rs_build(h), r.freal);
     CR_LAUNCH(h, "pair_force_kernel");
     force_combine_kernel<R><<<blocks_for(N, 256), 256, 0, h->stream>>>(N, m.force, q64, h->field[0], h->field[1],
                                                                        h->field[2], r.freal, force_out);
