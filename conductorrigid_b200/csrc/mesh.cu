@@ -36,7 +36,17 @@ struct MeshShape {
     int T;         // tile edge
     int P;         // support
     int Bd;        // halo buffer edge T + P - 1
+    int zp;        // z pitch of the contraction halo buffer
 };
+
+// z pitch of the contraction halo buffer: P + 32 (>= T + P - 1 for T <= 32, and congruent
+// to P modulo 32, so that the P*P window columns a warp reads in order fall on distinct
+// banks) where that buffer fits in 227 KB of shared memory, else T + P - 1.
+inline int contract_pitch(int T, int P, size_t elem) {
+    const size_t Bd = (size_t)T + P - 1;
+    const size_t padded = (Bd * Bd * (P + 32) + 8 * 6 * (size_t)P) * elem;
+    return padded <= 227 * 1024 ? P + 32 : (int)Bd;
+}
 
 template <typename R> struct WindowConst {
     R h[3], halfL[3], inv_eta[3];
@@ -221,7 +231,12 @@ __global__ void __launch_bounds__(256) contract_tiles_kernel(
     const int P = PT ? PT : ms.P;
     const int T = PT ? 8 : ms.T;
     const int Bd = PT ? 8 + PT - 1 : ms.Bd;
-    const int nbuf = Bd * Bd * Bd;
+    // halo buffer [x][y][z] with the z rows at a pitch of P + 32 (>= Bd): column (b, c) of
+    // a window then sits at bank (b * P + c) mod 32, so a warp reading P*P columns in
+    // order touches 32 distinct banks
+    const int zp = ms.zp;
+    const int plane = Bd * zp;
+    const int nbuf = Bd * plane;
     const int tile = blockIdx.x;
     const int b0 = tile_start[tile], b1 = tile_start[tile + 1];
     if (b0 == b1) return;
@@ -229,12 +244,19 @@ __global__ void __launch_bounds__(256) contract_tiles_kernel(
     R *w = buf + nbuf + warp * 6 * P;
     R *u = w + 3 * P;
     const int tz = tile % ms.ntd[2], ty = (tile / ms.ntd[2]) % ms.ntd[1], tx = tile / (ms.ntd[2] * ms.ntd[1]);
-    for (int n = threadIdx.x; n < nbuf; n += blockDim.x) {
-        const int bz = n % Bd, by = (n / Bd) % Bd, bx = n / (Bd * Bd);
-        const int gx = fold(tx * T + bx, ms.Ng[0]);
+    // fill: one (y, z) column per thread, x marched with an incremental fold
+    for (int cidx = threadIdx.x; cidx < Bd * Bd; cidx += blockDim.x) {
+        const int by = cidx / Bd, bz = cidx - by * Bd;
         const int gy = fold(ty * T + by, ms.Ng[1]);
         const int gz = fold(tz * T + bz, ms.Ng[2]);
-        buf[n] = grid[((size_t)gx * ms.Ng[1] + gy) * ms.Ng[2] + gz];
+        const R *src = grid + (size_t)gy * ms.Ng[2] + gz;
+        const size_t xstride = (size_t)ms.Ng[1] * ms.Ng[2];
+        int gx = fold(tx * T, ms.Ng[0]);
+        R *dst = buf + by * zp + bz;
+        for (int bx = 0; bx < Bd; ++bx) {
+            dst[bx * plane] = src[(size_t)gx * xstride];
+            if (++gx == ms.Ng[0]) gx = 0;
+        }
     }
     __syncthreads();
     for (int k = b0 + warp; k < b1; k += nw) {
@@ -251,10 +273,10 @@ __global__ void __launch_bounds__(256) contract_tiles_kernel(
             for (int e = lane; e < P * P; e += 32) {
                 const int b = e / P, cc = e - b * P;
                 const R wyz = w[P + b] * w[2 * P + cc];
-                const R *col = buf + ((size_t)ox * Bd + (oy + b)) * Bd + (oz + cc);
+                const R *col = buf + (size_t)ox * plane + (oy + b) * zp + (oz + cc);
                 R s0 = 0, sx = 0;
                 for (int a = 0; a < P; ++a) {
-                    const R g = w[a] * col[(size_t)a * Bd * Bd];
+                    const R g = w[a] * col[(size_t)a * plane];
                     s0 += g;
                     if (FORCE) sx += g * u[a];
                 }
@@ -337,6 +359,7 @@ template <typename R> MeshShape mesh_shape(const cr_handle *h) {
     ms.T = h->tile;
     ms.P = h->d.support;
     ms.Bd = h->tile + h->d.support - 1;
+    ms.zp = contract_pitch(h->tile, h->d.support, sizeof(R));
     return ms;
 }
 
@@ -357,7 +380,8 @@ template <typename R> size_t spread_smem(const cr_handle *h) {
 }
 template <typename R> size_t contract_smem(const cr_handle *h) {
     const int Bd = h->tile + h->d.support - 1;
-    return ((size_t)Bd * Bd * Bd + 8 * 6 * (size_t)h->d.support) * sizeof(R);
+    return ((size_t)Bd * Bd * contract_pitch(h->tile, h->d.support, sizeof(R)) + 8 * 6 * (size_t)h->d.support) *
+           sizeof(R);
 }
 
 // The dynamic shared-memory limit is a process-wide attribute of each kernel: it only
