@@ -452,6 +452,8 @@ def main() -> None:
                     choices=[WORKLOAD, "replicas_256", "dynamics_420k", "mlp", "polydisperse_204k"],
                     help="headline solve (default), 256 batched replicas, or Brownian dynamics")
     ap.add_argument("--scale", type=float, default=1.0, help="dynamics workload: body-count fraction")
+    ap.add_argument("--tiling", default="", help="T,MODE: fixed mesh tiling of the headline solver instead of "
+                                                 "cr_autotune (for runs under a profiler)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "ours" and args.workload == "replicas_256":
@@ -509,7 +511,12 @@ def main() -> None:
         h.set_topology(s.body, s.rigid, s.body_charge)
     pos = h_fast.dev(s.pos)
     bpos = h_fast.dev(s.body_pos)
-    tiling = h_fast.autotune(pos, bpos, reps=5)  # untimed set-up
+    if args.tiling:  # an explicit tiling (profiling runs: timing-based choices are not valid under a profiler)
+        t_edge, t_mode = (int(v) for v in args.tiling.split(","))
+        h_fast.set_tiling(t_edge, t_mode)
+        tiling = {"tile_edge": t_edge, "spread_mode": t_mode, "mesh_ms": None}
+    else:
+        tiling = h_fast.autotune(pos, bpos, reps=5)  # untimed set-up
     q = torch.zeros(s.n_beads, dtype=torch.float64, device="cuda")
     phi = torch.zeros(s.n_bodies, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
