@@ -210,10 +210,20 @@ def paired_run(params_plain, params_learned, system, radius, steps, *, train_sol
 
     from .device import Handle
 
-    hp = Handle(params_plain, system.L)
+    stream = torch.cuda.Stream()  # a stream of their own: the solvers capture their Arnoldi steps
+    hp = Handle(params_plain, system.L, stream=stream)
     hp.set_topology(system.body, system.rigid, system.body_charge)
-    hl = Handle(params_learned, system.L)
+    hl = Handle(params_learned, system.L, stream=stream)
     hl.set_topology(system.body, system.rigid, system.body_charge)
+    with torch.cuda.stream(stream):
+        return _paired_loop(hp, hl, system, radius, steps, train_solves, seed, dt, use_network, use_transport,
+                            passes, lr, repulsion, contact_gap, relax_steps, mode)
+
+
+def _paired_loop(hp, hl, system, radius, steps, train_solves, seed, dt, use_network, use_transport, passes, lr,
+                 repulsion, contact_gap, relax_steps, mode):
+    import torch
+
     run = BrownianRun(hp, system, radius, dt=dt, seed=seed, repulsion=repulsion, contact_gap=contact_gap,
                       relax_steps=relax_steps)
     guess = LearnedGuess(hl, radius, train_solves=train_solves if train_solves is not None else steps,
@@ -227,10 +237,10 @@ def paired_run(params_plain, params_learned, system, radius, steps, *, train_sol
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         if prev is not None:
-            k = guess.prepare(prev[2], prev[0], prev[1], pos, bpos, None if mode == "add" else prev[3])
+            nd = guess.prepare(prev[2], prev[0], prev[1], pos, bpos, None if mode == "add" else prev[3])
             if mode == "add":
                 # unit-weight corrections on top of the warm start
-                for j in range(k):
+                for j in range(nd):
                     ql += guess.dirs[j, :hl.N]
                 _lib.lib().cr_set_guess_directions(hl.h, 0, None)
         _, stl = hl.compute(pos, bpos, ql, pl)
