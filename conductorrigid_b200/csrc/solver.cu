@@ -12,8 +12,9 @@
 //     reorthogonalisation), Givens rotations and the least-squares update are FP64;
 //   - CR_MIXED runs the inner iterations with the FP32 operator and wraps them in
 //     FP64 iterative refinement: r = b - A64 x, solve A32 d ~= r, x += d.
-// All vectors stay on the device; each Arnoldi step copies its j+2 Hessenberg
-// entries to pinned host memory for the Givens update (one small copy per step).
+// All vectors stay on the device.  An uncaptured Arnoldi step copies its Hessenberg
+// column to pinned host memory for the Givens update; a captured step (below) does that
+// update on the device and copies back only its small state.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -660,10 +661,17 @@ int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {
     CR_TRY(norm(h, b, &bnorm));
     if (!std::isfinite(bnorm)) return fail(h, CR_NUMERICAL, "non-finite right-hand side");
     const double atol = tol * bnorm;
-    // initial FP64 residual r0 = b - A x0
-    CR_TRY(op_apply(h, CR_FP64, x, K.r, oc));
-    residual_kernel<<<nb, 256, 0, h->stream>>>(n, b, K.r);
-    CR_LAUNCH(h, "residual_kernel");
+    // initial FP64 residual r0 = b - A x0; from a zero start A x0 is exactly zero (no
+    // charge reaches the mesh or a pair sum), so r0 = b without an operator application
+    double xnorm = 0;
+    CR_TRY(norm(h, x, &xnorm));
+    if (xnorm == 0.0) {
+        CR_CUDA(h, cudaMemcpyAsync(K.r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        CR_TRY(op_apply(h, CR_FP64, x, K.r, oc));
+        residual_kernel<<<nb, 256, 0, h->stream>>>(n, b, K.r);
+        CR_LAUNCH(h, "residual_kernel");
+    }
     CR_TRY(norm(h, K.r, &rnorm));
     if (!std::isfinite(rnorm)) return fail(h, CR_NUMERICAL, "non-finite residual");
     s.initial_residual = bnorm > 0 ? rnorm / bnorm : rnorm;
