@@ -454,6 +454,8 @@ def main() -> None:
     ap.add_argument("--scale", type=float, default=1.0, help="dynamics workload: body-count fraction")
     ap.add_argument("--tiling", default="", help="T,MODE: fixed mesh tiling of the headline solver instead of "
                                                  "cr_autotune (for runs under a profiler)")
+    ap.add_argument("--precond", default="two_level", choices=["two_level", "conductor"],
+                    help="preconditioner of the headline (fast) arm")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "ours" and args.workload == "replicas_256":
@@ -501,7 +503,7 @@ def main() -> None:
     base = {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")}
     common = dict(field=tuple(s.field), gmres_tol=TOL, maxiter=20000, **base)
     stream = torch.cuda.Stream()
-    h_fast = Handle(_lib.make_params(precision="mixed", learned=bool(args.learned), precond="conductor",
+    h_fast = Handle(_lib.make_params(precision="mixed", learned=bool(args.learned), precond=args.precond,
                                      restart=RESTART, **common), s.L, stream=stream)
     h_plain = Handle(_lib.make_params(precision="fp64", precond="diagonal", restart=RESTART_PLAIN, **common), s.L,
                      stream=stream)
@@ -635,7 +637,9 @@ def main() -> None:
         "vs_baseline": None, "dtype": "f32 operator / f64 Krylov", "data": "synthetic",
         "config": {"workload": WORKLOAD, "charges": s.n_beads, "bodies": s.n_bodies, "mesh": p["grid"],
                    "support": p["support"], "rcut": p["rcut"], "xi": p["xi"], "tol": TOL, "restart": RESTART,
-                   "preconditioner": "conductor response", "learned": bool(args.learned),
+                   "preconditioner": {"two_level": "two-level (conductor response + induced-dipole coarse "
+                                                    "correction)", "conductor": "conductor response"}[args.precond],
+                   "learned": bool(args.learned),
                    "mesh_tiling": tiling,
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every step"},
         "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain, "preconditioner": "diagonal (reference)",
@@ -646,6 +650,7 @@ def main() -> None:
                            "iterations": st_f64c[-1]["iterations"], "final_residual": st_f64c[-1]["final_residual"]},
         "speedup_vs_plain_fp64": value / plain_value,
         "solve": {"iterations": st_fast[-1]["iterations"], "refinements": st_fast[-1]["refinements"],
+                  "coarse_level": h_fast.coarse_info() if args.precond == "two_level" else None,
                   "matvecs_fp32": st_fast[-1]["matvecs_fp32"], "matvecs_fp64": st_fast[-1]["matvecs_fp64"],
                   "final_residual": st_fast[-1]["final_residual"]},
         "kernel_share": shares,

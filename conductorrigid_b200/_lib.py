@@ -31,11 +31,13 @@ PRECISIONS = {"fp64": CR_FP64, "mixed": CR_MIXED, "fp32": CR_FP32}
 
 CR_PRECOND_DIAGONAL = 0
 CR_PRECOND_CONDUCTOR = 1
-PRECONDITIONERS = {"diagonal": CR_PRECOND_DIAGONAL, "conductor": CR_PRECOND_CONDUCTOR}
+CR_PRECOND_TWO_LEVEL = 2
+PRECONDITIONERS = {"diagonal": CR_PRECOND_DIAGONAL, "conductor": CR_PRECOND_CONDUCTOR,
+                   "two_level": CR_PRECOND_TWO_LEVEL}
 
 #: kernel classes of cr_profile_read
 PROFILE_CLASSES = ["spread", "fft", "scale", "contract", "real_space", "contract_force", "real_space_force",
-                   "krylov", "body", "geometry", "precondition"]
+                   "krylov", "body", "geometry", "precondition", "coarse"]
 
 
 class CrParams(C.Structure):
@@ -149,6 +151,7 @@ _SIGS = {
     "cr_set_positions": ([_P, _P, _P], _I),
     "cr_apply_operator": ([_P, _P, _P, _I], _I),
     "cr_precondition": ([_P, _P, _P], _I),
+    "cr_coarse_info": ([_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int)], _I),
     "cr_objective": ([_P, _P], _I),
     "cr_wave_potential": ([_P, _P, _P, _I], _I),
     "cr_spread": ([_P, _P, _P, _I], _I),

@@ -60,6 +60,7 @@ namespace {
 
 void free_all(cr_handle *h) {
     conductor_free(h);
+    coarse_free(h);
     mesh_free(h->m64);
     mesh_free(h->m32);
     geometry_free(h);
@@ -139,7 +140,9 @@ int need_geometry(cr_handle *h) {
 }
 
 bool finite_params(const cr_params *p) {
-    if (p->precond != CR_PRECOND_DIAGONAL && p->precond != CR_PRECOND_CONDUCTOR) return false;
+    if (p->precond != CR_PRECOND_DIAGONAL && p->precond != CR_PRECOND_CONDUCTOR &&
+        p->precond != CR_PRECOND_TWO_LEVEL)
+        return false;
     if (p->precision < CR_FP64 || p->precision > CR_FP32) return false;
     if (!std::isfinite(p->xi) || !std::isfinite(p->errortol) || !std::isfinite(p->rcut) ||
         !std::isfinite(p->gmres_tol))
@@ -258,6 +261,7 @@ int cr_set_params(cr_handle *h, const cr_params *p, const double L[3]) {
     h->geo.valid = false;
     if (h->have_topology) {
         conductor_free(h);
+        coarse_free(h);
         mesh_free(h->m64);
         mesh_free(h->m32);
         geometry_free(h);
@@ -403,8 +407,21 @@ int cr_precondition(cr_handle *h, const double *d_x, double *d_y) {
     CR_TRY(need_ready(h));
     if (h->N == 0) return CR_OK;
     if (!d_x || !d_y) return fail(h, CR_BAD_PARAM, "null vector");
+    CR_TRY(coarse_prepare(h));
     CR_TRY(precondition(h, d_x, d_y));
     return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_precondition");
+}
+
+int cr_coarse_info(cr_handle *h, int *active, int *n_coarse, long long *n_pairs, int *n_modes) {
+    CR_TRY(need_ready(h));
+    CR_TRY(coarse_prepare(h));
+    const CoarseSpace &c = h->coarse;
+    const bool on = h->user.precond == CR_PRECOND_TWO_LEVEL && c.active;
+    if (active) *active = on ? 1 : 0;
+    if (n_coarse) *n_coarse = on ? c.nc : 0;
+    if (n_pairs) *n_pairs = on ? c.npairs : 0;
+    if (n_modes) *n_modes = on ? c.nmodes : 0;
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_coarse_info");
 }
 
 int cr_objective(cr_handle *h, double *d_rhs) {

@@ -134,6 +134,7 @@ int objective(cr_handle *h, double *rhs) {
 int precondition(cr_handle *h, const double *x, double *y) {
     ProfScope ps(h, PROF_PRECOND);
     if (h->user.precond == CR_PRECOND_CONDUCTOR) return conductor_apply(h, x, y);
+    if (h->user.precond == CR_PRECOND_TWO_LEVEL) return coarse_apply(h, x, y);
     const int n = h->N + h->B;
     precondition_kernel<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->N, h->B, h->d_rigid, h->d_bsize, x, y);
     CR_LAUNCH(h, "precondition_kernel");

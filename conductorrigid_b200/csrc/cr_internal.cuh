@@ -144,6 +144,41 @@ struct ConductorPrecond {
     double *d_invs = nullptr;           // [S] 1 / (1^T K^-1 1)
 };
 
+// Coarse level of the two-level preconditioner (coarse.cu): three induced-dipole
+// vectors per rigid body, the inverse of their model operator, and what the A-DEF1
+// correction reads every iteration.  Buffers only grow; `gen` is the geometry generation
+// they describe.
+struct CoarseSpace {
+    long long gen = -1;
+    bool active = false, failed = false;
+    int nbc = 0, nc = 0, np = 0;        // coarse bodies, unknowns (3 nbc), padded order
+    int nmodes = 0, K2 = 0;             // half-space wave vectors, padded 2*nmodes
+    long long npairs = 0;               // ordered near body pairs
+    double kc = 0.0;                    // wave-vector cut used
+    int *cidx = nullptr;                // [B] coarse index of a body or -1
+    int *cbody = nullptr;               // [nbc] body of a coarse index
+    double *zq = nullptr;               // [3N] the bead's values in its body's three columns
+    double *zp = nullptr;               // [3B] body-potential rows of the columns
+    double4 *cent = nullptr;            // [B] centroid, bounding radius in .w
+    double *basis = nullptr;            // [6 (N+B)] right-hand sides and solutions of the basis
+    int *phead = nullptr, *pcount = nullptr;  // [nbc] near pairs of each coarse body
+    int *pair_a = nullptr, *pair_b = nullptr; // [npairs]
+    long long *woff = nullptr;          // [npairs] first W value of the pair
+    float *W = nullptr;                 // per pair: [n_a][3] real-space blocks M_real Z_q
+    float4 *kv = nullptr;               // [nmodes] (mx, my, mz, sqrt w)
+    float *F = nullptr, *FT = nullptr;  // [nc][K2] scaled structure factors and transpose
+    double *C = nullptr;                // [np][np] coarse operator, inverted in place
+    float *Ci = nullptr;                // [np][np] FP32 copy of C^-1
+    double *R = nullptr, *Fc = nullptr, *Dinv = nullptr;  // Gauss-Jordan panels
+    double *g = nullptr, *y = nullptr;  // [nc] restricted residual, coarse solution
+    float *u = nullptr;                 // [K2] wave coefficients of Z y
+    double *t = nullptr;                // [N+B] r - A~ Z y
+    size_t cap_cidx = 0, cap_cbody = 0, cap_zq = 0, cap_zp = 0, cap_cent = 0, cap_basis = 0, cap_phead = 0,
+           cap_pcount = 0, cap_pair_a = 0, cap_pair_b = 0, cap_woff = 0, cap_W = 0, cap_kv = 0, cap_F = 0,
+           cap_FT = 0, cap_C = 0, cap_Ci = 0, cap_R = 0, cap_Fc = 0, cap_Dinv = 0, cap_g = 0, cap_y = 0,
+           cap_u = 0, cap_t = 0;
+};
+
 // Kernel classes timed by the built-in profiler (CUDA events on the handle's stream).
 enum ProfId {
     PROF_SPREAD = 0,
@@ -157,6 +192,7 @@ enum ProfId {
     PROF_BODY,
     PROF_GEOMETRY,
     PROF_PRECOND,
+    PROF_COARSE,
     PROF_COUNT
 };
 
@@ -189,6 +225,7 @@ struct cr_handle {
     double4 *d_bpos = nullptr;        // [B] body centres
     std::vector<int> h_body_start, h_body_members;  // host copy of the member lists
     cr::ConductorPrecond cond;
+    cr::CoarseSpace coarse;
 
     // tables on the host (FP64)
     std::vector<double> h_phiq, h_gradphiq;
@@ -322,6 +359,11 @@ int precondition(cr_handle *h, const double *x, double *y);
 int conductor_setup(cr_handle *h);
 int conductor_apply(cr_handle *h, const double *x, double *y);
 void conductor_free(cr_handle *h);
+// Coarse level of CR_PRECOND_TWO_LEVEL for the current geometry (no-op otherwise or when
+// already built); coarse_apply is the whole two-level preconditioner.
+int coarse_prepare(cr_handle *h);
+int coarse_apply(cr_handle *h, const double *x, double *z);
+void coarse_free(cr_handle *h);
 // y = A x in the given precision (full operator).
 int apply_operator(cr_handle *h, const double *x, double *y, int precision);
 // Solve A x = b (x holds the warm start).

@@ -386,7 +386,7 @@ int geometry_update(cr_handle *h, const double *d_pos, const double *d_body_pos)
     if (bad) return fail(h, CR_NUMERICAL, "non-finite or out-of-range bead position");
     CR_TRY(bin_beads(h, h->d_keys, h->ntiles, g.tile_count, g.tile_start, g.tile_beads));
     CR_TRY(realspace_build(h));
-    if (h->user.precond == CR_PRECOND_CONDUCTOR && !h->cond.ready) CR_TRY(conductor_setup(h));
+    if (h->user.precond != CR_PRECOND_DIAGONAL && !h->cond.ready) CR_TRY(conductor_setup(h));
     if (d_body_pos && h->B > 0) {
         CR_CUDA(h, cudaMemcpy2DAsync(h->d_bpos, sizeof(double4), d_body_pos, 3 * sizeof(double), 3 * sizeof(double),
                                      h->B, cudaMemcpyDeviceToDevice, h->stream));

@@ -658,6 +658,7 @@ int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {
     cr_solve_stats s{};
     OpCount oc;
     double bnorm = 0, rnorm = 0;
+    CR_TRY(coarse_prepare(h));  // two-level preconditioner: coarse level of this geometry
     CR_TRY(norm(h, b, &bnorm));
     if (!std::isfinite(bnorm)) return fail(h, CR_NUMERICAL, "non-finite right-hand side");
     const double atol = tol * bnorm;

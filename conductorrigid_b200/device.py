@@ -122,6 +122,14 @@ class Handle:
         self._check(_lib.lib().cr_precondition(self.h, _ptr(x), _ptr(y)), "cr_precondition")
         return y
 
+    def coarse_info(self) -> dict:
+        """Coarse level of the two-level preconditioner for the current positions."""
+        a, n, m = C.c_int(0), C.c_int(0), C.c_int(0)
+        p = C.c_longlong(0)
+        self._check(_lib.lib().cr_coarse_info(self.h, C.byref(a), C.byref(n), C.byref(p), C.byref(m)),
+                    "cr_coarse_info")
+        return {"active": bool(a.value), "n_coarse": n.value, "near_pairs": p.value, "wave_vectors": m.value}
+
     def objective(self):
         y = self.empty(self.N + self.B)
         self._check(_lib.lib().cr_objective(self.h, _ptr(y)), "cr_objective")

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define CR_ABI_VERSION 2
+#define CR_ABI_VERSION 3
 
 typedef enum {
     CR_OK = 0,
@@ -47,7 +47,9 @@ typedef enum {
 
 typedef enum {
     CR_PRECOND_DIAGONAL = 0,  /* the reference's diagonal preconditioner (ConductorRigid.cu:816-859) */
-    CR_PRECOND_CONDUCTOR = 1  /* exact isolated-conductor response per body (block inverse) */
+    CR_PRECOND_CONDUCTOR = 1, /* exact isolated-conductor response per body (block inverse) */
+    CR_PRECOND_TWO_LEVEL = 2  /* conductor response + a coarse correction on the span of the
+                                 bodies' induced dipoles (deflation, built per geometry) */
 } cr_preconditioner;
 
 typedef enum {
@@ -176,6 +178,10 @@ int cr_apply_operator(cr_handle *h, const double *d_x, double *d_y, int precisio
 /* The handle's preconditioner: the reference's diagonal scaling (Precondition,
  * ConductorRigid.cu:1023-1044) or the conductor response (cr_params.precond). */
 int cr_precondition(cr_handle *h, const double *d_x, double *d_y);
+/* Coarse level of CR_PRECOND_TWO_LEVEL for the current positions (built here if the
+ * positions changed since): active 1/0, coarse unknowns (three per rigid body of at least
+ * four beads), ordered near body pairs, half-space wave vectors of the coarse operator. */
+int cr_coarse_info(cr_handle *h, int *active, int *n_coarse, long long *n_pairs, int *n_modes);
 /* Right-hand side [-(r_i - R_b).E0 ; Q_b] (compute_objective, cu:764-813). */
 int cr_objective(cr_handle *h, double *d_rhs);
 /* Wave-space potential of charges q (spread, FFT, scale, inverse FFT, contract;
