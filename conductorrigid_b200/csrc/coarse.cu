@@ -27,7 +27,7 @@
 //
 // P the conductor response.  A~ Z y = [Phi(Z y) - M~ Z_q y ; 0] is evaluated from blocks
 // W = M_real Z_q stored per pair of near bodies and from the same k-sum; C^-1 is formed
-// once per geometry (in-place blocked Gauss-Jordan, FP64) and applied as an FP32 matrix.
+// once per geometry (assembled in FP64, inverted in place by blocked Gauss-Jordan in FP32).
 // In flexible GMRES any preconditioner leaves the solution unchanged: only the iteration
 // count moves (at 162 beads per sphere, phi = 0.30: 133 -> 40 iterations against the
 // conductor response alone, on 100 bodies).
@@ -187,7 +187,7 @@ struct RealArgs {
 // One CTA per ordered near pair p = (a, b):  W_p[k][c] = sum_{j in b} T(d_kj) z_bc(j) for
 // the beads k of a (the operator's pair rule dr <= d < rc under the minimum image), and
 // C[3a+e][3b+c] += sum_k z_ae(k) W_p[k][c] (+ the self term when a == b).
-__global__ void __launch_bounds__(128) coarse_real_kernel(
+__global__ void __launch_bounds__(256) coarse_real_kernel(
     const int *__restrict__ pair_a, const int *__restrict__ pair_b, const long long *__restrict__ woff,
     const int *__restrict__ cbody, const int *__restrict__ body_start, const int *__restrict__ members,
     const float4 *__restrict__ pos, const double *__restrict__ zq, const float2 *__restrict__ tab, RealArgs g,
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(128) coarse_real_kernel(
 __global__ void coarse_wave_basis_kernel(int nmodes, const float4 *__restrict__ kv, const int *__restrict__ cbody,
                                          const int *__restrict__ body_start, const int *__restrict__ members,
                                          const double4 *__restrict__ pos, double3 Linv, const double *__restrict__ zq,
-                                         int ldf, int nc, float *__restrict__ F, float *__restrict__ FT) {
+                                         int ldf, int ldt, float *__restrict__ F, float *__restrict__ FT) {
     __shared__ float4 sf[kChunk];
     __shared__ float2 sz[kChunk];
     const int a = blockIdx.x, ba = cbody[a];
@@ -305,8 +305,8 @@ __global__ void coarse_wave_basis_kernel(int nmodes, const float4 *__restrict__ 
                 const int row = 3 * a + e;
                 F[(size_t)row * ldf + 2 * m] = k.w * re[e];
                 F[(size_t)row * ldf + 2 * m + 1] = k.w * im[e];
-                FT[(size_t)(2 * m) * nc + row] = k.w * re[e];
-                FT[(size_t)(2 * m + 1) * nc + row] = k.w * im[e];
+                FT[(size_t)(2 * m) * ldt + row] = k.w * re[e];
+                FT[(size_t)(2 * m + 1) * ldt + row] = k.w * im[e];
             }
     }
 }
@@ -372,78 +372,82 @@ __global__ void symmetrise_kernel(int n, double *__restrict__ C, int ldc) {
     C[(size_t)c * ldc + r] = v;
 }
 
-// ---- blocked Gauss-Jordan inversion of an SPD matrix, in place (no pivoting) ----
+// ---- blocked Gauss-Jordan inversion of an SPD matrix, in place (no pivoting, FP32) ----
 // Step k (block K = [k0, k0+NB)):  Dinv = A_KK^-1;  R = Dinv A_K* with A_KK := I;
 // Fc = A_*K;  A_i* = (A_i* with A_iK := 0) - Fc_i R  (i not in K);  A_K* = R.
+// FP32 is enough for a preconditioner: the coarse operators met here have condition
+// numbers of 1e2-1e3, so C^-1 carries relative errors ~1e-4 at worst.
 
-// Dinv of the pivot block (one CTA, scalar in-place Gauss-Jordan in shared memory).
-__global__ void gj_pivot_kernel(int k0, int np, const double *__restrict__ A, double *__restrict__ Dinv,
-                                int *__restrict__ flag) {
-    __shared__ double D[NB][NB + 1];
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) D[t / NB][t % NB] = A[(size_t)(k0 + t / NB) * np + k0 + t % NB];
+// Dinv of the pivot block (one CTA of 1024 threads, scalar in-place Gauss-Jordan in
+// shared memory; thread t owns entries (t/64 + 16u, t%64), u = 0..3); a pivot that is
+// not positive and finite sets *flag and leaves Dinv untouched.
+__global__ void __launch_bounds__(1024) gj_pivot_kernel(int k0, int np, const float *__restrict__ A,
+                                                        float *__restrict__ Dinv, int *__restrict__ flag) {
+    __shared__ float D[NB][NB + 1];
+    const int c = threadIdx.x % NB, r0 = threadIdx.x / NB;  // rows r0, r0+16, r0+32, r0+48
+    for (int u = 0; u < 4; ++u) D[r0 + 16 * u][c] = A[(size_t)(k0 + r0 + 16 * u) * np + k0 + c];
     __syncthreads();
     for (int s = 0; s < NB; ++s) {
-        const double piv = D[s][s];
-        __syncthreads();
-        if (!(piv > 0.0) || !isfinite(piv)) {
+        const float piv = D[s][s];
+        if (!(piv > 0.0f) || !isfinite(piv)) {  // uniform over the block
             if (threadIdx.x == 0) atomicExch(flag, 1);
             return;
         }
-        const double inv = 1.0 / piv;
-        // row s scaled, with the identity column in place of column s
-        if (threadIdx.x < NB) {
-            const int c = threadIdx.x;
-            D[s][c] = c == s ? inv : D[s][c] * inv;
-        }
+        const float inv = 1.0f / piv;
+        float rs[4];
+        for (int u = 0; u < 4; ++u) rs[u] = D[r0 + 16 * u][s];
+        const float sc = D[s][c];
         __syncthreads();
-        for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
-            const int r = t / NB, c = t % NB;
-            if (r == s) continue;
-            const double f = D[r][s];
-            // column s of the other rows becomes -f * inv (the identity column eliminated)
-            if (c == s) continue;
-            D[r][c] -= f * D[s][c];
-        }
-        __syncthreads();
-        if (threadIdx.x < NB && threadIdx.x != s) {
-            const int r = threadIdx.x;
-            D[r][s] = -D[r][s] * inv;
+        // row s: scaled, with the identity column in place of column s;
+        // other rows: D[r][c] -= D[r][s] D[s][c] / piv, and column s becomes -D[r][s] / piv
+        const float scs = c == s ? inv : sc * inv;
+        for (int u = 0; u < 4; ++u) {
+            const int r = r0 + 16 * u;
+            if (r == s) D[r][c] = scs;
+            else D[r][c] = c == s ? -rs[u] * inv : D[r][c] - rs[u] * scs;
         }
         __syncthreads();
     }
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) Dinv[t] = D[t / NB][t % NB];
+    for (int u = 0; u < 4; ++u) Dinv[(r0 + 16 * u) * NB + c] = D[r0 + 16 * u][c];
 }
 
 // R = Dinv A_K* (with A_KK := I, so R_KK = Dinv) and Fc = A_*K.  blockIdx.x: 64 columns.
-__global__ void gj_panel_kernel(int k0, int np, const double *__restrict__ A, const double *__restrict__ Dinv,
-                                double *__restrict__ R, double *__restrict__ Fc) {
-    __shared__ double Ds[NB][NB + 1];
+__global__ void gj_panel_kernel(int k0, int np, const float *__restrict__ A, const float *__restrict__ Dinv,
+                                float *__restrict__ R, float *__restrict__ Fc) {
+    __shared__ float Ds[NB][NB + 1];
+    __shared__ float As[NB][NB + 1];
     const int j0 = blockIdx.x * NB;
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) Ds[t / NB][t % NB] = Dinv[t];
+    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
+        const int r = t / NB, c = t % NB;
+        Ds[r][c] = Dinv[t];
+        As[r][c] = A[(size_t)(k0 + r) * np + j0 + c];
+    }
     __syncthreads();
     const bool diag = j0 == k0;
     for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
         const int r = t / NB, c = t % NB;
-        double v;
+        float v;
         if (diag) {
             v = Ds[r][c];
         } else {
-            v = 0.0;
-            for (int s = 0; s < NB; ++s) v += Ds[r][s] * __ldg(A + (size_t)(k0 + s) * np + j0 + c);
+            v = 0.0f;
+#pragma unroll 16
+            for (int s = 0; s < NB; ++s) v += Ds[r][s] * As[s][c];
         }
         R[(size_t)r * np + j0 + c] = v;
     }
-    // the column panel: rows j0..j0+NB of column block K
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
+    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {  // rows j0.. of the column panel
         const int r = t / NB, c = t % NB;
         Fc[(size_t)(j0 + r) * NB + c] = A[(size_t)(j0 + r) * np + k0 + c];
     }
 }
 
-// A_i* = (A_i*, A_iK := 0) - Fc_i R for i outside K; A_K* = R.  64 x 64 tile per CTA.
-__global__ void __launch_bounds__(256) gj_update_kernel(int k0, int np, double *__restrict__ A,
-                                                        const double *__restrict__ R, const double *__restrict__ Fc) {
-    __shared__ double Fs[32][64 + 1], Rs[32][64 + 1];
+// A_i* = (A_i*, A_iK := 0) - Fc_i R for i outside K; A_K* = R.  64 x 64 tile per CTA,
+// 4 x 4 outputs per thread, the whole NB = 64 inner dimension staged at once.
+__global__ void __launch_bounds__(256) gj_update_kernel(int k0, int np, float *__restrict__ A,
+                                                        const float *__restrict__ R, const float *__restrict__ Fc) {
+    __shared__ __align__(16) float Fs[NB][64 + 4];
+    __shared__ __align__(16) float Rs[NB][64 + 4];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int r0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
     if (r0 == k0) {  // the pivot rows take R
@@ -453,41 +457,34 @@ __global__ void __launch_bounds__(256) gj_update_kernel(int k0, int np, double *
         }
         return;
     }
-    double acc[4][4];
+    for (int t = threadIdx.x; t < NB * 64; t += 256) {
+        const int s = t / 64, q = t % 64;
+        Fs[s][q] = Fc[(size_t)(r0 + q) * NB + s];
+        Rs[s][q] = R[(size_t)s * np + c0 + q];
+    }
+    __syncthreads();
+    float acc[4][4];
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
-    for (int s0 = 0; s0 < NB; s0 += 32) {
-        for (int t = threadIdx.x; t < 32 * 64; t += 256) {
-            const int s = t / 64, q = t % 64;
-            Fs[s][q] = Fc[(size_t)(r0 + q) * NB + s0 + s];
-            Rs[s][q] = R[(size_t)(s0 + s) * np + c0 + q];
-        }
-        __syncthreads();
+        for (int v = 0; v < 4; ++v) acc[u][v] = 0.f;
 #pragma unroll 8
-        for (int s = 0; s < 32; ++s) {
-            double fv[4], rv[4];
+    for (int s = 0; s < NB; ++s) {
+        const float4 fv = *reinterpret_cast<const float4 *>(&Fs[s][ty * 4]);
+        const float4 rv = *reinterpret_cast<const float4 *>(&Rs[s][tx * 4]);
+        const float f[4] = {fv.x, fv.y, fv.z, fv.w}, r[4] = {rv.x, rv.y, rv.z, rv.w};
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                fv[u] = Fs[s][ty * 4 + u];
-                rv[u] = Rs[s][tx * 4 + u];
-            }
+        for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) acc[u][v] += fv[u] * rv[v];
-        }
-        __syncthreads();
+            for (int v = 0; v < 4; ++v) acc[u][v] += f[u] * r[v];
     }
     const bool kcols = c0 == k0;
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const size_t idx = (size_t)(r0 + ty * 4 + u) * np + c0 + tx * 4 + v;
-            A[idx] = (kcols ? 0.0 : A[idx]) - acc[u][v];
-        }
+    for (int u = 0; u < 4; ++u) {
+        float4 *dst = reinterpret_cast<float4 *>(A + (size_t)(r0 + ty * 4 + u) * np + c0 + tx * 4);
+        const float4 old = kcols ? make_float4(0.f, 0.f, 0.f, 0.f) : *dst;
+        *dst = make_float4(old.x - acc[u][0], old.y - acc[u][1], old.z - acc[u][2], old.w - acc[u][3]);
+    }
 }
 
 __global__ void to_float_kernel(long long n, const double *__restrict__ a, float *__restrict__ b) {
@@ -516,91 +513,110 @@ __global__ void coarse_restrict_kernel(int N, const int *__restrict__ cbody, con
         for (int e = 0; e < 3; ++e) g[3 * a + e] = s[e] + zp[3 * ba + e] * x[N + ba];
 }
 
-// y = -Cinv g (one warp per row)
+// sum_c row[c] v[c] over a zero-padded row of n4 float4 (one warp; row 16-byte aligned).
+__device__ __forceinline__ double warp_row_dot(const float *__restrict__ row, const double *__restrict__ v, int n4) {
+    const int lane = threadIdx.x & 31;
+    const float4 *r4 = reinterpret_cast<const float4 *>(row);
+    const double2 *v2 = reinterpret_cast<const double2 *>(v);
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll 4
+    for (int c = lane; c < n4; c += 32) {
+        const float4 a = __ldg(r4 + c);
+        const double2 p = v2[2 * c], q = v2[2 * c + 1];
+        s0 += (double)a.x * p.x + (double)a.y * p.y;
+        s1 += (double)a.z * q.x + (double)a.w * q.y;
+    }
+    double s = s0 + s1;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+// y = -Cinv g (one warp per row; rows of ld floats, g zero beyond n)
 __global__ void coarse_gemv_kernel(int n, int ld, const float *__restrict__ Ci, const double *__restrict__ g,
                                    double *__restrict__ y) {
     const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
     if (r >= n) return;
-    const float *row = Ci + (size_t)r * ld;
-    double s = 0.0;
-    for (int c = lane; c < n; c += 32) s += (double)row[c] * g[c];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) y[r] = -s;
+    const double s = warp_row_dot(Ci + (size_t)r * ld, g, ld / 4);
+    if ((threadIdx.x & 31) == 0) y[r] = -s;
 }
 
-// u[m] = sum_c FT[m][c] y[c] (one warp per row of FT)
-__global__ void coarse_wave_coef_kernel(int rows, int nc, const float *__restrict__ FT, const double *__restrict__ y,
-                                        float *__restrict__ u) {
+// u[r] = sqrt(w_m) sum_c FT[r][c] y[c], m = r / 2 (one warp per row of FT): the
+// coefficients w_m (Re, Im) S_{Zy}(k_m) of the potential of the coarse charges Z_q y.
+__global__ void coarse_wave_coef_kernel(int rows, int ld, const float *__restrict__ FT, const float4 *__restrict__ kv,
+                                        const double *__restrict__ y, float *__restrict__ u) {
     const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
     if (r >= rows) return;
-    const float *row = FT + (size_t)r * nc;
-    double s = 0.0;
-    for (int c = lane; c < nc; c += 32) s += (double)row[c] * y[c];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) u[r] = (float)s;
+    const double s = warp_row_dot(FT + (size_t)r * ld, y, ld / 4);
+    if ((threadIdx.x & 31) == 0) u[r] = (float)(s * kv[r >> 1].w);
 }
 
 // t = x - A~ Z y on the bead rows of body b (one CTA per body), t[N+b] = x[N+b]:
 //   (A~ Z y)_i = Phi_b(Z y) - [ self (Z_q y)_i + sum_p W_p y_b(p) + wave_i ],
-//   wave_i = sum_m sqrt(w_m) (cos(k_m.r_i) u_re[m] - sin(k_m.r_i) u_im[m]).
-__global__ void coarse_model_kernel(int N, int nmodes, const int *__restrict__ cidx, const int *__restrict__ body_start,
+//   wave_i = sum_m (cos(k_m.r_i) u_re[m] - sin(k_m.r_i) u_im[m]).
+// The wave vectors come in rows of consecutive m_z at fixed (m_x, m_y): one sincospi per
+// row, then rotation by exp(2 pi i z / L_z) along the row.  The body's near pairs (partner
+// coefficients and W offsets) are staged in shared memory first.
+__global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__restrict__ rows,
+                                    const int *__restrict__ cidx, const int *__restrict__ body_start,
                                     const int *__restrict__ members, const double4 *__restrict__ pos, double3 Linv,
                                     const double *__restrict__ zq, const double *__restrict__ zp,
                                     const int *__restrict__ phead, const int *__restrict__ pcount,
                                     const int *__restrict__ pair_b, const long long *__restrict__ woff,
-                                    const float *__restrict__ W, const float4 *__restrict__ kv,
-                                    const float *__restrict__ u, double selfc, const double *__restrict__ y,
-                                    const double *__restrict__ x, double *__restrict__ t) {
-    __shared__ float4 sk[256];
-    __shared__ float2 su[256];
+                                    const float *__restrict__ W, const float *__restrict__ u, double selfc,
+                                    const double *__restrict__ y, const double *__restrict__ x,
+                                    double *__restrict__ t) {
+    extern __shared__ float4 dyn[];
     const int b = blockIdx.x;
     const int beg = body_start[b], nb = body_start[b + 1] - beg;
     const int a = cidx[b];
-    for (int k0 = 0; k0 < nb; k0 += blockDim.x) {
-        const int k = k0 + threadIdx.x;
-        int i = -1;
-        double f[3] = {0.0, 0.0, 0.0};
-        if (k < nb) {
-            i = members[beg + k];
-            const double4 p = pos[i];
-            f[0] = p.x * Linv.x;
-            f[1] = p.y * Linv.y;
-            f[2] = p.z * Linv.z;
-        }
-        const float fx = (float)f[0], fy = (float)f[1], fz = (float)f[2];
+    const int h0 = a >= 0 ? phead[a] : 0, npr = a >= 0 ? pcount[a] : 0;
+    int4 *srow = reinterpret_cast<int4 *>(dyn);                                // [nrows] (mx, my, mz0, first mode)
+    float2 *su = reinterpret_cast<float2 *>(dyn + nrows);                     // [nmodes]
+    double2 *sy = reinterpret_cast<double2 *>(dyn + nrows + (nmodes + 1) / 2); // [npr][2] partner y, W offset
+    for (int q = threadIdx.x; q < nrows; q += blockDim.x) srow[q] = rows[q];
+    for (int q = threadIdx.x; q < nmodes; q += blockDim.x) su[q] = make_float2(u[2 * q], u[2 * q + 1]);
+    for (int q = threadIdx.x; q < npr; q += blockDim.x) {
+        const int c = pair_b[h0 + q];
+        sy[2 * q] = make_double2(y[3 * c], y[3 * c + 1]);
+        sy[2 * q + 1] = make_double2(y[3 * c + 2], __longlong_as_double(woff[h0 + q]));
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        const int i = members[beg + k];
+        const double4 p = pos[i];
+        const float fx = (float)(p.x * Linv.x), fy = (float)(p.y * Linv.y), fz = (float)(p.z * Linv.z);
+        float sz, cz;
+        sincospif(2.0f * fz, &sz, &cz);
         float wave = 0.f;
-        for (int m0 = 0; m0 < nmodes; m0 += 256) {
-            const int nm = min(256, nmodes - m0);
-            __syncthreads();
-            for (int q = threadIdx.x; q < nm; q += blockDim.x) {
-                sk[q] = kv[m0 + q];
-                su[q] = make_float2(u[2 * (m0 + q)], u[2 * (m0 + q) + 1]);
+        for (int q = 0; q < nrows; ++q) {
+            const int4 r = srow[q];
+            const int end = q + 1 < nrows ? srow[q + 1].w : nmodes;
+            float s, c;
+            sincospif(2.0f * ((float)r.x * fx + (float)r.y * fy + (float)r.z * fz), &s, &c);
+            for (int m = r.w; m < end; ++m) {
+                const float2 uu = su[m];
+                wave += c * uu.x - s * uu.y;
+                const float c2 = c * cz - s * sz;
+                s = s * cz + c * sz;
+                c = c2;
             }
-            __syncthreads();
-            if (i >= 0)
-                for (int q = 0; q < nm; ++q) {
-                    const float4 kk = sk[q];
-                    float s, c;
-                    sincospif(2.0f * (kk.x * fx + kk.y * fy + kk.z * fz), &s, &c);
-                    const float2 uu = su[q];
-                    wave += kk.w * (c * uu.x - s * uu.y);
-                }
         }
-        if (i < 0) continue;
         double m = (double)wave;
         double phi = 0.0;
         if (a >= 0) {
             const double y0 = y[3 * a], y1 = y[3 * a + 1], y2 = y[3 * a + 2];
             m += selfc * (zq[3 * i] * y0 + zq[3 * i + 1] * y1 + zq[3 * i + 2] * y2);
             phi = zp[3 * b] * y0 + zp[3 * b + 1] * y1 + zp[3 * b + 2] * y2;
-            const int h0 = phead[a], np_ = pcount[a];
-            for (int q = 0; q < np_; ++q) {
-                const int c = pair_b[h0 + q];
-                const float *w = W + woff[h0 + q] + 3 * (size_t)k;
-                m += (double)w[0] * y[3 * c] + (double)w[1] * y[3 * c + 1] + (double)w[2] * y[3 * c + 2];
+            double m0 = 0.0, m1 = 0.0;
+#pragma unroll 4
+            for (int q = 0; q < npr; ++q) {
+                const double2 y01 = sy[2 * q], y2o = sy[2 * q + 1];
+                const float *w = W + __double_as_longlong(y2o.y) + 3 * (size_t)k;
+                const float w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+                m0 += (double)w0 * y01.x + (double)w1 * y01.y;
+                m1 += (double)w2 * y2o.x;
             }
+            m += m0 + m1;
         }
         t[i] = x[i] - (phi - m);
     }
@@ -647,6 +663,7 @@ void coarse_free(cr_handle *h) {
     dfree(&c.woff);
     dfree(&c.W);
     dfree(&c.kv);
+    dfree(&c.rows);
     dfree(&c.F);
     dfree(&c.FT);
     dfree(&c.C);
@@ -769,27 +786,50 @@ int coarse_prepare(cr_handle *h) {
         kc *= 0.95;
     }
     const int nmodes = (int)kv.size();
+    std::vector<int4> rows;  // runs of consecutive m_z at fixed (m_x, m_y): (mx, my, mz0, first mode)
+    for (int m = 0; m < nmodes; ++m) {
+        const int mx = (int)kv[m].x, my = (int)kv[m].y, mz = (int)kv[m].z;
+        if (m == 0 || mx != (int)kv[m - 1].x || my != (int)kv[m - 1].y || mz != (int)kv[m - 1].z + 1)
+            rows.push_back(make_int4(mx, my, mz, m));
+    }
+    const int nrows = (int)rows.size();
     const int K2 = std::max(16, (2 * nmodes + 15) / 16 * 16);
     const int np = (nc + NB - 1) / NB * NB;
     CR_TRY(grow(h, &cs.kv, cs.cap_kv, (size_t)std::max(nmodes, 1), moved));
+    CR_TRY(grow(h, &cs.rows, cs.cap_rows, (size_t)std::max(nrows, 1), moved));
     CR_TRY(grow(h, &cs.F, cs.cap_F, (size_t)nc * K2, moved));
-    CR_TRY(grow(h, &cs.FT, cs.cap_FT, (size_t)K2 * nc, moved));
+    CR_TRY(grow(h, &cs.FT, cs.cap_FT, (size_t)K2 * np, moved));
     CR_TRY(grow(h, &cs.C, cs.cap_C, (size_t)np * np, moved));
     CR_TRY(grow(h, &cs.Ci, cs.cap_Ci, (size_t)np * np, moved));
     CR_TRY(grow(h, &cs.R, cs.cap_R, (size_t)NB * np, moved));
     CR_TRY(grow(h, &cs.Fc, cs.cap_Fc, (size_t)np * NB, moved));
     CR_TRY(grow(h, &cs.Dinv, cs.cap_Dinv, (size_t)NB * NB, moved));
-    CR_TRY(grow(h, &cs.g, cs.cap_g, (size_t)nc, moved));
-    CR_TRY(grow(h, &cs.y, cs.cap_y, (size_t)nc, moved));
+    CR_TRY(grow(h, &cs.g, cs.cap_g, (size_t)np, moved));  // zero beyond nc: the padded GEMV rows
+    CR_TRY(grow(h, &cs.y, cs.cap_y, (size_t)np, moved));
     CR_TRY(grow(h, &cs.u, cs.cap_u, (size_t)K2, moved));
     CR_TRY(grow(h, &cs.t, cs.cap_t, n1, moved));
-    if (nmodes > 0)
+    if (nmodes > 0) {
         CR_CUDA(h, cudaMemcpyAsync(cs.kv, kv.data(), nmodes * sizeof(float4), cudaMemcpyHostToDevice, h->stream));
+        CR_CUDA(h, cudaMemcpyAsync(cs.rows, rows.data(), nrows * sizeof(int4), cudaMemcpyHostToDevice, h->stream));
+    }
+    // threads per body CTA: the largest body rounded up to whole warps
+    int max_n = 0;
+    for (int b = 0; b < B; ++b) max_n = std::max(max_n, h->h_body_start[b + 1] - h->h_body_start[b]);
+    const int bs = std::min(256, std::max(32, (max_n + 31) / 32 * 32));
+    int max_pairs = 0;
+    for (int a = 0; a < nbc; ++a) max_pairs = std::max(max_pairs, pcount[a]);
+    const size_t model_smem =
+        ((size_t)nrows + (nmodes + 1) / 2) * sizeof(float4) + (size_t)max_pairs * 2 * sizeof(double2);
+    if (model_smem > 48 * 1024)
+        CR_CUDA(h, cudaFuncSetAttribute(coarse_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)model_smem));
     CR_CUDA(h, cudaMemsetAsync(cs.F, 0, (size_t)nc * K2 * sizeof(float), h->stream));
-    CR_CUDA(h, cudaMemsetAsync(cs.FT, 0, (size_t)K2 * nc * sizeof(float), h->stream));
+    CR_CUDA(h, cudaMemsetAsync(cs.FT, 0, (size_t)K2 * np * sizeof(float), h->stream));
+    CR_CUDA(h, cudaMemsetAsync(cs.g, 0, (size_t)np * sizeof(double), h->stream));
+    CR_CUDA(h, cudaMemsetAsync(cs.y, 0, (size_t)np * sizeof(double), h->stream));
     if (nmodes > 0) {
         coarse_wave_basis_kernel<<<nbc, 128, 0, h->stream>>>(nmodes, cs.kv, cs.cbody, h->d_body_start,
-                                                             h->d_body_members, h->m64.pos, Linv, cs.zq, K2, nc,
+                                                             h->d_body_members, h->m64.pos, Linv, cs.zq, K2, np,
                                                              cs.F, cs.FT);
         CR_LAUNCH(h, "coarse_wave_basis_kernel");
     }
@@ -809,7 +849,7 @@ int coarse_prepare(cr_handle *h) {
     ra.inv_dr = (float)(1.0 / h->d.dr);
     ra.ntab = h->d.n_table;
     ra.selfc = h->d.selfcoeff;
-    coarse_real_kernel<<<(unsigned)npairs, 128, 0, h->stream>>>(cs.pair_a, cs.pair_b, cs.woff, cs.cbody,
+    coarse_real_kernel<<<(unsigned)npairs, bs, 0, h->stream>>>(cs.pair_a, cs.pair_b, cs.woff, cs.cbody,
                                                                  h->d_body_start, h->d_body_members, h->m32.pos,
                                                                  cs.zq, h->m32.phiq, ra, np, cs.W, cs.C);
     CR_LAUNCH(h, "coarse_real_kernel");
@@ -818,18 +858,18 @@ int coarse_prepare(cr_handle *h) {
     pad_identity_kernel<<<blocks_for((long)np * np, 256), 256, 0, h->stream>>>(nc, np, cs.C);
     CR_LAUNCH(h, "pad_identity_kernel");
 
-    // C^-1 in place
-    CR_CUDA(h, cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-    for (int k0 = 0; k0 < np; k0 += NB) {
-        gj_pivot_kernel<<<1, 256, 0, h->stream>>>(k0, np, cs.C, cs.Dinv, h->d_flag);
-        CR_LAUNCH(h, "gj_pivot_kernel");
-        gj_panel_kernel<<<np / NB, 256, 0, h->stream>>>(k0, np, cs.C, cs.Dinv, cs.R, cs.Fc);
-        CR_LAUNCH(h, "gj_panel_kernel");
-        gj_update_kernel<<<dim3(np / 64, np / 64), 256, 0, h->stream>>>(k0, np, cs.C, cs.R, cs.Fc);
-        CR_LAUNCH(h, "gj_update_kernel");
-    }
+    // C^-1: FP32 copy inverted in place
     to_float_kernel<<<blocks_for((long)np * np, 256), 256, 0, h->stream>>>((long long)np * np, cs.C, cs.Ci);
     CR_LAUNCH(h, "to_float_kernel");
+    CR_CUDA(h, cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+    for (int k0 = 0; k0 < np; k0 += NB) {
+        gj_pivot_kernel<<<1, 1024, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, h->d_flag);
+        CR_LAUNCH(h, "gj_pivot_kernel");
+        gj_panel_kernel<<<np / NB, 256, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, cs.R, cs.Fc);
+        CR_LAUNCH(h, "gj_panel_kernel");
+        gj_update_kernel<<<dim3(np / 64, np / 64), 256, 0, h->stream>>>(k0, np, cs.Ci, cs.R, cs.Fc);
+        CR_LAUNCH(h, "gj_update_kernel");
+    }
     int bad = 0;
     CR_CUDA(h, cudaMemcpyAsync(&bad, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CR_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -841,6 +881,9 @@ int coarse_prepare(cr_handle *h) {
     cs.nc = nc;
     cs.np = np;
     cs.nmodes = nmodes;
+    cs.nrows = nrows;
+    cs.bs = bs;
+    cs.model_smem = model_smem;
     cs.K2 = K2;
     cs.npairs = npairs;
     cs.kc = kc;
@@ -861,12 +904,13 @@ int coarse_apply(cr_handle *h, const double *x, double *z) {
     CR_LAUNCH(h, "coarse_gemv_kernel");
     if (cs.nmodes > 0) {
         coarse_wave_coef_kernel<<<blocks_for((long)2 * cs.nmodes * 32, 256), 256, 0, h->stream>>>(
-            2 * cs.nmodes, cs.nc, cs.FT, cs.y, cs.u);
+            2 * cs.nmodes, cs.np, cs.FT, cs.kv, cs.y, cs.u);
         CR_LAUNCH(h, "coarse_wave_coef_kernel");
     }
-    coarse_model_kernel<<<B, 128, 0, h->stream>>>(N, cs.nmodes, cs.cidx, h->d_body_start, h->d_body_members,
-                                                  h->m64.pos, Linv, cs.zq, cs.zp, cs.phead, cs.pcount, cs.pair_b,
-                                                  cs.woff, cs.W, cs.kv, cs.u, h->d.selfcoeff, cs.y, x, cs.t);
+    coarse_model_kernel<<<B, cs.bs, cs.model_smem, h->stream>>>(N, cs.nmodes, cs.nrows, cs.rows, cs.cidx,
+                                                                 h->d_body_start, h->d_body_members, h->m64.pos,
+                                                                 Linv, cs.zq, cs.zp, cs.phead, cs.pcount, cs.pair_b,
+                                                                 cs.woff, cs.W, cs.u, h->d.selfcoeff, cs.y, x, cs.t);
     CR_LAUNCH(h, "coarse_model_kernel");
     CR_TRY(conductor_apply(h, cs.t, z));
     coarse_prolong_kernel<<<cs.nbc, 128, 0, h->stream>>>(N, cs.cbody, h->d_body_start, h->d_body_members, cs.zq,

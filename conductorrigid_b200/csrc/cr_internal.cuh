@@ -166,17 +166,20 @@ struct CoarseSpace {
     long long *woff = nullptr;          // [npairs] first W value of the pair
     float *W = nullptr;                 // per pair: [n_a][3] real-space blocks M_real Z_q
     float4 *kv = nullptr;               // [nmodes] (mx, my, mz, sqrt w)
-    float *F = nullptr, *FT = nullptr;  // [nc][K2] scaled structure factors and transpose
-    double *C = nullptr;                // [np][np] coarse operator, inverted in place
-    float *Ci = nullptr;                // [np][np] FP32 copy of C^-1
-    double *R = nullptr, *Fc = nullptr, *Dinv = nullptr;  // Gauss-Jordan panels
+    int4 *rows = nullptr;               // [nrows] runs of consecutive mz: (mx, my, mz0, first mode)
+    int nrows = 0, bs = 128;            // runs; threads per body CTA
+    size_t model_smem = 0;              // dynamic shared memory of the A~ Z y kernel
+    float *F = nullptr, *FT = nullptr;  // [nc][K2] scaled structure factors, [K2][np] transpose
+    double *C = nullptr;                // [np][np] coarse operator (assembled in FP64)
+    float *Ci = nullptr;                // [np][np] FP32 copy of C, inverted in place
+    float *R = nullptr, *Fc = nullptr, *Dinv = nullptr;   // Gauss-Jordan panels (FP32)
     double *g = nullptr, *y = nullptr;  // [nc] restricted residual, coarse solution
     float *u = nullptr;                 // [K2] wave coefficients of Z y
     double *t = nullptr;                // [N+B] r - A~ Z y
     size_t cap_cidx = 0, cap_cbody = 0, cap_zq = 0, cap_zp = 0, cap_cent = 0, cap_basis = 0, cap_phead = 0,
            cap_pcount = 0, cap_pair_a = 0, cap_pair_b = 0, cap_woff = 0, cap_W = 0, cap_kv = 0, cap_F = 0,
            cap_FT = 0, cap_C = 0, cap_Ci = 0, cap_R = 0, cap_Fc = 0, cap_Dinv = 0, cap_g = 0, cap_y = 0,
-           cap_u = 0, cap_t = 0;
+           cap_u = 0, cap_t = 0, cap_rows = 0;
 };
 
 // Kernel classes timed by the built-in profiler (CUDA events on the handle's stream).
