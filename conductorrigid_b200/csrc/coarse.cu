@@ -43,7 +43,7 @@ namespace {
 
 constexpr int kMinBeads = 4;        // bodies with fewer beads get no coarse vectors
 constexpr int kMaxCoarse = 12288;   // coarse unknowns above which the level is skipped
-constexpr int kMaxModes = 4096;     // half-space wave vectors kept (kc shrinks above)
+constexpr int kMaxModes = 1024;     // half-space wave vectors kept (kc shrinks above)
 constexpr int NB = 64;              // Gauss-Jordan block
 constexpr int kChunk = 512;         // beads staged in shared memory per pass
 
@@ -442,48 +442,66 @@ __global__ void gj_panel_kernel(int k0, int np, const float *__restrict__ A, con
     }
 }
 
-// A_i* = (A_i*, A_iK := 0) - Fc_i R for i outside K; A_K* = R.  64 x 64 tile per CTA,
-// 4 x 4 outputs per thread, the whole NB = 64 inner dimension staged at once.
+// A_i* = (A_i*, A_iK := 0) - Fc_i R for i outside K; A_K* = R.  128 x 128 tile per CTA,
+// 8 x 8 outputs per thread (rows and columns {4t..4t+3} and {64+4t..64+4t+3}, so every
+// shared-memory read is a conflict-free float4), the inner dimension in two halves of 32.
+constexpr int GT = 128;  // update tile; the padded order is a multiple of it
 __global__ void __launch_bounds__(256) gj_update_kernel(int k0, int np, float *__restrict__ A,
                                                         const float *__restrict__ R, const float *__restrict__ Fc) {
-    __shared__ __align__(16) float Fs[NB][64 + 4];
-    __shared__ __align__(16) float Rs[NB][64 + 4];
+    __shared__ __align__(16) float Fs[32][GT + 4];
+    __shared__ __align__(16) float Rs[32][GT + 4];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int r0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
-    if (r0 == k0) {  // the pivot rows take R
-        for (int t = threadIdx.x; t < 64 * 64; t += 256) {
-            const int r = t / 64, c = t % 64;
-            A[(size_t)(r0 + r) * np + c0 + c] = R[(size_t)r * np + c0 + c];
+    const int r0 = blockIdx.y * GT, c0 = blockIdx.x * GT;
+    float acc[8][8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[u][v] = 0.f;
+    for (int s0 = 0; s0 < NB; s0 += 32) {
+        for (int f = threadIdx.x; f < GT * 8; f += 256) {
+            const int q = f % GT, j = f / GT;  // row r0+q of the column panel, entries s0+4j..
+            const float4 v = *reinterpret_cast<const float4 *>(Fc + (size_t)(r0 + q) * NB + s0 + 4 * j);
+            Fs[4 * j][q] = v.x;
+            Fs[4 * j + 1][q] = v.y;
+            Fs[4 * j + 2][q] = v.z;
+            Fs[4 * j + 3][q] = v.w;
+            const int sr = f / 32, c4 = f % 32;
+            *reinterpret_cast<float4 *>(&Rs[sr][4 * c4]) =
+                *reinterpret_cast<const float4 *>(R + (size_t)(s0 + sr) * np + c0 + 4 * c4);
         }
-        return;
+        __syncthreads();
+#pragma unroll 4
+        for (int s = 0; s < 32; ++s) {
+            const float4 a0 = *reinterpret_cast<const float4 *>(&Fs[s][ty * 4]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&Fs[s][64 + ty * 4]);
+            const float4 b0 = *reinterpret_cast<const float4 *>(&Rs[s][tx * 4]);
+            const float4 b1 = *reinterpret_cast<const float4 *>(&Rs[s][64 + tx * 4]);
+            const float fa[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float fb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int v = 0; v < 8; ++v) acc[u][v] += fa[u] * fb[v];
+        }
+        __syncthreads();
     }
-    for (int t = threadIdx.x; t < NB * 64; t += 256) {
-        const int s = t / 64, q = t % 64;
-        Fs[s][q] = Fc[(size_t)(r0 + q) * NB + s];
-        Rs[s][q] = R[(size_t)s * np + c0 + q];
-    }
-    __syncthreads();
-    float acc[4][4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int u = 0; u < 8; ++u) {
+        const int i = r0 + (u < 4 ? ty * 4 + u : 64 + ty * 4 + u - 4);
+        const bool krow = i >= k0 && i < k0 + NB;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = 0.f;
-#pragma unroll 8
-    for (int s = 0; s < NB; ++s) {
-        const float4 fv = *reinterpret_cast<const float4 *>(&Fs[s][ty * 4]);
-        const float4 rv = *reinterpret_cast<const float4 *>(&Rs[s][tx * 4]);
-        const float f[4] = {fv.x, fv.y, fv.z, fv.w}, r[4] = {rv.x, rv.y, rv.z, rv.w};
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) acc[u][v] += f[u] * r[v];
-    }
-    const bool kcols = c0 == k0;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        float4 *dst = reinterpret_cast<float4 *>(A + (size_t)(r0 + ty * 4 + u) * np + c0 + tx * 4);
-        const float4 old = kcols ? make_float4(0.f, 0.f, 0.f, 0.f) : *dst;
-        *dst = make_float4(old.x - acc[u][0], old.y - acc[u][1], old.z - acc[u][2], old.w - acc[u][3]);
+        for (int h = 0; h < 2; ++h) {
+            const int j = c0 + h * 64 + tx * 4;
+            float4 *dst = reinterpret_cast<float4 *>(A + (size_t)i * np + j);
+            if (krow) {  // the pivot rows take R
+                *dst = *reinterpret_cast<const float4 *>(R + (size_t)(i - k0) * np + j);
+            } else {
+                const bool kcol = j >= k0 && j < k0 + NB;
+                const float4 old = kcol ? make_float4(0.f, 0.f, 0.f, 0.f) : *dst;
+                *dst = make_float4(old.x - acc[u][4 * h], old.y - acc[u][4 * h + 1], old.z - acc[u][4 * h + 2],
+                                   old.w - acc[u][4 * h + 3]);
+            }
+        }
     }
 }
 
@@ -794,7 +812,7 @@ int coarse_prepare(cr_handle *h) {
     }
     const int nrows = (int)rows.size();
     const int K2 = std::max(16, (2 * nmodes + 15) / 16 * 16);
-    const int np = (nc + NB - 1) / NB * NB;
+    const int np = (nc + GT - 1) / GT * GT;  // padded order (identity on the padding)
     CR_TRY(grow(h, &cs.kv, cs.cap_kv, (size_t)std::max(nmodes, 1), moved));
     CR_TRY(grow(h, &cs.rows, cs.cap_rows, (size_t)std::max(nrows, 1), moved));
     CR_TRY(grow(h, &cs.F, cs.cap_F, (size_t)nc * K2, moved));
@@ -867,7 +885,7 @@ int coarse_prepare(cr_handle *h) {
         CR_LAUNCH(h, "gj_pivot_kernel");
         gj_panel_kernel<<<np / NB, 256, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, cs.R, cs.Fc);
         CR_LAUNCH(h, "gj_panel_kernel");
-        gj_update_kernel<<<dim3(np / 64, np / 64), 256, 0, h->stream>>>(k0, np, cs.Ci, cs.R, cs.Fc);
+        gj_update_kernel<<<dim3(np / GT, np / GT), 256, 0, h->stream>>>(k0, np, cs.Ci, cs.R, cs.Fc);
         CR_LAUNCH(h, "gj_update_kernel");
     }
     int bad = 0;
