@@ -457,6 +457,7 @@ def main() -> None:
     ap.add_argument("--scale", type=float, default=1.0, help="dynamics workload: body-count fraction")
     ap.add_argument("--tiling", default="", help="T,MODE: fixed mesh tiling of the headline solver instead of "
                                                  "cr_autotune (for runs under a profiler)")
+    ap.add_argument("--restart", type=int, default=RESTART, help="FGMRES restart of the headline (fast) arm")
     ap.add_argument("--precond", default="two_level", choices=["two_level", "conductor"],
                     help="preconditioner of the headline (fast) arm")
     args = ap.parse_args()
@@ -507,7 +508,7 @@ def main() -> None:
     common = dict(field=tuple(s.field), gmres_tol=TOL, maxiter=20000, **base)
     stream = torch.cuda.Stream()
     h_fast = Handle(_lib.make_params(precision="mixed", learned=bool(args.learned), precond=args.precond,
-                                     restart=RESTART, **common), s.L, stream=stream)
+                                     restart=args.restart, **common), s.L, stream=stream)
     h_plain = Handle(_lib.make_params(precision="fp64", precond="diagonal", restart=RESTART_PLAIN, **common), s.L,
                      stream=stream)
     h_f64c = Handle(_lib.make_params(precision="fp64", precond="conductor", restart=RESTART, **common), s.L,
@@ -639,7 +640,7 @@ def main() -> None:
         "warmup": args.warmup, "ms_per_step": ms_fast, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 operator / f64 Krylov", "data": "synthetic",
         "config": {"workload": WORKLOAD, "charges": s.n_beads, "bodies": s.n_bodies, "mesh": p["grid"],
-                   "support": p["support"], "rcut": p["rcut"], "xi": p["xi"], "tol": TOL, "restart": RESTART,
+                   "support": p["support"], "rcut": p["rcut"], "xi": p["xi"], "tol": TOL, "restart": args.restart,
                    "preconditioner": {"two_level": "two-level (conductor response + induced-dipole coarse "
                                                     "correction)", "conductor": "conductor response"}[args.precond],
                    "learned": bool(args.learned),

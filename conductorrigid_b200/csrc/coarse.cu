@@ -178,6 +178,7 @@ __device__ __forceinline__ float table_lerp32(const float2 *__restrict__ tab, in
 }
 
 struct RealArgs {
+    double Ld[3];
     float L[3], Linv[3];
     float rc, rc2, rmin2, dr, inv_dr;
     int ntab;
@@ -187,11 +188,16 @@ struct RealArgs {
 // One CTA per ordered near pair p = (a, b):  W_p[k][c] = sum_{j in b} T(d_kj) z_bc(j) for
 // the beads k of a (the operator's pair rule dr <= d < rc under the minimum image), and
 // C[3a+e][3b+c] += sum_k z_ae(k) W_p[k][c] (+ the self term when a == b).
+// SHIFT (boxes of edge >= 2 (rc + 2 max radius)): every bead pair of two near bodies takes
+// the image of the centroids' minimum image, so positions are staged relative to a's
+// centroid once per bead and the pair loop needs no minimum image; otherwise each bead
+// pair takes its own.
+template <bool SHIFT>
 __global__ void __launch_bounds__(256) coarse_real_kernel(
     const int *__restrict__ pair_a, const int *__restrict__ pair_b, const long long *__restrict__ woff,
     const int *__restrict__ cbody, const int *__restrict__ body_start, const int *__restrict__ members,
-    const float4 *__restrict__ pos, const double *__restrict__ zq, const float2 *__restrict__ tab, RealArgs g,
-    int ldc, float *__restrict__ W, double *__restrict__ C) {
+    const double4 *__restrict__ pos, const double4 *__restrict__ cent, const double *__restrict__ zq,
+    const float2 *__restrict__ tab, RealArgs g, int ldc, float *__restrict__ W, double *__restrict__ C) {
     __shared__ float4 sp[kChunk];
     __shared__ float2 sz[kChunk];
     __shared__ double red[9 * 32];
@@ -200,16 +206,26 @@ __global__ void __launch_bounds__(256) coarse_real_kernel(
     const int ba = cbody[a], bb = cbody[b];
     const int abeg = body_start[ba], na = body_start[ba + 1] - abeg;
     const int bbeg = body_start[bb], nbb = body_start[bb + 1] - bbeg;
+    const double4 ca = cent[ba], cb = cent[bb];
+    const double Ld[3] = {g.Ld[0], g.Ld[1], g.Ld[2]}, Li[3] = {1.0 / g.Ld[0], 1.0 / g.Ld[1], 1.0 / g.Ld[2]};
+    // b's centroid in the image nearest a's, relative to a's
+    const double sh[3] = {mimgd(cb.x - ca.x, Ld[0], Li[0]), mimgd(cb.y - ca.y, Ld[1], Li[1]),
+                          mimgd(cb.z - ca.z, Ld[2], Li[2])};
     double cacc[9];
 #pragma unroll
     for (int t = 0; t < 9; ++t) cacc[t] = 0.0;
     for (int k0 = 0; k0 < na; k0 += blockDim.x) {
         const int k = k0 + threadIdx.x;
-        float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+        float3 pi = make_float3(0.f, 0.f, 0.f);
         float zi[3] = {0.f, 0.f, 0.f};
         if (k < na) {
             const int i = members[abeg + k];
-            pi = pos[i];
+            const double4 q = pos[i];
+            if (SHIFT)
+                pi = make_float3((float)mimgd(q.x - ca.x, Ld[0], Li[0]), (float)mimgd(q.y - ca.y, Ld[1], Li[1]),
+                                 (float)mimgd(q.z - ca.z, Ld[2], Li[2]));
+            else
+                pi = make_float3((float)q.x, (float)q.y, (float)q.z);
             for (int c = 0; c < 3; ++c) zi[c] = (float)zq[3 * i + c];
         }
         float acc[3] = {0.f, 0.f, 0.f};
@@ -218,17 +234,27 @@ __global__ void __launch_bounds__(256) coarse_real_kernel(
             __syncthreads();
             for (int t = threadIdx.x; t < nj; t += blockDim.x) {
                 const int j = members[bbeg + j0 + t];
-                const float4 q = pos[j];
-                sp[t] = make_float4(q.x, q.y, q.z, (float)zq[3 * j]);
+                const double4 q = pos[j];
+                float3 r;
+                if (SHIFT)
+                    r = make_float3((float)(mimgd(q.x - cb.x, Ld[0], Li[0]) + sh[0]),
+                                    (float)(mimgd(q.y - cb.y, Ld[1], Li[1]) + sh[1]),
+                                    (float)(mimgd(q.z - cb.z, Ld[2], Li[2]) + sh[2]));
+                else
+                    r = make_float3((float)q.x, (float)q.y, (float)q.z);
+                sp[t] = make_float4(r.x, r.y, r.z, (float)zq[3 * j]);
                 sz[t] = make_float2((float)zq[3 * j + 1], (float)zq[3 * j + 2]);
             }
             __syncthreads();
             if (k < na) {
                 for (int t = 0; t < nj; ++t) {
                     const float4 q = sp[t];
-                    const float dx = mimgf(pi.x - q.x, g.L[0], g.Linv[0]);
-                    const float dy = mimgf(pi.y - q.y, g.L[1], g.Linv[1]);
-                    const float dz = mimgf(pi.z - q.z, g.L[2], g.Linv[2]);
+                    float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+                    if (!SHIFT) {
+                        dx = mimgf(dx, g.L[0], g.Linv[0]);
+                        dy = mimgf(dy, g.L[1], g.Linv[1]);
+                        dz = mimgf(dz, g.L[2], g.Linv[2]);
+                    }
                     const float d2 = dx * dx + dy * dy + dz * dz;
                     if (d2 < g.rc2 && d2 >= g.rmin2) {
                         const float T = table_lerp32(tab, g.ntab, g.rc, g.dr, g.inv_dr, sqrtf(d2));
@@ -754,7 +780,9 @@ int coarse_prepare(cr_handle *h) {
         nbc, cs.cbody, cs.cent, L, Linv, rc, cs.pcount, nullptr, nullptr);
     CR_LAUNCH(h, "near_pairs_kernel");
     std::vector<int> pcount(nbc), phead(nbc);
+    std::vector<double4> cent(B);
     CR_CUDA(h, cudaMemcpyAsync(pcount.data(), cs.pcount, nbc * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CR_CUDA(h, cudaMemcpyAsync(cent.data(), cs.cent, B * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
     CR_CUDA(h, cudaStreamSynchronize(h->stream));
     long long npairs = 0, wtotal = 0;
     std::vector<long long> woff;
@@ -856,9 +884,14 @@ int coarse_prepare(cr_handle *h) {
     syrk_kernel<<<tg, 256, 0, h->stream>>>(nc, K2, cs.F, K2, cs.C, np);
     CR_LAUNCH(h, "syrk_kernel");
     RealArgs ra;
+    double max_rad = 0.0;
+    for (int b : cbody) max_rad = std::max(max_rad, cent[b].w);
+    bool shift = true;
     for (int d = 0; d < 3; ++d) {
+        ra.Ld[d] = h->L[d];
         ra.L[d] = (float)h->L[d];
         ra.Linv[d] = (float)(1.0 / h->L[d]);
+        shift = shift && h->L[d] >= 2.0 * (h->d.rcut + 2.0 * max_rad) + 1e-6;
     }
     ra.rc = (float)h->d.rcut;
     ra.rc2 = (float)(h->d.rcut * h->d.rcut);
@@ -867,9 +900,14 @@ int coarse_prepare(cr_handle *h) {
     ra.inv_dr = (float)(1.0 / h->d.dr);
     ra.ntab = h->d.n_table;
     ra.selfc = h->d.selfcoeff;
-    coarse_real_kernel<<<(unsigned)npairs, bs, 0, h->stream>>>(cs.pair_a, cs.pair_b, cs.woff, cs.cbody,
-                                                                 h->d_body_start, h->d_body_members, h->m32.pos,
-                                                                 cs.zq, h->m32.phiq, ra, np, cs.W, cs.C);
+    if (shift)
+        coarse_real_kernel<true><<<(unsigned)npairs, bs, 0, h->stream>>>(
+            cs.pair_a, cs.pair_b, cs.woff, cs.cbody, h->d_body_start, h->d_body_members, h->m64.pos, cs.cent, cs.zq,
+            h->m32.phiq, ra, np, cs.W, cs.C);
+    else
+        coarse_real_kernel<false><<<(unsigned)npairs, bs, 0, h->stream>>>(
+            cs.pair_a, cs.pair_b, cs.woff, cs.cbody, h->d_body_start, h->d_body_members, h->m64.pos, cs.cent, cs.zq,
+            h->m32.phiq, ra, np, cs.W, cs.C);
     CR_LAUNCH(h, "coarse_real_kernel");
     symmetrise_kernel<<<blocks_for((long)nc * nc, 256), 256, 0, h->stream>>>(nc, cs.C, np);
     CR_LAUNCH(h, "symmetrise_kernel");

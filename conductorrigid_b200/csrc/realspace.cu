@@ -29,6 +29,7 @@
 // cluster pairs in FP64.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "cr_internal.cuh"
@@ -160,9 +161,15 @@ __device__ __forceinline__ double table_lerp64(const double2 *__restrict__ tab, 
 
 // Bit masks of the in-range bead pairs of every cluster pair (row i = bead i of I,
 // bit j = bead j of J) and the stored slots of the pair (32 x its longest row).
+// The test runs on the FP32 copies of the positions; only a pair whose FP32 squared
+// distance lies within `band` of rc^2 (or below 2 dr^2 + band) is decided again in FP64,
+// exactly as the oracle decides it.  `band` is ten times a bound on the FP32 error of
+// d^2 for |d| <= rc in a box of edge L (positions rounded to FP32: |error of dx| <= 2e-7 L),
+// so the masks equal the FP64 ones bit for bit.
 __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
-                                 const int *__restrict__ members, const double4 *__restrict__ pos, RSBuild c,
-                                 unsigned *__restrict__ masks, int *__restrict__ nnz,
+                                 const int *__restrict__ members, const double4 *__restrict__ pos,
+                                 const float4 *__restrict__ pos32, RSBuild c, float3 L32, float3 Linv32, float rc2,
+                                 float band, float low, unsigned *__restrict__ masks, int *__restrict__ nnz,
                                  unsigned long long *__restrict__ bits) {
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -170,20 +177,34 @@ __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_
     const int I = pair_i[p], J = pair_j[p];
     const int bi = members[I * CS + lane];
     const int bj = members[J * CS + lane];
-    const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
-    const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
+    const float4 pi = bi >= 0 ? pos32[bi] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 pjl = bj >= 0 ? pos32[bj] : make_float4(0.f, 0.f, 0.f, 0.f);
     unsigned m = 0;
     for (int j = 0; j < CS; ++j) {
         const int vj = __shfl_sync(0xffffffffu, bj, j);
-        const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
-        const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
-        const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
+        const float xj = __shfl_sync(0xffffffffu, pjl.x, j);
+        const float yj = __shfl_sync(0xffffffffu, pjl.y, j);
+        const float zj = __shfl_sync(0xffffffffu, pjl.z, j);
         if (bi >= 0 && vj >= 0) {
-            const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
-            const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
-            const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
-            const double d2 = dx * dx + dy * dy + dz * dz;
-            if (d2 < c.rc2 && d2 >= c.rmin2) m |= 1u << j;
+            float dx = pi.x - xj, dy = pi.y - yj, dz = pi.z - zj;
+            dx -= L32.x * rintf(dx * Linv32.x);
+            dy -= L32.y * rintf(dy * Linv32.y);
+            dz -= L32.z * rintf(dz * Linv32.z);
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            bool in;
+            if (d2 > rc2 + band) {
+                in = false;
+            } else if (d2 < rc2 - band && d2 > low) {
+                in = true;
+            } else {  // near a boundary: the FP64 decision
+                const double4 a = pos[bi], b = pos[vj];
+                const double ex = mimg(a.x - b.x, c.L[0], c.Linv[0]);
+                const double ey = mimg(a.y - b.y, c.L[1], c.Linv[1]);
+                const double ez = mimg(a.z - b.z, c.L[2], c.Linv[2]);
+                const double e2 = ex * ex + ey * ey + ez * ez;
+                in = e2 < c.rc2 && e2 >= c.rmin2;
+            }
+            if (in) m |= 1u << j;
         }
     }
     masks[p * CS + lane] = m;
@@ -581,8 +602,16 @@ int realspace_build(cr_handle *h) {
     CR_LAUNCH(h, "pair_owner_kernel");
     const int pb = blocks_for(r.npairs * 32, 256);
     CR_CUDA(h, cudaMemsetAsync(r.bits, 0, sizeof(unsigned long long), s));
-    pair_mask_kernel<<<pb, 256, 0, s>>>(r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, c, r.masks, r.nnz_pair,
-                                        r.bits);
+    {
+        const double Lmax = std::max(h->L[0], std::max(h->L[1], h->L[2]));
+        const float band = (float)(1e-5 * c.rc * Lmax + 4e-6 * c.rc2);
+        const float low = (float)(2.0 * c.rmin2) + band;
+        pair_mask_kernel<<<pb, 256, 0, s>>>(r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m32.pos, c,
+                                            make_float3((float)h->L[0], (float)h->L[1], (float)h->L[2]),
+                                            make_float3((float)(1.0 / h->L[0]), (float)(1.0 / h->L[1]),
+                                                        (float)(1.0 / h->L[2])),
+                                            (float)c.rc2, band, low, r.masks, r.nnz_pair, r.bits);
+    }
     CR_LAUNCH(h, "pair_mask_kernel");
     bytes = h->sort_tmp_bytes;
     CR_CUDA(h, cub::DeviceScan::ExclusiveSum(h->d_sort_tmp, bytes, r.nnz_pair, r.voff, (int)r.npairs, s));
