@@ -454,7 +454,7 @@ def main() -> None:
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=[WORKLOAD, "replicas_256", "dynamics_420k", "mlp", "polydisperse_204k"],
                     help="headline solve (default), 256 batched replicas, or Brownian dynamics")
-    ap.add_argument("--scale", type=float, default=1.0, help="dynamics workload: body-count fraction")
+    ap.add_argument("--scale", type=float, default=1.0, help="body-count fraction (dynamics; headline profiling cases)")
     ap.add_argument("--tiling", default="", help="T,MODE: fixed mesh tiling of the headline solver instead of "
                                                  "cr_autotune (for runs under a profiler)")
     ap.add_argument("--restart", type=int, default=RESTART, help="FGMRES restart of the headline (fast) arm")
@@ -502,8 +502,11 @@ def main() -> None:
     def max_over_ranks(v: float) -> float:
         return ranks.max_over_ranks(v, world, device="cuda")
 
-    w = systems.workload(WORKLOAD, seed=ranks.replica_seed(1, rank))
+    w = systems.workload(WORKLOAD, seed=ranks.replica_seed(1, rank), scale=args.scale)
     s, p = w.system, w.params
+    if args.scale != 1.0:  # profiling case: fewer bodies at the same mesh spacing
+        full_L = systems.workload(WORKLOAD).system.L[0]
+        p = dict(p, grid=systems.smooth_at_least(int(np.ceil(p["grid"] * s.L[0] / full_L)), 4096))
     base = {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")}
     common = dict(field=tuple(s.field), gmres_tol=TOL, maxiter=20000, **base)
     stream = torch.cuda.Stream()

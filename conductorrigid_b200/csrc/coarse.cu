@@ -168,19 +168,20 @@ __global__ void near_pairs_kernel(int nbc, const int *__restrict__ cbody, const 
     if (!FILL && lane == 0) count[a] = n;
 }
 
-__device__ __forceinline__ float table_lerp32(const float2 *__restrict__ tab, int ntab, float rc, float dr,
+// T(d) from the FP32 table with the reference's index and weight (ConductorRigid.cu:549-554):
+// index floor((d - dr) ntab / (rc - dr)) (scale = ntab / (rc - dr)), weight d/dr - index - 1.
+__device__ __forceinline__ float table_lerp32(const float2 *__restrict__ tab, int ntab, float scale, float dr,
                                               float inv_dr, float d) {
-    int ind = (int)floorf(ntab * (d - dr) / (rc - dr));
-    ind = min(max(ind, 0), ntab - 1);
-    const float lin = d * inv_dr - ind - 1.0f;
-    const float2 e = tab[ind];
-    return e.x + (e.y - e.x) * lin;
+    const int ind = min(max((int)((d - dr) * scale), 0), ntab - 1);
+    const float lin = fmaf(d, inv_dr, -1.0f) - (float)ind;
+    const float2 e = __ldg(tab + ind);
+    return fmaf(e.y - e.x, lin, e.x);
 }
 
 struct RealArgs {
     double Ld[3];
     float L[3], Linv[3];
-    float rc, rc2, rmin2, dr, inv_dr;
+    float rc, rc2, rmin2, dr, inv_dr, scale;
     int ntab;
     double selfc;
 };
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(256) coarse_real_kernel(
                     }
                     const float d2 = dx * dx + dy * dy + dz * dz;
                     if (d2 < g.rc2 && d2 >= g.rmin2) {
-                        const float T = table_lerp32(tab, g.ntab, g.rc, g.dr, g.inv_dr, sqrtf(d2));
+                        const float T = table_lerp32(tab, g.ntab, g.scale, g.dr, g.inv_dr, d2 * rsqrtf(d2));
                         const float2 z12 = sz[t];
                         acc[0] += T * q.w;
                         acc[1] += T * z12.x;
@@ -267,7 +268,7 @@ __global__ void __launch_bounds__(256) coarse_real_kernel(
             }
         }
         if (k < na) {
-            float *w = W + woff[p] + 3 * (size_t)k;
+            float *w = W + woff[p] + 3 * (size_t)k;  // [na][3]
             for (int c = 0; c < 3; ++c) w[c] = acc[c];
             for (int e = 0; e < 3; ++e)
                 for (int c = 0; c < 3; ++c) {
@@ -627,6 +628,15 @@ __global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__
     __syncthreads();
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
         const int i = members[beg + k];
+        double m0 = 0.0, m1 = 0.0;
+#pragma unroll 4
+        for (int q = 0; q < npr; ++q) {
+            const double2 y01 = sy[2 * q], y2o = sy[2 * q + 1];
+            const float *w = W + __double_as_longlong(y2o.y) + 3 * (size_t)k;
+            const float w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+            m0 += (double)w0 * y01.x + (double)w1 * y01.y;
+            m1 += (double)w2 * y2o.x;
+        }
         const double4 p = pos[i];
         const float fx = (float)(p.x * Linv.x), fy = (float)(p.y * Linv.y), fz = (float)(p.z * Linv.z);
         float sz, cz;
@@ -637,30 +647,20 @@ __global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__
             const int end = q + 1 < nrows ? srow[q + 1].w : nmodes;
             float s, c;
             sincospif(2.0f * ((float)r.x * fx + (float)r.y * fy + (float)r.z * fz), &s, &c);
-            for (int m = r.w; m < end; ++m) {
-                const float2 uu = su[m];
+            for (int mm = r.w; mm < end; ++mm) {
+                const float2 uu = su[mm];
                 wave += c * uu.x - s * uu.y;
                 const float c2 = c * cz - s * sz;
                 s = s * cz + c * sz;
                 c = c2;
             }
         }
-        double m = (double)wave;
+        double m = (double)wave + m0 + m1;
         double phi = 0.0;
         if (a >= 0) {
             const double y0 = y[3 * a], y1 = y[3 * a + 1], y2 = y[3 * a + 2];
             m += selfc * (zq[3 * i] * y0 + zq[3 * i + 1] * y1 + zq[3 * i + 2] * y2);
             phi = zp[3 * b] * y0 + zp[3 * b + 1] * y1 + zp[3 * b + 2] * y2;
-            double m0 = 0.0, m1 = 0.0;
-#pragma unroll 4
-            for (int q = 0; q < npr; ++q) {
-                const double2 y01 = sy[2 * q], y2o = sy[2 * q + 1];
-                const float *w = W + __double_as_longlong(y2o.y) + 3 * (size_t)k;
-                const float w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
-                m0 += (double)w0 * y01.x + (double)w1 * y01.y;
-                m1 += (double)w2 * y2o.x;
-            }
-            m += m0 + m1;
         }
         t[i] = x[i] - (phi - m);
     }
@@ -898,6 +898,7 @@ int coarse_prepare(cr_handle *h) {
     ra.rmin2 = (float)(h->d.dr * h->d.dr);
     ra.dr = (float)h->d.dr;
     ra.inv_dr = (float)(1.0 / h->d.dr);
+    ra.scale = (float)(h->d.n_table / (h->d.rcut - h->d.dr));
     ra.ntab = h->d.n_table;
     ra.selfc = h->d.selfcoeff;
     if (shift)

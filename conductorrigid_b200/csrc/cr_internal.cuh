@@ -167,7 +167,7 @@ struct CoarseSpace {
     float *W = nullptr;                 // per pair: [n_a][3] real-space blocks M_real Z_q
     float4 *kv = nullptr;               // [nmodes] (mx, my, mz, sqrt w)
     int4 *rows = nullptr;               // [nrows] runs of consecutive mz: (mx, my, mz0, first mode)
-    int nrows = 0, bs = 128;            // runs; threads per body CTA
+    int nrows = 0, bs = 128;            // runs; threads per body CTA of the A~ Z y kernel
     size_t model_smem = 0;              // dynamic shared memory of the A~ Z y kernel
     float *F = nullptr, *FT = nullptr;  // [nc][K2] scaled structure factors, [K2][np] transpose
     double *C = nullptr;                // [np][np] coarse operator (assembled in FP64)
