@@ -249,25 +249,26 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
     const unsigned m = masks[p * CS + lane];
     R *out = vals + voff[p] + lane;
     double *out2 = BOTH ? vals2 + voff[p] + lane : nullptr;
-    int k = 0;
-    for (int j = 0; j < CS; ++j) {
+    // lane i walks its own set bits (the k-th bit j at step k), fetching bead j's position
+    // from lane j; lanes past their last bit write the zero padding of the slot
+    const int rows = slots[p] / CS;
+    unsigned mm = m;
+    for (int k = 0; k < rows; ++k) {
+        const bool has = mm != 0;
+        const int j = has ? __ffs(mm) - 1 : 0;
+        mm &= mm - 1;
         const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
         const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
         const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
-        if (m & (1u << j)) {
+        double t = 0.0;
+        if (has) {
             const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
             const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
             const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
-            const double t = table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
-            out[(size_t)k * CS] = (R)t;
-            if (BOTH) out2[(size_t)k * CS] = t;
-            ++k;
+            t = table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
         }
-    }
-    const int rows = slots[p] / CS;
-    for (; k < rows; ++k) {
-        out[(size_t)k * CS] = (R)0;
-        if (BOTH) out2[(size_t)k * CS] = 0.0;
+        out[(size_t)k * CS] = (R)t;
+        if (BOTH) out2[(size_t)k * CS] = t;
     }
 }
 
@@ -394,12 +395,19 @@ __global__ void __launch_bounds__(W * 32) pair_force_kernel(const long long *__r
         const int bj = members[J * CS + lane];
         const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
         const double qjl = bj >= 0 ? q[bj] : 0.0;
-        for (int j = 0; j < CS; ++j) {
+        // lane i walks its own set bits in ascending order (the in-range test of
+        // pair_mask_kernel), the warp as many steps as its longest row
+        const unsigned steps = __reduce_max_sync(0xffffffffu, (unsigned)__popc(m));
+        unsigned mm = m;
+        for (unsigned t = 0; t < steps; ++t) {
+            const bool has = mm != 0;
+            const int j = has ? __ffs(mm) - 1 : 0;
+            mm &= mm - 1;
             const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
             const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
             const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
             const double qj = __shfl_sync(0xffffffffu, qjl, j);
-            if (m & (1u << j)) {  // the in-range test of pair_mask_kernel
+            if (has) {
                 const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
                 const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
                 const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
