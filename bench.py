@@ -279,7 +279,7 @@ def run_dynamics(args) -> None:
     grid = p["grid"] if args.scale == 1.0 else systems.smooth_at_least(int(np.ceil(256 * s.L[0] / 49.28)), 4096)
     common = dict(field=tuple(s.field), xi=p["xi"], errortol=p["errortol"], grid=grid, support=p["support"],
                   rcut=p["rcut"], gmres_tol=TOL, restart=RESTART, maxiter=20000, precision="mixed",
-                  precond="conductor")
+                  precond=args.precond)
     steps = args.warmup + args.steps
     train = min(200, max(1, steps // 2))
     out, guess = paired_run(_lib.make_params(**common), _lib.make_params(learned=True, **common), s,
@@ -297,6 +297,7 @@ def run_dynamics(args) -> None:
         "value": arm("learned")["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": len(tail),
         "warmup": len(out) - len(tail), "higher_is_better": True,
         "learned": arm("learned"), "plain_warm_start": arm("plain"), "trained_solves": guess.trained,
+        "preconditioner": args.precond,
         "heldout_explained": round(float(np.mean(guess.heldout[-len(tail):])) if guess.heldout else 0.0, 3),
         "dtype": "f32 operator, f64 Krylov; bf16 network", "data": "synthetic (seeded placement, relaxed)",
         "config": {"workload": f"dynamics_420k scale {args.scale}: {s.n_bodies} spheres x 42, phi 0.35, "
@@ -377,10 +378,11 @@ def run_polydisperse(args) -> None:
     base = {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")}
     common = dict(field=tuple(s.field), maxiter=40000, **base)
     stream = torch.cuda.Stream()
-    # the conductor response: at phi = 0.25 the induced-dipole coarse level saves 75 -> 57
-    # iterations but its set-up and application cost more than that (136 vs 130 ms per solve)
-    h_fast = Handle(_lib.make_params(precision="mixed", precond="conductor", restart=RESTART, gmres_tol=TOL,
+    # default: the conductor response; at phi = 0.25 the dense induced-dipole coarse level
+    # saves 75 -> 57 iterations but costs more than that (136 vs 130 ms per solve)
+    h_fast = Handle(_lib.make_params(precision="mixed", precond=args.precond, restart=RESTART, gmres_tol=TOL,
                                      **common), s.L, stream=stream)
+    h_fast.set_coarse(args.coarse_max_dense, args.coarse_cg)
     h_plain = Handle(_lib.make_params(precision="fp64", precond="diagonal", restart=RESTART_PLAIN, gmres_tol=TOL,
                                       **common), s.L, stream=stream)
     h_ref = Handle(_lib.make_params(precision="fp64", precond="conductor", restart=RESTART, gmres_tol=1e-10,
@@ -421,7 +423,8 @@ def run_polydisperse(args) -> None:
         "value": round(1e3 / ms_fast, 3), "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_fast, 1), "higher_is_better": True,
         "iterations": st["iterations"], "final_residual": st["final_residual"],
-        "preconditioner": "conductor",
+        "preconditioner": args.precond,
+        "coarse_level": h_fast.coarse_info() if args.precond == "two_level" else None,
         "plain_fp64": {"value": round(1e3 / ms_plain, 4), "ms_per_step": round(ms_plain, 1),
                        "iterations": stp["iterations"], "converged": stp["converged"],
                        "final_residual": stp["final_residual"]},
@@ -458,10 +461,17 @@ def main() -> None:
     ap.add_argument("--tiling", default="", help="T,MODE: fixed mesh tiling of the headline solver instead of "
                                                  "cr_autotune (for runs under a profiler)")
     ap.add_argument("--restart", type=int, default=RESTART, help="FGMRES restart of the headline (fast) arm")
-    ap.add_argument("--precond", default="two_level", choices=["two_level", "conductor"],
-                    help="preconditioner of the headline (fast) arm")
+    ap.add_argument("--precond", default=None, choices=["two_level", "conductor"],
+                    help="preconditioner of the fast arm (default: two_level; conductor for the polydisperse "
+                         "mixture and the dynamics)")
+    ap.add_argument("--coarse-max-dense", type=int, default=12288,
+                    help="coarse problems above this many unknowns use the sparse form (--coarse-cg steps of CG on "
+                         "near-pair blocks) or, with --coarse-cg 0, no coarse level")
+    ap.add_argument("--coarse-cg", type=int, default=0, help="CG steps of the sparse coarse form")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.precond is None:
+        args.precond = "conductor" if args.workload in ("polydisperse_204k", "dynamics_420k") else "two_level"
     if args.impl == "ours" and args.workload == "replicas_256":
         run_replicas(args)
         return
@@ -512,6 +522,7 @@ def main() -> None:
     stream = torch.cuda.Stream()
     h_fast = Handle(_lib.make_params(precision="mixed", learned=bool(args.learned), precond=args.precond,
                                      restart=args.restart, **common), s.L, stream=stream)
+    h_fast.set_coarse(args.coarse_max_dense, args.coarse_cg)
     h_plain = Handle(_lib.make_params(precision="fp64", precond="diagonal", restart=RESTART_PLAIN, **common), s.L,
                      stream=stream)
     h_f64c = Handle(_lib.make_params(precision="fp64", precond="conductor", restart=RESTART, **common), s.L,

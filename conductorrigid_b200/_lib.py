@@ -151,7 +151,9 @@ _SIGS = {
     "cr_set_positions": ([_P, _P, _P], _I),
     "cr_apply_operator": ([_P, _P, _P, _I], _I),
     "cr_precondition": ([_P, _P, _P], _I),
-    "cr_coarse_info": ([_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int)], _I),
+    "cr_coarse_info": ([_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                        C.POINTER(C.c_int)], _I),
+    "cr_set_coarse": ([_P, C.c_int, C.c_int], _I),
     "cr_objective": ([_P, _P], _I),
     "cr_wave_potential": ([_P, _P, _P, _I], _I),
     "cr_spread": ([_P, _P, _P, _I], _I),

@@ -412,7 +412,7 @@ int cr_precondition(cr_handle *h, const double *d_x, double *d_y) {
     return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_precondition");
 }
 
-int cr_coarse_info(cr_handle *h, int *active, int *n_coarse, long long *n_pairs, int *n_modes) {
+int cr_coarse_info(cr_handle *h, int *active, int *n_coarse, long long *n_pairs, int *n_modes, int *sparse) {
     CR_TRY(need_ready(h));
     CR_TRY(coarse_prepare(h));
     const CoarseSpace &c = h->coarse;
@@ -421,7 +421,19 @@ int cr_coarse_info(cr_handle *h, int *active, int *n_coarse, long long *n_pairs,
     if (n_coarse) *n_coarse = on ? c.nc : 0;
     if (n_pairs) *n_pairs = on ? c.npairs : 0;
     if (n_modes) *n_modes = on ? c.nmodes : 0;
+    if (sparse) *sparse = on && c.sparse ? 1 : 0;
     return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_coarse_info");
+}
+
+int cr_set_coarse(cr_handle *h, int max_dense, int pcg_iterations) {
+    if (!h) return CR_BAD_PARAM;
+    if (max_dense < 0 || pcg_iterations < 0 || pcg_iterations > 64)
+        return fail(h, CR_BAD_PARAM, "cr_set_coarse: max_dense >= 0 and 0 <= pcg_iterations <= 64");
+    h->coarse.max_dense = max_dense;
+    h->coarse.pcg_iters = pcg_iterations;
+    h->coarse.gen = -1;                                // rebuilt by the next solve
+    h->kry.exec_gen[0] = h->kry.exec_gen[1] = -1;      // captured steps hold the old sequence
+    return CR_OK;
 }
 
 int cr_objective(cr_handle *h, double *d_rhs) {

@@ -28,6 +28,11 @@
 // P the conductor response.  A~ Z y = [Phi(Z y) - M~ Z_q y ; 0] is evaluated from blocks
 // W = M_real Z_q stored per pair of near bodies and from the same k-sum; C^-1 is formed
 // once per geometry (assembled in FP64, inverted in place by blocked Gauss-Jordan in FP32).
+// Above a dense limit (max_dense coarse unknowns, 12,288 by default) the level is skipped
+// unless the caller asks for the sparse form (cr_set_coarse with CG steps > 0): the coarse
+// operator then keeps only its self and real-space terms, stored as 3 x 3 blocks of the
+// near pairs, and C y = -Z^T r is solved by that many block-Jacobi preconditioned CG
+// steps; no wave-space term is used in C or in A~ Z y there.
 // In flexible GMRES any preconditioner leaves the solution unchanged: only the iteration
 // count moves (at 162 beads per sphere, phi = 0.30: 133 -> 40 iterations against the
 // conductor response alone, on 100 bodies).
@@ -42,7 +47,7 @@ namespace cr {
 namespace {
 
 constexpr int kMinBeads = 4;        // bodies with fewer beads get no coarse vectors
-constexpr int kMaxCoarse = 12288;   // coarse unknowns above which the level is skipped
+constexpr int kMaxSparse = 786432;  // coarse unknowns above which the level is skipped
 constexpr int kMaxModes = 1024;     // half-space wave vectors kept (kc shrinks above)
 constexpr int NB = 64;              // Gauss-Jordan block
 constexpr int kChunk = 512;         // beads staged in shared memory per pass
@@ -198,7 +203,8 @@ __global__ void __launch_bounds__(256) coarse_real_kernel(
     const int *__restrict__ pair_a, const int *__restrict__ pair_b, const long long *__restrict__ woff,
     const int *__restrict__ cbody, const int *__restrict__ body_start, const int *__restrict__ members,
     const double4 *__restrict__ pos, const double4 *__restrict__ cent, const double *__restrict__ zq,
-    const float2 *__restrict__ tab, RealArgs g, int ldc, float *__restrict__ W, double *__restrict__ C) {
+    const float2 *__restrict__ tab, RealArgs g, int ldc, float *__restrict__ W, double *__restrict__ C,
+    double *__restrict__ Cblk) {
     __shared__ float4 sp[kChunk];
     __shared__ float2 sz[kChunk];
     __shared__ double red[9 * 32];
@@ -282,9 +288,14 @@ __global__ void __launch_bounds__(256) coarse_real_kernel(
         }
     }
     block_sum<9>(cacc, red);
-    if (threadIdx.x == 0)
-        for (int e = 0; e < 3; ++e)
-            for (int c = 0; c < 3; ++c) C[(size_t)(3 * a + e) * ldc + 3 * b + c] += cacc[3 * e + c];
+    if (threadIdx.x == 0) {
+        if (Cblk) {  // sparse coarse operator: the pair's own 3 x 3 block
+            for (int t = 0; t < 9; ++t) Cblk[9 * (size_t)p + t] = cacc[t];
+        } else {
+            for (int e = 0; e < 3; ++e)
+                for (int c = 0; c < 3; ++c) C[(size_t)(3 * a + e) * ldc + 3 * b + c] += cacc[3 * e + c];
+        }
+    }
 }
 
 // Structure factors of the coarse columns: F[3a+e][2m] = sqrt(w_m) Re S_ae(k_m),
@@ -537,6 +548,171 @@ __global__ void to_float_kernel(long long n, const double *__restrict__ a, float
     if (t < n) b[t] = (float)a[t];
 }
 
+// ---- sparse coarse level: block-Jacobi preconditioned CG on the near-pair blocks ----
+// For coarse problems above the dense limit the coarse operator keeps only the self and
+// real-space terms (C_ab = Z_a^T M_real Z_b for near pairs, 3 x 3 blocks) and C y = -g is
+// solved approximately by a fixed number of conjugate-gradient steps with the inverse
+// diagonal blocks as preconditioner; the flexible outer iteration accepts the resulting
+// (slightly varying) preconditioner.  Sums over blocks are reduced in a fixed order.
+constexpr int kVecThreads = 256, kSpmvWarpsC = 8;
+
+// sum of a[0..n) on every thread of the block (fixed order: strided partial sums, tree)
+__device__ double block_sum_array(const double *__restrict__ a, int n, double *red /* [32] */) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v += a[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += red[w];
+    __syncthreads();
+    return t;
+}
+
+__device__ __forceinline__ void mat3_vec(const double *__restrict__ M, const double v[3], double out[3]) {
+    for (int e = 0; e < 3; ++e) out[e] = M[3 * e] * v[0] + M[3 * e + 1] * v[1] + M[3 * e + 2] * v[2];
+}
+
+// inverse of each body's diagonal block (symmetrised); a block that is not positive
+// definite sets *flag
+__global__ void block_jacobi_kernel(int nbc, const int *__restrict__ phead, const int *__restrict__ pcount,
+                                    const int *__restrict__ pair_b, const double *__restrict__ Cblk,
+                                    double *__restrict__ Dblk, int *__restrict__ flag) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nbc) return;
+    int q = -1;
+    for (int k = 0; k < pcount[a]; ++k)
+        if (pair_b[phead[a] + k] == a) q = phead[a] + k;
+    double m[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (q >= 0)
+        for (int e = 0; e < 3; ++e)
+            for (int c = 0; c < 3; ++c) m[3 * e + c] = 0.5 * (Cblk[9 * (size_t)q + 3 * e + c] + Cblk[9 * (size_t)q + 3 * c + e]);
+    const double c00 = m[4] * m[8] - m[5] * m[7], c01 = m[5] * m[6] - m[3] * m[8], c02 = m[3] * m[7] - m[4] * m[6];
+    const double det = m[0] * c00 + m[1] * c01 + m[2] * c02;
+    double *d = Dblk + 9 * (size_t)a;
+    if (!(det > 0.0) || !(m[0] > 0.0) || !isfinite(det)) {
+        atomicExch(flag, 1);
+        for (int t = 0; t < 9; ++t) d[t] = 0.0;
+        return;
+    }
+    const double id = 1.0 / det;
+    d[0] = c00 * id;
+    d[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+    d[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+    d[3] = c01 * id;
+    d[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+    d[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    d[6] = c02 * id;
+    d[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+    d[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+// y = 0, r = -g, z = D r, p = z; partial r.z per block
+__global__ void __launch_bounds__(kVecThreads) pcg_init_kernel(int nbc, const double *__restrict__ Dblk,
+                                                               const double *__restrict__ g, double *__restrict__ y,
+                                                               double *__restrict__ r, double *__restrict__ z,
+                                                               double *__restrict__ p, double *__restrict__ part_rz) {
+    __shared__ double red[32];
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    double rz = 0.0;
+    if (a < nbc) {
+        const double rv[3] = {-g[3 * a], -g[3 * a + 1], -g[3 * a + 2]};
+        double zv[3];
+        mat3_vec(Dblk + 9 * (size_t)a, rv, zv);
+        for (int e = 0; e < 3; ++e) {
+            y[3 * a + e] = 0.0;
+            r[3 * a + e] = rv[e];
+            z[3 * a + e] = zv[e];
+            p[3 * a + e] = zv[e];
+            rz += rv[e] * zv[e];
+        }
+    }
+    double v[1] = {rz};
+    block_sum<1>(v, red);
+    if (threadIdx.x == 0) part_rz[blockIdx.x] = v[0];
+}
+
+// q = C p (one warp per body, lanes over its near pairs); partial p.q per block
+__global__ void __launch_bounds__(kSpmvWarpsC * 32) pcg_spmv_kernel(int nbc, const int *__restrict__ phead,
+                                                                    const int *__restrict__ pcount,
+                                                                    const int *__restrict__ pair_b,
+                                                                    const double *__restrict__ Cblk,
+                                                                    const double *__restrict__ p,
+                                                                    double *__restrict__ q,
+                                                                    double *__restrict__ part_pq) {
+    __shared__ double red[32];
+    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    double pq = 0.0;
+    if (a < nbc) {
+        double acc[3] = {0.0, 0.0, 0.0};
+        const int h0 = phead[a], n = pcount[a];
+        for (int k = lane; k < n; k += 32) {
+            const int b = pair_b[h0 + k];
+            const double pb[3] = {p[3 * b], p[3 * b + 1], p[3 * b + 2]};
+            double t[3];
+            mat3_vec(Cblk + 9 * (size_t)(h0 + k), pb, t);
+            for (int e = 0; e < 3; ++e) acc[e] += t[e];
+        }
+        for (int e = 0; e < 3; ++e)
+            for (int o = 16; o > 0; o >>= 1) acc[e] += __shfl_xor_sync(0xffffffffu, acc[e], o);
+        if (lane == 0) {
+            for (int e = 0; e < 3; ++e) q[3 * a + e] = acc[e];
+            pq = p[3 * a] * acc[0] + p[3 * a + 1] * acc[1] + p[3 * a + 2] * acc[2];
+        }
+    }
+    double v[1] = {pq};
+    block_sum<1>(v, red);
+    if (threadIdx.x == 0) part_pq[blockIdx.x] = v[0];
+}
+
+// alpha = (r.z) / (p.q); y += alpha p; r -= alpha q; z = D r; partial r.z (new) per block
+__global__ void __launch_bounds__(kVecThreads) pcg_update_kernel(int nbc, int nspmv, const double *__restrict__ part_pq,
+                                                                 int nvec, const double *__restrict__ part_rz,
+                                                                 const double *__restrict__ Dblk,
+                                                                 const double *__restrict__ p,
+                                                                 const double *__restrict__ q,
+                                                                 double *__restrict__ y, double *__restrict__ r,
+                                                                 double *__restrict__ z,
+                                                                 double *__restrict__ part_rz_next) {
+    __shared__ double red[32];
+    const double pq = block_sum_array(part_pq, nspmv, red);
+    const double rz = block_sum_array(part_rz, nvec, red);
+    const double alpha = pq > 0.0 ? rz / pq : 0.0;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    double rzn = 0.0;
+    if (a < nbc) {
+        double rv[3];
+        for (int e = 0; e < 3; ++e) {
+            y[3 * a + e] += alpha * p[3 * a + e];
+            rv[e] = r[3 * a + e] - alpha * q[3 * a + e];
+            r[3 * a + e] = rv[e];
+        }
+        double zv[3];
+        mat3_vec(Dblk + 9 * (size_t)a, rv, zv);
+        for (int e = 0; e < 3; ++e) {
+            z[3 * a + e] = zv[e];
+            rzn += rv[e] * zv[e];
+        }
+    }
+    double v[1] = {rzn};
+    block_sum<1>(v, red);
+    if (threadIdx.x == 0) part_rz_next[blockIdx.x] = v[0];
+}
+
+// p = z + beta p, beta = (r.z)_new / (r.z)_old
+__global__ void __launch_bounds__(kVecThreads) pcg_dir_kernel(int nbc, int nvec, const double *__restrict__ part_old,
+                                                              const double *__restrict__ part_new,
+                                                              const double *__restrict__ z, double *__restrict__ p) {
+    __shared__ double red[32];
+    const double ro = block_sum_array(part_old, nvec, red);
+    const double rn = block_sum_array(part_new, nvec, red);
+    const double beta = ro > 0.0 ? rn / ro : 0.0;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 3 * nbc) p[i] = z[i] + beta * p[i];
+}
+
 // ---- application ----
 
 // g[3a+e] = sum_{i in a} z_ae(i) x_i + zp[a][e] x[N+a]
@@ -708,6 +884,14 @@ void coarse_free(cr_handle *h) {
     dfree(&c.W);
     dfree(&c.kv);
     dfree(&c.rows);
+    dfree(&c.Cblk);
+    dfree(&c.Dblk);
+    dfree(&c.pr);
+    dfree(&c.pz);
+    dfree(&c.pp);
+    dfree(&c.pq);
+    dfree(&c.part_pq);
+    dfree(&c.part_rz);
     dfree(&c.F);
     dfree(&c.FT);
     dfree(&c.C);
@@ -719,7 +903,10 @@ void coarse_free(cr_handle *h) {
     dfree(&c.y);
     dfree(&c.u);
     dfree(&c.t);
+    const int max_dense = c.max_dense, pcg_iters = c.pcg_iters;  // caller settings survive
     c = CoarseSpace{};
+    c.max_dense = max_dense;
+    c.pcg_iters = pcg_iters;
 }
 
 int coarse_prepare(cr_handle *h) {
@@ -745,7 +932,8 @@ int coarse_prepare(cr_handle *h) {
             cbody.push_back(b);
         }
     const int nbc = (int)cbody.size(), nc = 3 * nbc;
-    if (nbc == 0 || nc > kMaxCoarse) {
+    const bool sparse = nc > cs.max_dense;  // above the dense limit: near-pair blocks and PCG
+    if (nbc == 0 || nc > kMaxSparse || (sparse && cs.pcg_iters == 0)) {
         cs.gen = h->geo_gen;
         return CR_OK;
     }
@@ -811,9 +999,9 @@ int coarse_prepare(cr_handle *h) {
 
     // wave vectors of the half space with 0 < |k| < kc (kc lowered if there are too many)
     const double xi = h->user.xi, V = h->L[0] * h->L[1] * h->L[2];
-    double kc = 2.0 * xi;
+    double kc = sparse ? 0.0 : 2.0 * xi;  // the sparse level keeps no wave-space term
     std::vector<float4> kv;
-    for (int attempt = 0; attempt < 40; ++attempt) {
+    for (int attempt = 0; attempt < 40 && kc > 0.0; ++attempt) {
         kv.clear();
         int mmax[3];
         for (int d = 0; d < 3; ++d) mmax[d] = (int)std::floor(kc * h->L[d] / (2.0 * kPi));
@@ -840,16 +1028,29 @@ int coarse_prepare(cr_handle *h) {
     }
     const int nrows = (int)rows.size();
     const int K2 = std::max(16, (2 * nmodes + 15) / 16 * 16);
-    const int np = (nc + GT - 1) / GT * GT;  // padded order (identity on the padding)
+    const int np = sparse ? nc : (nc + GT - 1) / GT * GT;  // dense: padded order (identity on the padding)
+    const int K = cs.pcg_iters;
+    const int nspmv = (nbc + kSpmvWarpsC - 1) / kSpmvWarpsC, nvec = (nbc + kVecThreads - 1) / kVecThreads;
     CR_TRY(grow(h, &cs.kv, cs.cap_kv, (size_t)std::max(nmodes, 1), moved));
     CR_TRY(grow(h, &cs.rows, cs.cap_rows, (size_t)std::max(nrows, 1), moved));
-    CR_TRY(grow(h, &cs.F, cs.cap_F, (size_t)nc * K2, moved));
-    CR_TRY(grow(h, &cs.FT, cs.cap_FT, (size_t)K2 * np, moved));
-    CR_TRY(grow(h, &cs.C, cs.cap_C, (size_t)np * np, moved));
-    CR_TRY(grow(h, &cs.Ci, cs.cap_Ci, (size_t)np * np, moved));
-    CR_TRY(grow(h, &cs.R, cs.cap_R, (size_t)NB * np, moved));
-    CR_TRY(grow(h, &cs.Fc, cs.cap_Fc, (size_t)np * NB, moved));
-    CR_TRY(grow(h, &cs.Dinv, cs.cap_Dinv, (size_t)NB * NB, moved));
+    if (!sparse) {
+        CR_TRY(grow(h, &cs.F, cs.cap_F, (size_t)nc * K2, moved));
+        CR_TRY(grow(h, &cs.FT, cs.cap_FT, (size_t)K2 * np, moved));
+        CR_TRY(grow(h, &cs.C, cs.cap_C, (size_t)np * np, moved));
+        CR_TRY(grow(h, &cs.Ci, cs.cap_Ci, (size_t)np * np, moved));
+        CR_TRY(grow(h, &cs.R, cs.cap_R, (size_t)NB * np, moved));
+        CR_TRY(grow(h, &cs.Fc, cs.cap_Fc, (size_t)np * NB, moved));
+        CR_TRY(grow(h, &cs.Dinv, cs.cap_Dinv, (size_t)NB * NB, moved));
+    } else {
+        CR_TRY(grow(h, &cs.Cblk, cs.cap_Cblk, (size_t)npairs * 9, moved));
+        CR_TRY(grow(h, &cs.Dblk, cs.cap_Dblk, (size_t)nbc * 9, moved));
+        CR_TRY(grow(h, &cs.pr, cs.cap_pr, (size_t)nc, moved));
+        CR_TRY(grow(h, &cs.pz, cs.cap_pz, (size_t)nc, moved));
+        CR_TRY(grow(h, &cs.pp, cs.cap_pp, (size_t)nc, moved));
+        CR_TRY(grow(h, &cs.pq, cs.cap_pq, (size_t)nc, moved));
+        CR_TRY(grow(h, &cs.part_pq, cs.cap_part_pq, (size_t)K * nspmv, moved));
+        CR_TRY(grow(h, &cs.part_rz, cs.cap_part_rz, (size_t)(K + 1) * nvec, moved));
+    }
     CR_TRY(grow(h, &cs.g, cs.cap_g, (size_t)np, moved));  // zero beyond nc: the padded GEMV rows
     CR_TRY(grow(h, &cs.y, cs.cap_y, (size_t)np, moved));
     CR_TRY(grow(h, &cs.u, cs.cap_u, (size_t)K2, moved));
@@ -869,8 +1070,10 @@ int coarse_prepare(cr_handle *h) {
     if (model_smem > 48 * 1024)
         CR_CUDA(h, cudaFuncSetAttribute(coarse_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)model_smem));
-    CR_CUDA(h, cudaMemsetAsync(cs.F, 0, (size_t)nc * K2 * sizeof(float), h->stream));
-    CR_CUDA(h, cudaMemsetAsync(cs.FT, 0, (size_t)K2 * np * sizeof(float), h->stream));
+    if (!sparse) {
+        CR_CUDA(h, cudaMemsetAsync(cs.F, 0, (size_t)nc * K2 * sizeof(float), h->stream));
+        CR_CUDA(h, cudaMemsetAsync(cs.FT, 0, (size_t)K2 * np * sizeof(float), h->stream));
+    }
     CR_CUDA(h, cudaMemsetAsync(cs.g, 0, (size_t)np * sizeof(double), h->stream));
     CR_CUDA(h, cudaMemsetAsync(cs.y, 0, (size_t)np * sizeof(double), h->stream));
     if (nmodes > 0) {
@@ -879,10 +1082,14 @@ int coarse_prepare(cr_handle *h) {
                                                              cs.F, cs.FT);
         CR_LAUNCH(h, "coarse_wave_basis_kernel");
     }
-    // C = F F^T + real-space blocks (+ self), padded with the identity
-    dim3 tg((nc + 63) / 64, (nc + 63) / 64);
-    syrk_kernel<<<tg, 256, 0, h->stream>>>(nc, K2, cs.F, K2, cs.C, np);
-    CR_LAUNCH(h, "syrk_kernel");
+    // dense: C = F F^T + real-space blocks (+ self), padded with the identity;
+    // sparse: the near-pair blocks only
+    if (!sparse) {
+        dim3 tg((nc + 63) / 64, (nc + 63) / 64);
+        syrk_kernel<<<tg, 256, 0, h->stream>>>(nc, K2, cs.F, K2, cs.C, np);
+        CR_LAUNCH(h, "syrk_kernel");
+    }
+    double *cblk = sparse ? cs.Cblk : nullptr;
     RealArgs ra;
     double max_rad = 0.0;
     for (int b : cbody) max_rad = std::max(max_rad, cent[b].w);
@@ -904,28 +1111,34 @@ int coarse_prepare(cr_handle *h) {
     if (shift)
         coarse_real_kernel<true><<<(unsigned)npairs, bs, 0, h->stream>>>(
             cs.pair_a, cs.pair_b, cs.woff, cs.cbody, h->d_body_start, h->d_body_members, h->m64.pos, cs.cent, cs.zq,
-            h->m32.phiq, ra, np, cs.W, cs.C);
+            h->m32.phiq, ra, np, cs.W, cs.C, cblk);
     else
         coarse_real_kernel<false><<<(unsigned)npairs, bs, 0, h->stream>>>(
             cs.pair_a, cs.pair_b, cs.woff, cs.cbody, h->d_body_start, h->d_body_members, h->m64.pos, cs.cent, cs.zq,
-            h->m32.phiq, ra, np, cs.W, cs.C);
+            h->m32.phiq, ra, np, cs.W, cs.C, cblk);
     CR_LAUNCH(h, "coarse_real_kernel");
-    symmetrise_kernel<<<blocks_for((long)nc * nc, 256), 256, 0, h->stream>>>(nc, cs.C, np);
-    CR_LAUNCH(h, "symmetrise_kernel");
-    pad_identity_kernel<<<blocks_for((long)np * np, 256), 256, 0, h->stream>>>(nc, np, cs.C);
-    CR_LAUNCH(h, "pad_identity_kernel");
-
-    // C^-1: FP32 copy inverted in place
-    to_float_kernel<<<blocks_for((long)np * np, 256), 256, 0, h->stream>>>((long long)np * np, cs.C, cs.Ci);
-    CR_LAUNCH(h, "to_float_kernel");
     CR_CUDA(h, cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-    for (int k0 = 0; k0 < np; k0 += NB) {
-        gj_pivot_kernel<<<1, 1024, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, h->d_flag);
-        CR_LAUNCH(h, "gj_pivot_kernel");
-        gj_panel_kernel<<<np / NB, 256, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, cs.R, cs.Fc);
-        CR_LAUNCH(h, "gj_panel_kernel");
-        gj_update_kernel<<<dim3(np / GT, np / GT), 256, 0, h->stream>>>(k0, np, cs.Ci, cs.R, cs.Fc);
-        CR_LAUNCH(h, "gj_update_kernel");
+    if (!sparse) {
+        symmetrise_kernel<<<blocks_for((long)nc * nc, 256), 256, 0, h->stream>>>(nc, cs.C, np);
+        CR_LAUNCH(h, "symmetrise_kernel");
+        pad_identity_kernel<<<blocks_for((long)np * np, 256), 256, 0, h->stream>>>(nc, np, cs.C);
+        CR_LAUNCH(h, "pad_identity_kernel");
+
+        // C^-1: FP32 copy inverted in place
+        to_float_kernel<<<blocks_for((long)np * np, 256), 256, 0, h->stream>>>((long long)np * np, cs.C, cs.Ci);
+        CR_LAUNCH(h, "to_float_kernel");
+        for (int k0 = 0; k0 < np; k0 += NB) {
+            gj_pivot_kernel<<<1, 1024, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, h->d_flag);
+            CR_LAUNCH(h, "gj_pivot_kernel");
+            gj_panel_kernel<<<np / NB, 256, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, cs.R, cs.Fc);
+            CR_LAUNCH(h, "gj_panel_kernel");
+            gj_update_kernel<<<dim3(np / GT, np / GT), 256, 0, h->stream>>>(k0, np, cs.Ci, cs.R, cs.Fc);
+            CR_LAUNCH(h, "gj_update_kernel");
+        }
+    } else {
+        block_jacobi_kernel<<<blocks_for(nbc, 128), 128, 0, h->stream>>>(nbc, cs.phead, cs.pcount, cs.pair_b, cs.Cblk,
+                                                                          cs.Dblk, h->d_flag);
+        CR_LAUNCH(h, "block_jacobi_kernel");
     }
     int bad = 0;
     CR_CUDA(h, cudaMemcpyAsync(&bad, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -939,6 +1152,9 @@ int coarse_prepare(cr_handle *h) {
     cs.np = np;
     cs.nmodes = nmodes;
     cs.nrows = nrows;
+    cs.sparse = sparse;
+    cs.nspmv = nspmv;
+    cs.nvec = nvec;
     cs.bs = bs;
     cs.model_smem = model_smem;
     cs.K2 = K2;
@@ -957,8 +1173,30 @@ int coarse_apply(cr_handle *h, const double *x, double *z) {
     coarse_restrict_kernel<<<cs.nbc, 128, 0, h->stream>>>(N, cs.cbody, h->d_body_start, h->d_body_members, cs.zq,
                                                            cs.zp, x, cs.g);
     CR_LAUNCH(h, "coarse_restrict_kernel");
-    coarse_gemv_kernel<<<blocks_for((long)cs.nc * 32, 256), 256, 0, h->stream>>>(cs.nc, cs.np, cs.Ci, cs.g, cs.y);
-    CR_LAUNCH(h, "coarse_gemv_kernel");
+    if (!cs.sparse) {
+        coarse_gemv_kernel<<<blocks_for((long)cs.nc * 32, 256), 256, 0, h->stream>>>(cs.nc, cs.np, cs.Ci, cs.g,
+                                                                                     cs.y);
+        CR_LAUNCH(h, "coarse_gemv_kernel");
+    } else {  // y ~= -C^-1 g by pcg_iters block-Jacobi CG steps
+        const int K = cs.pcg_iters, nv = cs.nvec, ns = cs.nspmv;
+        pcg_init_kernel<<<nv, kVecThreads, 0, h->stream>>>(cs.nbc, cs.Dblk, cs.g, cs.y, cs.pr, cs.pz, cs.pp,
+                                                            cs.part_rz);
+        CR_LAUNCH(h, "pcg_init_kernel");
+        for (int it = 0; it < K; ++it) {
+            pcg_spmv_kernel<<<ns, kSpmvWarpsC * 32, 0, h->stream>>>(cs.nbc, cs.phead, cs.pcount, cs.pair_b, cs.Cblk,
+                                                                     cs.pp, cs.pq, cs.part_pq + (size_t)it * ns);
+            CR_LAUNCH(h, "pcg_spmv_kernel");
+            pcg_update_kernel<<<nv, kVecThreads, 0, h->stream>>>(cs.nbc, ns, cs.part_pq + (size_t)it * ns, nv,
+                                                                  cs.part_rz + (size_t)it * nv, cs.Dblk, cs.pp, cs.pq,
+                                                                  cs.y, cs.pr, cs.pz, cs.part_rz + (size_t)(it + 1) * nv);
+            CR_LAUNCH(h, "pcg_update_kernel");
+            if (it + 1 < K) {
+                pcg_dir_kernel<<<blocks_for(3L * cs.nbc, kVecThreads), kVecThreads, 0, h->stream>>>(
+                    cs.nbc, nv, cs.part_rz + (size_t)it * nv, cs.part_rz + (size_t)(it + 1) * nv, cs.pz, cs.pp);
+                CR_LAUNCH(h, "pcg_dir_kernel");
+            }
+        }
+    }
     if (cs.nmodes > 0) {
         coarse_wave_coef_kernel<<<blocks_for((long)2 * cs.nmodes * 32, 256), 256, 0, h->stream>>>(
             2 * cs.nmodes, cs.np, cs.FT, cs.kv, cs.y, cs.u);

@@ -169,6 +169,16 @@ struct CoarseSpace {
     int4 *rows = nullptr;               // [nrows] runs of consecutive mz: (mx, my, mz0, first mode)
     int nrows = 0, bs = 128;            // runs; threads per body CTA of the A~ Z y kernel
     size_t model_smem = 0;              // dynamic shared memory of the A~ Z y kernel
+    // sparse level (coarse problems above max_dense unknowns): near-pair blocks, PCG
+    int max_dense = 12288, pcg_iters = 0;  // pcg_iters 0: no coarse level above max_dense
+    bool sparse = false;
+    int nspmv = 0, nvec = 0;            // blocks of the PCG kernels (partial sums per block)
+    double *Cblk = nullptr;             // [npairs][9] C_ab of each ordered near pair
+    double *Dblk = nullptr;             // [nbc][9] inverse diagonal blocks
+    double *pr = nullptr, *pz = nullptr, *pp = nullptr, *pq = nullptr;  // [nc] CG vectors
+    double *part_pq = nullptr, *part_rz = nullptr;  // per-iteration block partial sums
+    size_t cap_Cblk = 0, cap_Dblk = 0, cap_pr = 0, cap_pz = 0, cap_pp = 0, cap_pq = 0, cap_part_pq = 0,
+           cap_part_rz = 0;
     float *F = nullptr, *FT = nullptr;  // [nc][K2] scaled structure factors, [K2][np] transpose
     double *C = nullptr;                // [np][np] coarse operator (assembled in FP64)
     float *Ci = nullptr;                // [np][np] FP32 copy of C, inverted in place

@@ -124,11 +124,17 @@ class Handle:
 
     def coarse_info(self) -> dict:
         """Coarse level of the two-level preconditioner for the current positions."""
-        a, n, m = C.c_int(0), C.c_int(0), C.c_int(0)
+        a, n, m, sp = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
         p = C.c_longlong(0)
-        self._check(_lib.lib().cr_coarse_info(self.h, C.byref(a), C.byref(n), C.byref(p), C.byref(m)),
+        self._check(_lib.lib().cr_coarse_info(self.h, C.byref(a), C.byref(n), C.byref(p), C.byref(m), C.byref(sp)),
                     "cr_coarse_info")
-        return {"active": bool(a.value), "n_coarse": n.value, "near_pairs": p.value, "wave_vectors": m.value}
+        return {"active": bool(a.value), "n_coarse": n.value, "near_pairs": p.value, "wave_vectors": m.value,
+                "sparse": bool(sp.value)}
+
+    def set_coarse(self, max_dense: int = 12288, pcg_iterations: int = 0):
+        """Dense limit of the two-level preconditioner's coarse level; above it the level is
+        skipped (pcg_iterations 0) or solved in its sparse form by that many CG steps."""
+        self._check(_lib.lib().cr_set_coarse(self.h, int(max_dense), int(pcg_iterations)), "cr_set_coarse")
 
     def objective(self):
         y = self.empty(self.N + self.B)

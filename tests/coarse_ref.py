@@ -7,7 +7,9 @@ C = Z_q^T (self I + T + W_k) Z_q with T the tabulated real-space kernel under th
 operator's pair rule (dr <= d < rc, minimum image; ConductorRigid.cu:536-557) and W_k
 the wave-space kernel restricted to 0 < |k| < 2 xi (form factor j0(k)^2, Ewald factor
 exp(-k^2/4xi^2), 1/(k^2 V); ConductorRigid.cc:245-274), and the A-DEF1 application
-z = P (r - A~ Z y) + Z y with y = -C^-1 Z^T r.  Small systems only (dense N x N).
+z = P (r - A~ Z y) + Z y with y = -C^-1 Z^T r.  With pcg_steps > 0 the sparse form:
+no wave-space term, y from that many block-Jacobi CG steps on C y = -Z^T r.  Small
+systems only (dense N x N).
 """
 import numpy as np
 
@@ -23,7 +25,7 @@ def _mimg(d, L):
 
 
 class TwoLevelRef:
-    def __init__(self, s, derived: dict, phiq: np.ndarray, xi: float, min_beads: int = 4):
+    def __init__(self, s, derived: dict, phiq: np.ndarray, xi: float, min_beads: int = 4, pcg_steps: int = 0):
         self.s = s
         N, B = s.n_beads, s.n_bodies
         L = np.asarray(s.L, dtype=float)
@@ -76,6 +78,9 @@ class TwoLevelRef:
                     kk = np.linalg.norm(k)
                     if kk < kc:
                         ks.append(k)
+        self.pcg_steps = pcg_steps
+        if pcg_steps:  # sparse form: no wave-space term
+            ks = []
         self.n_modes = len(ks)
         Wk = np.zeros((N, N))
         for k in ks:
@@ -86,6 +91,38 @@ class TwoLevelRef:
         self.Mmodel = derived["selfcoeff"] * np.eye(N) + T + Wk
         self.C = Zq.T @ self.Mmodel @ Zq
         self.Cinv = np.linalg.inv(self.C)
+        nb = nc // 3
+        self.Dblk = [np.linalg.inv(0.5 * (self.C[3 * a:3 * a + 3, 3 * a:3 * a + 3] +
+                                          self.C[3 * a:3 * a + 3, 3 * a:3 * a + 3].T)) for a in range(nb)]
+
+    def _jacobi(self, r):
+        z = np.empty_like(r)
+        for a, D in enumerate(self.Dblk):
+            z[3 * a:3 * a + 3] = D @ r[3 * a:3 * a + 3]
+        return z
+
+    def coarse_solve(self, g):
+        """y = -C^-1 g: exact (dense form) or pcg_steps block-Jacobi CG steps (sparse form)."""
+        if not self.pcg_steps:
+            return -self.Cinv @ g
+        y = np.zeros_like(g)
+        r = -g
+        z = self._jacobi(r)
+        p = z.copy()
+        rz = r @ z
+        for it in range(self.pcg_steps):
+            q = self.C @ p
+            pq = p @ q
+            alpha = rz / pq if pq > 0 else 0.0
+            y += alpha * p
+            r = r - alpha * q
+            z = self._jacobi(r)
+            rzn = r @ z
+            if it + 1 < self.pcg_steps:
+                beta = rzn / rz if rz > 0 else 0.0
+                p = z + beta * p
+            rz = rzn
+        return y
 
     def conductor(self, v):
         N = self.N
@@ -99,7 +136,7 @@ class TwoLevelRef:
 
     def apply(self, r):
         N = self.N
-        y = -self.Cinv @ (self.Z.T @ r)
+        y = self.coarse_solve(self.Z.T @ r)
         zy = self.Z @ y
         t = r.copy()
         # A~ Z y = [Phi(Z y) - M~ (Z_q y); S Z_q y = 0]

@@ -42,7 +42,7 @@ def test_two_level_apply_matches_dense(cuda, product_lib, oracle_lib):
                                                   params["support"], params["rcut"]))
     ref = TwoLevelRef(s, dict(rcut=d.rcut, dr=d.dr, n_table=d.n_table, selfcoeff=d.selfcoeff), phiq, params["xi"])
     info = h.coarse_info()
-    assert info["active"] and info["n_coarse"] == 3 * s.n_bodies
+    assert info["active"] and not info["sparse"] and info["n_coarse"] == 3 * s.n_bodies
     assert info["wave_vectors"] == ref.n_modes
     rng = np.random.default_rng(11)
     for _ in range(2):
@@ -111,3 +111,49 @@ def test_two_level_follows_moving_bodies(cuda, product_lib):
         s.pos -= s.L * np.floor(s.pos / s.L + 0.5)
     assert h.coarse_info()["active"]
     h.close()
+
+
+def test_sparse_coarse_apply_matches_dense(cuda, product_lib, oracle_lib):
+    """The sparse form (near-pair blocks, block-Jacobi CG steps) against its restatement."""
+    from coarse_ref import TwoLevelRef
+
+    s, params = _system()
+    h = _handle(product_lib, s, params, precond="two_level")
+    h.set_coarse(max_dense=0, pcg_iterations=8)
+    d = h.derived()
+    phiq, _ = oracle_lib.tables(oracle_lib.derive(s.L, params["xi"], params["errortol"], params["grid"],
+                                                  params["support"], params["rcut"]))
+    ref = TwoLevelRef(s, dict(rcut=d.rcut, dr=d.dr, n_table=d.n_table, selfcoeff=d.selfcoeff), phiq, params["xi"],
+                      pcg_steps=8)
+    info = h.coarse_info()
+    assert info["active"] and info["sparse"] and info["wave_vectors"] == 0
+    rng = np.random.default_rng(12)
+    for _ in range(2):
+        v = rng.standard_normal(s.n_beads + s.n_bodies)
+        err = _rel(h.precondition(v), ref.apply(v))
+        print(f"\nsparse two-level apply: max rel err {err:.2e}")
+        assert err < 2e-4
+    h.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_sparse_coarse_solve_matches_oracle(cuda, product_lib, oracle_lib, precision):
+    s, params = _system()
+    orc = oracle_lib.Oracle(s, params["xi"], params["errortol"], params["grid"], params["support"], params["rcut"])
+    ref = orc.solve(s.field, restart=100, maxiter=4000, tol=1e-11)
+    its = {}
+    for pc, max_dense in (("conductor", 12288), ("two_level", 0)):
+        h = _handle(product_lib, s, params, gmres_tol=1e-8, restart=50, maxiter=4000, precision=precision,
+                    precond=pc)
+        h.set_coarse(max_dense=max_dense, pcg_iterations=8)
+        q = h.dev(np.zeros(s.n_beads))
+        phi = h.dev(np.zeros(s.n_bodies))
+        F, st = h.compute(s.pos, s.body_pos, q, phi)
+        h.close()
+        eq, ep, ef = _rel(q, ref["q"]), _rel(phi, ref["phi"]), _rel(F, ref["force"])
+        print(f"\n{pc} (sparse coarse) {precision}: iters={st['iterations']} resid={st['final_residual']:.2e} "
+              f"err q={eq:.2e} phi={ep:.2e} F={ef:.2e}")
+        assert st["converged"] == 1 and st["final_residual"] <= 1e-8
+        assert eq < 1e-5 and ep < 1e-5 and ef < 1e-5
+        its[pc] = st["iterations"]
+    assert 3 * its["two_level"] <= 2 * its["conductor"]
