@@ -416,14 +416,17 @@ __global__ void symmetrise_kernel(int n, double *__restrict__ C, int ldc) {
 // FP32 is enough for a preconditioner: the coarse operators met here have condition
 // numbers of 1e2-1e3, so C^-1 carries relative errors ~1e-4 at worst.
 
-// Dinv of the pivot block (one CTA of 1024 threads, scalar in-place Gauss-Jordan in
-// shared memory; thread t owns entries (t/64 + 16u, t%64), u = 0..3); a pivot that is
-// not positive and finite sets *flag and leaves Dinv untouched.
-__global__ void __launch_bounds__(1024) gj_pivot_kernel(int k0, int np, const float *__restrict__ A,
-                                                        float *__restrict__ Dinv, int *__restrict__ flag) {
+// Dinv of the pivot block (one CTA of kPivThreads threads, scalar in-place Gauss-Jordan in
+// shared memory; thread t owns entries (t/64 + kPivStride u, t%64)); a pivot that is not
+// positive and finite sets *flag and leaves Dinv untouched.
+constexpr int kPivThreads = 1024, kPivStride = kPivThreads / NB, kPivRows = NB / kPivStride;
+__global__ void __launch_bounds__(kPivThreads) gj_pivot_kernel(int k0, int np, const float *__restrict__ A,
+                                                               float *__restrict__ Dinv, int *__restrict__ flag) {
     __shared__ float D[NB][NB + 1];
-    const int c = threadIdx.x % NB, r0 = threadIdx.x / NB;  // rows r0, r0+16, r0+32, r0+48
-    for (int u = 0; u < 4; ++u) D[r0 + 16 * u][c] = A[(size_t)(k0 + r0 + 16 * u) * np + k0 + c];
+    const int c = threadIdx.x % NB, r0 = threadIdx.x / NB;
+#pragma unroll
+    for (int u = 0; u < kPivRows; ++u)
+        D[r0 + kPivStride * u][c] = A[(size_t)(k0 + r0 + kPivStride * u) * np + k0 + c];
     __syncthreads();
     for (int s = 0; s < NB; ++s) {
         const float piv = D[s][s];
@@ -432,21 +435,24 @@ __global__ void __launch_bounds__(1024) gj_pivot_kernel(int k0, int np, const fl
             return;
         }
         const float inv = 1.0f / piv;
-        float rs[4];
-        for (int u = 0; u < 4; ++u) rs[u] = D[r0 + 16 * u][s];
+        float rs[kPivRows];
+#pragma unroll
+        for (int u = 0; u < kPivRows; ++u) rs[u] = D[r0 + kPivStride * u][s];
         const float sc = D[s][c];
         __syncthreads();
         // row s: scaled, with the identity column in place of column s;
         // other rows: D[r][c] -= D[r][s] D[s][c] / piv, and column s becomes -D[r][s] / piv
         const float scs = c == s ? inv : sc * inv;
-        for (int u = 0; u < 4; ++u) {
-            const int r = r0 + 16 * u;
+#pragma unroll
+        for (int u = 0; u < kPivRows; ++u) {
+            const int r = r0 + kPivStride * u;
             if (r == s) D[r][c] = scs;
             else D[r][c] = c == s ? -rs[u] * inv : D[r][c] - rs[u] * scs;
         }
         __syncthreads();
     }
-    for (int u = 0; u < 4; ++u) Dinv[(r0 + 16 * u) * NB + c] = D[r0 + 16 * u][c];
+#pragma unroll
+    for (int u = 0; u < kPivRows; ++u) Dinv[(r0 + kPivStride * u) * NB + c] = D[r0 + kPivStride * u][c];
 }
 
 // R = Dinv A_K* (with A_KK := I, so R_KK = Dinv) and Fc = A_*K.  blockIdx.x: 64 columns.
@@ -771,10 +777,16 @@ __global__ void coarse_wave_coef_kernel(int rows, int ld, const float *__restric
     if ((threadIdx.x & 31) == 0) u[r] = (float)(s * kv[r >> 1].w);
 }
 
+// sin and cos of 2 pi t: t reduced to [-1/2, 1/2] first, then the fast intrinsic, whose
+// absolute error on [-pi, pi] is below 4e-7
+__device__ __forceinline__ void sincos_turns(float t, float *s, float *c) {
+    __sincosf(6.283185307179586f * (t - rintf(t)), s, c);
+}
+
 // t = x - A~ Z y on the bead rows of body b (one CTA per body), t[N+b] = x[N+b]:
 //   (A~ Z y)_i = Phi_b(Z y) - [ self (Z_q y)_i + sum_p W_p y_b(p) + wave_i ],
 //   wave_i = sum_m (cos(k_m.r_i) u_re[m] - sin(k_m.r_i) u_im[m]).
-// The wave vectors come in rows of consecutive m_z at fixed (m_x, m_y): one sincospi per
+// The wave vectors come in rows of consecutive m_z at fixed (m_x, m_y): one sine/cosine per
 // row, then rotation by exp(2 pi i z / L_z) along the row.  The body's near pairs (partner
 // coefficients and W offsets) are staged in shared memory first.
 __global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__restrict__ rows,
@@ -816,13 +828,13 @@ __global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__
         const double4 p = pos[i];
         const float fx = (float)(p.x * Linv.x), fy = (float)(p.y * Linv.y), fz = (float)(p.z * Linv.z);
         float sz, cz;
-        sincospif(2.0f * fz, &sz, &cz);
+        sincos_turns(fz, &sz, &cz);
         float wave = 0.f;
         for (int q = 0; q < nrows; ++q) {
             const int4 r = srow[q];
             const int end = q + 1 < nrows ? srow[q + 1].w : nmodes;
             float s, c;
-            sincospif(2.0f * ((float)r.x * fx + (float)r.y * fy + (float)r.z * fz), &s, &c);
+            sincos_turns((float)r.x * fx + (float)r.y * fy + (float)r.z * fz, &s, &c);
             for (int mm = r.w; mm < end; ++mm) {
                 const float2 uu = su[mm];
                 wave += c * uu.x - s * uu.y;
@@ -1128,7 +1140,7 @@ int coarse_prepare(cr_handle *h) {
         to_float_kernel<<<blocks_for((long)np * np, 256), 256, 0, h->stream>>>((long long)np * np, cs.C, cs.Ci);
         CR_LAUNCH(h, "to_float_kernel");
         for (int k0 = 0; k0 < np; k0 += NB) {
-            gj_pivot_kernel<<<1, 1024, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, h->d_flag);
+            gj_pivot_kernel<<<1, kPivThreads, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, h->d_flag);
             CR_LAUNCH(h, "gj_pivot_kernel");
             gj_panel_kernel<<<np / NB, 256, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, cs.R, cs.Fc);
             CR_LAUNCH(h, "gj_panel_kernel");
