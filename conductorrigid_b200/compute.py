@@ -10,7 +10,7 @@ must be all beads in index order (the reference's GMRES vector mixes group and g
 indices, ConductorRigid.cu:169 and :994, which agree only for that group).  Extra
 keyword options that the reference hard-codes or derives: ``grid``, ``support``,
 ``rcut``, ``gmres_tol``, ``restart``, ``maxiter``, ``precision`` ("fp64", "mixed"),
-``precond`` ("diagonal", "conductor").
+``precond`` ("diagonal", "conductor", "two_level").
 """
 from __future__ import annotations
 
