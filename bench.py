@@ -283,7 +283,8 @@ def run_dynamics(args) -> None:
     steps = args.warmup + args.steps
     train = min(200, max(1, steps // 2))
     out, guess = paired_run(_lib.make_params(**common), _lib.make_params(learned=True, **common), s,
-                            np.ones(s.n_bodies), steps, train_solves=train, seed=1)
+                            np.ones(s.n_bodies), steps, train_solves=train, seed=1,
+                            coarse=(args.coarse_max_dense, args.coarse_cg))
     tail = out[max(train + 1, args.warmup):]
 
     def arm(name):
@@ -297,7 +298,7 @@ def run_dynamics(args) -> None:
         "value": arm("learned")["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": len(tail),
         "warmup": len(out) - len(tail), "higher_is_better": True,
         "learned": arm("learned"), "plain_warm_start": arm("plain"), "trained_solves": guess.trained,
-        "preconditioner": args.precond,
+        "preconditioner": args.precond, "coarse_cg": args.coarse_cg,
         "heldout_explained": round(float(np.mean(guess.heldout[-len(tail):])) if guess.heldout else 0.0, 3),
         "dtype": "f32 operator, f64 Krylov; bf16 network", "data": "synthetic (seeded placement, relaxed)",
         "config": {"workload": f"dynamics_420k scale {args.scale}: {s.n_bodies} spheres x 42, phi 0.35, "

@@ -202,10 +202,11 @@ class BrownianRun:
 
 def paired_run(params_plain, params_learned, system, radius, steps, *, train_solves=None, seed=1, dt=1e-3,
                use_network=True, use_transport=True, passes=4, lr=1e-3, repulsion=1000.0, contact_gap=0.1,
-               relax_steps=300, mode="lsq"):
+               relax_steps=300, mode="lsq", coarse=None):
     """Two solvers on ONE trajectory: the plain solver (warm start from its own previous
     solution) moves the bodies; the learned solver solves the same configurations from its
-    own previous solution plus the guess directions.  Returns per-step stats of both."""
+    own previous solution plus the guess directions.  Returns per-step stats of both.
+    ``coarse`` = (max_dense, cg_steps) sets both handles' two-level coarse level."""
     import torch
 
     from .device import Handle
@@ -215,6 +216,9 @@ def paired_run(params_plain, params_learned, system, radius, steps, *, train_sol
     hp.set_topology(system.body, system.rigid, system.body_charge)
     hl = Handle(params_learned, system.L, stream=stream)
     hl.set_topology(system.body, system.rigid, system.body_charge)
+    if coarse is not None:
+        for h in (hp, hl):
+            h.set_coarse(*coarse)
     with torch.cuda.stream(stream):
         return _paired_loop(hp, hl, system, radius, steps, train_solves, seed, dt, use_network, use_transport,
                             passes, lr, repulsion, contact_gap, relax_steps, mode)
