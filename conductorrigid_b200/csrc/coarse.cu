@@ -30,9 +30,9 @@
 // once per geometry (assembled in FP64, inverted in place by blocked Gauss-Jordan in FP32).
 // Above a dense limit (max_dense coarse unknowns, 12,288 by default) the level is skipped
 // unless the caller asks for the sparse form (cr_set_coarse with CG steps > 0): the coarse
-// operator then keeps only its self and real-space terms, stored as 3 x 3 blocks of the
-// near pairs, and C y = -Z^T r is solved by that many block-Jacobi preconditioned CG
-// steps; no wave-space term is used in C or in A~ Z y there.
+// operator is then kept as 3 x 3 blocks of the near pairs plus the low-rank F F^T (at most
+// 256 wave vectors), and C y = -Z^T r is solved by that many block-Jacobi preconditioned
+// CG steps.
 // In flexible GMRES any preconditioner leaves the solution unchanged: only the iteration
 // count moves (at 162 beads per sphere, phi = 0.30: 133 -> 40 iterations against the
 // conductor response alone, on 100 bodies).
@@ -49,6 +49,7 @@ namespace {
 constexpr int kMinBeads = 4;        // bodies with fewer beads get no coarse vectors
 constexpr int kMaxSparse = 786432;  // coarse unknowns above which the level is skipped
 constexpr int kMaxModes = 1024;     // half-space wave vectors kept (kc shrinks above)
+constexpr int kMaxModesSparse = 256;  // the same for the sparse form (its CG steps read F twice)
 constexpr int NB = 64;              // Gauss-Jordan block
 constexpr int kChunk = 512;         // beads staged in shared memory per pass
 
@@ -554,12 +555,31 @@ __global__ void to_float_kernel(long long n, const double *__restrict__ a, float
     if (t < n) b[t] = (float)a[t];
 }
 
-// ---- sparse coarse level: block-Jacobi preconditioned CG on the near-pair blocks ----
-// For coarse problems above the dense limit the coarse operator keeps only the self and
-// real-space terms (C_ab = Z_a^T M_real Z_b for near pairs, 3 x 3 blocks) and C y = -g is
-// solved approximately by a fixed number of conjugate-gradient steps with the inverse
-// diagonal blocks as preconditioner; the flexible outer iteration accepts the resulting
-// (slightly varying) preconditioner.  Sums over blocks are reduced in a fixed order.
+// sum_c row[c] v[c] over a zero-padded row of n4 float4 (one warp; row 16-byte aligned).
+__device__ __forceinline__ double warp_row_dot(const float *__restrict__ row, const double *__restrict__ v, int n4) {
+    const int lane = threadIdx.x & 31;
+    const float4 *r4 = reinterpret_cast<const float4 *>(row);
+    const double2 *v2 = reinterpret_cast<const double2 *>(v);
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll 4
+    for (int c = lane; c < n4; c += 32) {
+        const float4 a = __ldg(r4 + c);
+        const double2 p = v2[2 * c], q = v2[2 * c + 1];
+        s0 += (double)a.x * p.x + (double)a.y * p.y;
+        s1 += (double)a.z * q.x + (double)a.w * q.y;
+    }
+    double s = s0 + s1;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+// ---- sparse coarse level: block-Jacobi preconditioned CG ----
+// For coarse problems above the dense limit the coarse operator is kept as 3 x 3 blocks of
+// the near pairs (self and real-space terms) plus the low-rank wave-space term F F^T, and
+// C y = -g is solved approximately by a fixed number of conjugate-gradient steps with the
+// inverse diagonal blocks as preconditioner; the flexible outer iteration accepts the
+// resulting (slightly varying) preconditioner.  Sums over blocks are reduced in a fixed
+// order.
 constexpr int kVecThreads = 256, kSpmvWarpsC = 8;
 
 // sum of a[0..n) on every thread of the block (fixed order: strided partial sums, tree)
@@ -585,7 +605,8 @@ __device__ __forceinline__ void mat3_vec(const double *__restrict__ M, const dou
 // definite sets *flag
 __global__ void block_jacobi_kernel(int nbc, const int *__restrict__ phead, const int *__restrict__ pcount,
                                     const int *__restrict__ pair_b, const double *__restrict__ Cblk,
-                                    double *__restrict__ Dblk, int *__restrict__ flag) {
+                                    const float *__restrict__ F, int K2, double *__restrict__ Dblk,
+                                    int *__restrict__ flag) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= nbc) return;
     int q = -1;
@@ -595,6 +616,13 @@ __global__ void block_jacobi_kernel(int nbc, const int *__restrict__ phead, cons
     if (q >= 0)
         for (int e = 0; e < 3; ++e)
             for (int c = 0; c < 3; ++c) m[3 * e + c] = 0.5 * (Cblk[9 * (size_t)q + 3 * e + c] + Cblk[9 * (size_t)q + 3 * c + e]);
+    for (int e = 0; e < 3; ++e)  // + the wave-space part F_a F_a^T
+        for (int c = 0; c < 3; ++c) {
+            const float *fe = F + (size_t)(3 * a + e) * K2, *fc = F + (size_t)(3 * a + c) * K2;
+            double t = 0.0;
+            for (int k = 0; k < K2; ++k) t += (double)fe[k] * fc[k];
+            m[3 * e + c] += t;
+        }
     const double c00 = m[4] * m[8] - m[5] * m[7], c01 = m[5] * m[6] - m[3] * m[8], c02 = m[3] * m[7] - m[4] * m[6];
     const double det = m[0] * c00 + m[1] * c01 + m[2] * c02;
     double *d = Dblk + 9 * (size_t)a;
@@ -613,6 +641,15 @@ __global__ void block_jacobi_kernel(int nbc, const int *__restrict__ phead, cons
     d[6] = c02 * id;
     d[7] = (m[1] * m[6] - m[0] * m[7]) * id;
     d[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+// u = F^T p (one warp per row of F^T; rows of ld floats, p zero beyond nc)
+__global__ void pcg_lowrank_kernel(int rows, int ld, const float *__restrict__ FT, const double *__restrict__ p,
+                                   double *__restrict__ u) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= rows) return;
+    const double s = warp_row_dot(FT + (size_t)r * ld, p, ld / 4);
+    if ((threadIdx.x & 31) == 0) u[r] = s;
 }
 
 // y = 0, r = -g, z = D r, p = z; partial r.z per block
@@ -645,6 +682,8 @@ __global__ void __launch_bounds__(kSpmvWarpsC * 32) pcg_spmv_kernel(int nbc, con
                                                                     const int *__restrict__ pcount,
                                                                     const int *__restrict__ pair_b,
                                                                     const double *__restrict__ Cblk,
+                                                                    const float *__restrict__ F, int K2,
+                                                                    const double *__restrict__ u,
                                                                     const double *__restrict__ p,
                                                                     double *__restrict__ q,
                                                                     double *__restrict__ part_pq) {
@@ -660,6 +699,10 @@ __global__ void __launch_bounds__(kSpmvWarpsC * 32) pcg_spmv_kernel(int nbc, con
             double t[3];
             mat3_vec(Cblk + 9 * (size_t)(h0 + k), pb, t);
             for (int e = 0; e < 3; ++e) acc[e] += t[e];
+        }
+        for (int k = lane; k < K2; k += 32) {  // + (F F^T p)_a = F_a u
+            const double uk = u[k];
+            for (int e = 0; e < 3; ++e) acc[e] += (double)F[(size_t)(3 * a + e) * K2 + k] * uk;
         }
         for (int e = 0; e < 3; ++e)
             for (int o = 16; o > 0; o >>= 1) acc[e] += __shfl_xor_sync(0xffffffffu, acc[e], o);
@@ -738,24 +781,6 @@ __global__ void coarse_restrict_kernel(int N, const int *__restrict__ cbody, con
     block_sum<3>(s, red);
     if (threadIdx.x == 0)
         for (int e = 0; e < 3; ++e) g[3 * a + e] = s[e] + zp[3 * ba + e] * x[N + ba];
-}
-
-// sum_c row[c] v[c] over a zero-padded row of n4 float4 (one warp; row 16-byte aligned).
-__device__ __forceinline__ double warp_row_dot(const float *__restrict__ row, const double *__restrict__ v, int n4) {
-    const int lane = threadIdx.x & 31;
-    const float4 *r4 = reinterpret_cast<const float4 *>(row);
-    const double2 *v2 = reinterpret_cast<const double2 *>(v);
-    double s0 = 0.0, s1 = 0.0;
-#pragma unroll 4
-    for (int c = lane; c < n4; c += 32) {
-        const float4 a = __ldg(r4 + c);
-        const double2 p = v2[2 * c], q = v2[2 * c + 1];
-        s0 += (double)a.x * p.x + (double)a.y * p.y;
-        s1 += (double)a.z * q.x + (double)a.w * q.y;
-    }
-    double s = s0 + s1;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
 }
 
 // y = -Cinv g (one warp per row; rows of ld floats, g zero beyond n)
@@ -904,6 +929,7 @@ void coarse_free(cr_handle *h) {
     dfree(&c.pq);
     dfree(&c.part_pq);
     dfree(&c.part_rz);
+    dfree(&c.pu);
     dfree(&c.F);
     dfree(&c.FT);
     dfree(&c.C);
@@ -1011,9 +1037,10 @@ int coarse_prepare(cr_handle *h) {
 
     // wave vectors of the half space with 0 < |k| < kc (kc lowered if there are too many)
     const double xi = h->user.xi, V = h->L[0] * h->L[1] * h->L[2];
-    double kc = sparse ? 0.0 : 2.0 * xi;  // the sparse level keeps no wave-space term
+    double kc = 2.0 * xi;
+    const int max_modes = sparse ? kMaxModesSparse : kMaxModes;
     std::vector<float4> kv;
-    for (int attempt = 0; attempt < 40 && kc > 0.0; ++attempt) {
+    for (int attempt = 0; attempt < 80; ++attempt) {
         kv.clear();
         int mmax[3];
         for (int d = 0; d < 3; ++d) mmax[d] = (int)std::floor(kc * h->L[d] / (2.0 * kPi));
@@ -1028,7 +1055,7 @@ int coarse_prepare(cr_handle *h) {
                     const double w = 2.0 * j0 * j0 * std::exp(-k2 / (4.0 * xi * xi)) / (k2 * V);
                     kv.push_back(make_float4((float)mx, (float)my, (float)mz, (float)std::sqrt(w)));
                 }
-        if ((int)kv.size() <= kMaxModes) break;
+        if ((int)kv.size() <= max_modes) break;
         kc *= 0.95;
     }
     const int nmodes = (int)kv.size();
@@ -1040,14 +1067,15 @@ int coarse_prepare(cr_handle *h) {
     }
     const int nrows = (int)rows.size();
     const int K2 = std::max(16, (2 * nmodes + 15) / 16 * 16);
-    const int np = sparse ? nc : (nc + GT - 1) / GT * GT;  // dense: padded order (identity on the padding)
+    // dense: padded order (identity on the padding); sparse: rows of whole float4
+    const int np = sparse ? (nc + 3) / 4 * 4 : (nc + GT - 1) / GT * GT;
     const int K = cs.pcg_iters;
     const int nspmv = (nbc + kSpmvWarpsC - 1) / kSpmvWarpsC, nvec = (nbc + kVecThreads - 1) / kVecThreads;
     CR_TRY(grow(h, &cs.kv, cs.cap_kv, (size_t)std::max(nmodes, 1), moved));
     CR_TRY(grow(h, &cs.rows, cs.cap_rows, (size_t)std::max(nrows, 1), moved));
+    CR_TRY(grow(h, &cs.F, cs.cap_F, (size_t)nc * K2, moved));
+    CR_TRY(grow(h, &cs.FT, cs.cap_FT, (size_t)K2 * np, moved));
     if (!sparse) {
-        CR_TRY(grow(h, &cs.F, cs.cap_F, (size_t)nc * K2, moved));
-        CR_TRY(grow(h, &cs.FT, cs.cap_FT, (size_t)K2 * np, moved));
         CR_TRY(grow(h, &cs.C, cs.cap_C, (size_t)np * np, moved));
         CR_TRY(grow(h, &cs.Ci, cs.cap_Ci, (size_t)np * np, moved));
         CR_TRY(grow(h, &cs.R, cs.cap_R, (size_t)NB * np, moved));
@@ -1056,10 +1084,11 @@ int coarse_prepare(cr_handle *h) {
     } else {
         CR_TRY(grow(h, &cs.Cblk, cs.cap_Cblk, (size_t)npairs * 9, moved));
         CR_TRY(grow(h, &cs.Dblk, cs.cap_Dblk, (size_t)nbc * 9, moved));
-        CR_TRY(grow(h, &cs.pr, cs.cap_pr, (size_t)nc, moved));
-        CR_TRY(grow(h, &cs.pz, cs.cap_pz, (size_t)nc, moved));
-        CR_TRY(grow(h, &cs.pp, cs.cap_pp, (size_t)nc, moved));
-        CR_TRY(grow(h, &cs.pq, cs.cap_pq, (size_t)nc, moved));
+        CR_TRY(grow(h, &cs.pr, cs.cap_pr, (size_t)np, moved));
+        CR_TRY(grow(h, &cs.pz, cs.cap_pz, (size_t)np, moved));
+        CR_TRY(grow(h, &cs.pp, cs.cap_pp, (size_t)np, moved));  // zero beyond nc: read by whole float4 rows
+        CR_TRY(grow(h, &cs.pq, cs.cap_pq, (size_t)np, moved));
+        CR_TRY(grow(h, &cs.pu, cs.cap_pu, (size_t)K2, moved));
         CR_TRY(grow(h, &cs.part_pq, cs.cap_part_pq, (size_t)K * nspmv, moved));
         CR_TRY(grow(h, &cs.part_rz, cs.cap_part_rz, (size_t)(K + 1) * nvec, moved));
     }
@@ -1082,10 +1111,9 @@ int coarse_prepare(cr_handle *h) {
     if (model_smem > 48 * 1024)
         CR_CUDA(h, cudaFuncSetAttribute(coarse_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)model_smem));
-    if (!sparse) {
-        CR_CUDA(h, cudaMemsetAsync(cs.F, 0, (size_t)nc * K2 * sizeof(float), h->stream));
-        CR_CUDA(h, cudaMemsetAsync(cs.FT, 0, (size_t)K2 * np * sizeof(float), h->stream));
-    }
+    CR_CUDA(h, cudaMemsetAsync(cs.F, 0, (size_t)nc * K2 * sizeof(float), h->stream));
+    CR_CUDA(h, cudaMemsetAsync(cs.FT, 0, (size_t)K2 * np * sizeof(float), h->stream));
+    if (sparse) CR_CUDA(h, cudaMemsetAsync(cs.pp, 0, (size_t)np * sizeof(double), h->stream));
     CR_CUDA(h, cudaMemsetAsync(cs.g, 0, (size_t)np * sizeof(double), h->stream));
     CR_CUDA(h, cudaMemsetAsync(cs.y, 0, (size_t)np * sizeof(double), h->stream));
     if (nmodes > 0) {
@@ -1149,7 +1177,7 @@ int coarse_prepare(cr_handle *h) {
         }
     } else {
         block_jacobi_kernel<<<blocks_for(nbc, 128), 128, 0, h->stream>>>(nbc, cs.phead, cs.pcount, cs.pair_b, cs.Cblk,
-                                                                          cs.Dblk, h->d_flag);
+                                                                          cs.F, K2, cs.Dblk, h->d_flag);
         CR_LAUNCH(h, "block_jacobi_kernel");
     }
     int bad = 0;
@@ -1195,8 +1223,14 @@ int coarse_apply(cr_handle *h, const double *x, double *z) {
                                                             cs.part_rz);
         CR_LAUNCH(h, "pcg_init_kernel");
         for (int it = 0; it < K; ++it) {
+            if (cs.nmodes > 0) {
+                pcg_lowrank_kernel<<<blocks_for(32L * cs.K2, 256), 256, 0, h->stream>>>(cs.K2, cs.np, cs.FT, cs.pp,
+                                                                                         cs.pu);
+                CR_LAUNCH(h, "pcg_lowrank_kernel");
+            }
             pcg_spmv_kernel<<<ns, kSpmvWarpsC * 32, 0, h->stream>>>(cs.nbc, cs.phead, cs.pcount, cs.pair_b, cs.Cblk,
-                                                                     cs.pp, cs.pq, cs.part_pq + (size_t)it * ns);
+                                                                     cs.F, cs.nmodes > 0 ? cs.K2 : 0, cs.pu, cs.pp,
+                                                                     cs.pq, cs.part_pq + (size_t)it * ns);
             CR_LAUNCH(h, "pcg_spmv_kernel");
             pcg_update_kernel<<<nv, kVecThreads, 0, h->stream>>>(cs.nbc, ns, cs.part_pq + (size_t)it * ns, nv,
                                                                   cs.part_rz + (size_t)it * nv, cs.Dblk, cs.pp, cs.pq,

@@ -177,8 +177,9 @@ struct CoarseSpace {
     double *Dblk = nullptr;             // [nbc][9] inverse diagonal blocks
     double *pr = nullptr, *pz = nullptr, *pp = nullptr, *pq = nullptr;  // [nc] CG vectors
     double *part_pq = nullptr, *part_rz = nullptr;  // per-iteration block partial sums
+    double *pu = nullptr;               // [K2] F^T p of the current CG step
     size_t cap_Cblk = 0, cap_Dblk = 0, cap_pr = 0, cap_pz = 0, cap_pp = 0, cap_pq = 0, cap_part_pq = 0,
-           cap_part_rz = 0;
+           cap_part_rz = 0, cap_pu = 0;
     float *F = nullptr, *FT = nullptr;  // [nc][K2] scaled structure factors, [K2][np] transpose
     double *C = nullptr;                // [np][np] coarse operator (assembled in FP64)
     float *Ci = nullptr;                // [np][np] FP32 copy of C, inverted in place

@@ -8,8 +8,8 @@ operator's pair rule (dr <= d < rc, minimum image; ConductorRigid.cu:536-557) an
 the wave-space kernel restricted to 0 < |k| < 2 xi (form factor j0(k)^2, Ewald factor
 exp(-k^2/4xi^2), 1/(k^2 V); ConductorRigid.cc:245-274), and the A-DEF1 application
 z = P (r - A~ Z y) + Z y with y = -C^-1 Z^T r.  With pcg_steps > 0 the sparse form:
-no wave-space term, y from that many block-Jacobi CG steps on C y = -Z^T r.  Small
-systems only (dense N x N).
+y from that many block-Jacobi CG steps on C y = -Z^T r (the diagonal blocks include
+the wave-space term).  Small systems only (dense N x N).
 """
 import numpy as np
 
@@ -79,8 +79,6 @@ class TwoLevelRef:
                     if kk < kc:
                         ks.append(k)
         self.pcg_steps = pcg_steps
-        if pcg_steps:  # sparse form: no wave-space term
-            ks = []
         self.n_modes = len(ks)
         Wk = np.zeros((N, N))
         for k in ks:

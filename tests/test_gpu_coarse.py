@@ -114,7 +114,8 @@ def test_two_level_follows_moving_bodies(cuda, product_lib):
 
 
 def test_sparse_coarse_apply_matches_dense(cuda, product_lib, oracle_lib):
-    """The sparse form (near-pair blocks, block-Jacobi CG steps) against its restatement."""
+    """The sparse form (near-pair blocks + low-rank wave term, block-Jacobi CG steps)
+    against its restatement."""
     from coarse_ref import TwoLevelRef
 
     s, params = _system()
@@ -126,7 +127,7 @@ def test_sparse_coarse_apply_matches_dense(cuda, product_lib, oracle_lib):
     ref = TwoLevelRef(s, dict(rcut=d.rcut, dr=d.dr, n_table=d.n_table, selfcoeff=d.selfcoeff), phiq, params["xi"],
                       pcg_steps=8)
     info = h.coarse_info()
-    assert info["active"] and info["sparse"] and info["wave_vectors"] == 0
+    assert info["active"] and info["sparse"] and info["wave_vectors"] == ref.n_modes
     rng = np.random.default_rng(12)
     for _ in range(2):
         v = rng.standard_normal(s.n_beads + s.n_bodies)
