@@ -300,11 +300,11 @@ __global__ void __launch_bounds__(256) coarse_real_kernel(
 }
 
 // Structure factors of the coarse columns: F[3a+e][2m] = sqrt(w_m) Re S_ae(k_m),
-// F[3a+e][2m+1] = sqrt(w_m) Im S_ae(k_m); FT is the transpose.  One CTA per coarse body.
+// F[3a+e][2m+1] = sqrt(w_m) Im S_ae(k_m).  One CTA per coarse body.
 __global__ void coarse_wave_basis_kernel(int nmodes, const float4 *__restrict__ kv, const int *__restrict__ cbody,
                                          const int *__restrict__ body_start, const int *__restrict__ members,
                                          const double4 *__restrict__ pos, double3 Linv, const double *__restrict__ zq,
-                                         int ldf, int ldt, float *__restrict__ F, float *__restrict__ FT) {
+                                         int ldf, float *__restrict__ F) {
     __shared__ float4 sf[kChunk];
     __shared__ float2 sz[kChunk];
     const int a = blockIdx.x, ba = cbody[a];
@@ -344,8 +344,6 @@ __global__ void coarse_wave_basis_kernel(int nmodes, const float4 *__restrict__ 
                 const int row = 3 * a + e;
                 F[(size_t)row * ldf + 2 * m] = k.w * re[e];
                 F[(size_t)row * ldf + 2 * m + 1] = k.w * im[e];
-                FT[(size_t)(2 * m) * ldt + row] = k.w * re[e];
-                FT[(size_t)(2 * m + 1) * ldt + row] = k.w * im[e];
             }
     }
 }
@@ -643,13 +641,30 @@ __global__ void block_jacobi_kernel(int nbc, const int *__restrict__ phead, cons
     d[8] = (m[0] * m[4] - m[1] * m[3]) * id;
 }
 
-// u = F^T p (one warp per row of F^T; rows of ld floats, p zero beyond nc)
-__global__ void pcg_lowrank_kernel(int rows, int ld, const float *__restrict__ FT, const double *__restrict__ p,
-                                   double *__restrict__ u) {
-    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (r >= rows) return;
-    const double s = warp_row_dot(FT + (size_t)r * ld, p, ld / 4);
-    if ((threadIdx.x & 31) == 0) u[r] = s;
+// u = F^T v in two steps: partial column sums over chunks of kColRows rows of F (threads
+// over the columns, every load coalesced), then a reduction over the chunks in a fixed
+// order.  With kv, u[k] is also scaled by sqrt(w) of its wave vector (k / 2).
+constexpr int kColRows = 32;
+__global__ void __launch_bounds__(256) fcol_partial_kernel(int nc, int K2, const float *__restrict__ F,
+                                                           const double *__restrict__ v, double *__restrict__ part) {
+    const int c0 = blockIdx.x * kColRows, c1 = min(nc, c0 + kColRows);
+    for (int k = threadIdx.x; k < K2; k += blockDim.x) {
+        double acc = 0.0;
+#pragma unroll 8
+        for (int c = c0; c < c1; ++c) acc += (double)__ldg(F + (size_t)c * K2 + k) * v[c];
+        part[(size_t)blockIdx.x * K2 + k] = acc;
+    }
+}
+
+template <typename T>
+__global__ void fcol_reduce_kernel(int nchunk, int K2, const double *__restrict__ part, int nmodes,
+                                   const float4 *__restrict__ kv, T *__restrict__ u) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K2) return;
+    double s = 0.0;
+    for (int q = 0; q < nchunk; ++q) s += part[(size_t)q * K2 + k];
+    if (kv) s = k < 2 * nmodes ? s * kv[k >> 1].w : 0.0;
+    u[k] = (T)s;
 }
 
 // y = 0, r = -g, z = D r, p = z; partial r.z per block
@@ -792,16 +807,6 @@ __global__ void coarse_gemv_kernel(int n, int ld, const float *__restrict__ Ci, 
     if ((threadIdx.x & 31) == 0) y[r] = -s;
 }
 
-// u[r] = sqrt(w_m) sum_c FT[r][c] y[c], m = r / 2 (one warp per row of FT): the
-// coefficients w_m (Re, Im) S_{Zy}(k_m) of the potential of the coarse charges Z_q y.
-__global__ void coarse_wave_coef_kernel(int rows, int ld, const float *__restrict__ FT, const float4 *__restrict__ kv,
-                                        const double *__restrict__ y, float *__restrict__ u) {
-    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (r >= rows) return;
-    const double s = warp_row_dot(FT + (size_t)r * ld, y, ld / 4);
-    if ((threadIdx.x & 31) == 0) u[r] = (float)(s * kv[r >> 1].w);
-}
-
 // sin and cos of 2 pi t: t reduced to [-1/2, 1/2] first, then the fast intrinsic, whose
 // absolute error on [-pi, pi] is below 4e-7
 __device__ __forceinline__ void sincos_turns(float t, float *s, float *c) {
@@ -931,7 +936,7 @@ void coarse_free(cr_handle *h) {
     dfree(&c.part_rz);
     dfree(&c.pu);
     dfree(&c.F);
-    dfree(&c.FT);
+    dfree(&c.fpart);
     dfree(&c.C);
     dfree(&c.Ci);
     dfree(&c.R);
@@ -1074,7 +1079,8 @@ int coarse_prepare(cr_handle *h) {
     CR_TRY(grow(h, &cs.kv, cs.cap_kv, (size_t)std::max(nmodes, 1), moved));
     CR_TRY(grow(h, &cs.rows, cs.cap_rows, (size_t)std::max(nrows, 1), moved));
     CR_TRY(grow(h, &cs.F, cs.cap_F, (size_t)nc * K2, moved));
-    CR_TRY(grow(h, &cs.FT, cs.cap_FT, (size_t)K2 * np, moved));
+    const int nchunk = (nc + kColRows - 1) / kColRows;
+    CR_TRY(grow(h, &cs.fpart, cs.cap_fpart, (size_t)nchunk * K2, moved));
     if (!sparse) {
         CR_TRY(grow(h, &cs.C, cs.cap_C, (size_t)np * np, moved));
         CR_TRY(grow(h, &cs.Ci, cs.cap_Ci, (size_t)np * np, moved));
@@ -1112,14 +1118,13 @@ int coarse_prepare(cr_handle *h) {
         CR_CUDA(h, cudaFuncSetAttribute(coarse_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)model_smem));
     CR_CUDA(h, cudaMemsetAsync(cs.F, 0, (size_t)nc * K2 * sizeof(float), h->stream));
-    CR_CUDA(h, cudaMemsetAsync(cs.FT, 0, (size_t)K2 * np * sizeof(float), h->stream));
     if (sparse) CR_CUDA(h, cudaMemsetAsync(cs.pp, 0, (size_t)np * sizeof(double), h->stream));
     CR_CUDA(h, cudaMemsetAsync(cs.g, 0, (size_t)np * sizeof(double), h->stream));
     CR_CUDA(h, cudaMemsetAsync(cs.y, 0, (size_t)np * sizeof(double), h->stream));
     if (nmodes > 0) {
         coarse_wave_basis_kernel<<<nbc, 128, 0, h->stream>>>(nmodes, cs.kv, cs.cbody, h->d_body_start,
-                                                             h->d_body_members, h->m64.pos, Linv, cs.zq, K2, np,
-                                                             cs.F, cs.FT);
+                                                             h->d_body_members, h->m64.pos, Linv, cs.zq, K2,
+                                                             cs.F);
         CR_LAUNCH(h, "coarse_wave_basis_kernel");
     }
     // dense: C = F F^T + real-space blocks (+ self), padded with the identity;
@@ -1224,9 +1229,12 @@ int coarse_apply(cr_handle *h, const double *x, double *z) {
         CR_LAUNCH(h, "pcg_init_kernel");
         for (int it = 0; it < K; ++it) {
             if (cs.nmodes > 0) {
-                pcg_lowrank_kernel<<<blocks_for(32L * cs.K2, 256), 256, 0, h->stream>>>(cs.K2, cs.np, cs.FT, cs.pp,
-                                                                                         cs.pu);
-                CR_LAUNCH(h, "pcg_lowrank_kernel");
+                const int nchunk = (cs.nc + kColRows - 1) / kColRows;
+                fcol_partial_kernel<<<nchunk, 256, 0, h->stream>>>(cs.nc, cs.K2, cs.F, cs.pp, cs.fpart);
+                CR_LAUNCH(h, "fcol_partial_kernel");
+                fcol_reduce_kernel<double><<<blocks_for(cs.K2, 256), 256, 0, h->stream>>>(
+                    nchunk, cs.K2, cs.fpart, 0, nullptr, cs.pu);
+                CR_LAUNCH(h, "fcol_reduce_kernel");
             }
             pcg_spmv_kernel<<<ns, kSpmvWarpsC * 32, 0, h->stream>>>(cs.nbc, cs.phead, cs.pcount, cs.pair_b, cs.Cblk,
                                                                      cs.F, cs.nmodes > 0 ? cs.K2 : 0, cs.pu, cs.pp,
@@ -1244,9 +1252,12 @@ int coarse_apply(cr_handle *h, const double *x, double *z) {
         }
     }
     if (cs.nmodes > 0) {
-        coarse_wave_coef_kernel<<<blocks_for((long)2 * cs.nmodes * 32, 256), 256, 0, h->stream>>>(
-            2 * cs.nmodes, cs.np, cs.FT, cs.kv, cs.y, cs.u);
-        CR_LAUNCH(h, "coarse_wave_coef_kernel");
+        const int nchunk = (cs.nc + kColRows - 1) / kColRows;
+        fcol_partial_kernel<<<nchunk, 256, 0, h->stream>>>(cs.nc, cs.K2, cs.F, cs.y, cs.fpart);
+        CR_LAUNCH(h, "fcol_partial_kernel");
+        fcol_reduce_kernel<float><<<blocks_for(cs.K2, 256), 256, 0, h->stream>>>(nchunk, cs.K2, cs.fpart, cs.nmodes,
+                                                                               cs.kv, cs.u);
+        CR_LAUNCH(h, "fcol_reduce_kernel");
     }
     coarse_model_kernel<<<B, cs.bs, cs.model_smem, h->stream>>>(N, cs.nmodes, cs.nrows, cs.rows, cs.cidx,
                                                                  h->d_body_start, h->d_body_members, h->m64.pos,

@@ -180,7 +180,8 @@ struct CoarseSpace {
     double *pu = nullptr;               // [K2] F^T p of the current CG step
     size_t cap_Cblk = 0, cap_Dblk = 0, cap_pr = 0, cap_pz = 0, cap_pp = 0, cap_pq = 0, cap_part_pq = 0,
            cap_part_rz = 0, cap_pu = 0;
-    float *F = nullptr, *FT = nullptr;  // [nc][K2] scaled structure factors, [K2][np] transpose
+    float *F = nullptr;                 // [nc][K2] scaled structure factors
+    double *fpart = nullptr;            // [chunks][K2] partial column sums of F
     double *C = nullptr;                // [np][np] coarse operator (assembled in FP64)
     float *Ci = nullptr;                // [np][np] FP32 copy of C, inverted in place
     float *R = nullptr, *Fc = nullptr, *Dinv = nullptr;   // Gauss-Jordan panels (FP32)
@@ -189,7 +190,7 @@ struct CoarseSpace {
     double *t = nullptr;                // [N+B] r - A~ Z y
     size_t cap_cidx = 0, cap_cbody = 0, cap_zq = 0, cap_zp = 0, cap_cent = 0, cap_basis = 0, cap_phead = 0,
            cap_pcount = 0, cap_pair_a = 0, cap_pair_b = 0, cap_woff = 0, cap_W = 0, cap_kv = 0, cap_F = 0,
-           cap_FT = 0, cap_C = 0, cap_Ci = 0, cap_R = 0, cap_Fc = 0, cap_Dinv = 0, cap_g = 0, cap_y = 0,
+           cap_fpart = 0, cap_C = 0, cap_Ci = 0, cap_R = 0, cap_Fc = 0, cap_Dinv = 0, cap_g = 0, cap_y = 0,
            cap_u = 0, cap_t = 0, cap_rows = 0;
 };
 
