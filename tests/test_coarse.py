@@ -70,3 +70,23 @@ def test_two_level_reference_cuts_iterations(oracle_lib):
     assert np.abs(x2 - x1).max() <= 1e-4 * np.abs(x1).max()
     print(f"\nconductor {it1} iterations, two-level {it2}")
     assert it2 * 2 <= it1
+
+
+def test_sparse_coarse_solve_converges_to_dense(oracle_lib):
+    """The CG steps of the sparse form approach the exact coarse inverse."""
+    from conductorrigid_b200 import systems
+    from coarse_ref import TwoLevelRef
+
+    s = systems.spheres(np.ones(30), 1, 0.25, (0.0, 0.0, 1.0), seed=7)
+    o = oracle_lib.Oracle(s, systems.XI_DEFAULT, 1e-5, 32, 9, 4.0)
+    pd = oracle_lib.params_dict(o.p)
+    phiq, _ = oracle_lib.tables(o.p)
+    der = dict(rcut=pd["rc"], dr=pd["dr"], n_table=pd["N_table"], selfcoeff=pd["selfcoeff"])
+    ref = TwoLevelRef(s, der, phiq, systems.XI_DEFAULT)
+    g = np.random.default_rng(3).standard_normal(ref.C.shape[0])
+    exact = ref.coarse_solve(g)
+    errs = []
+    for k in (2, 8, 40):
+        ref.pcg_steps = k
+        errs.append(np.linalg.norm(ref.coarse_solve(g) - exact) / np.linalg.norm(exact))
+    assert errs[0] > errs[1] > errs[2] and errs[2] < 1e-8
