@@ -42,7 +42,7 @@ constexpr int CS = 32;  // beads per cluster
 
 struct RSBuild {
     double L[3], Linv[3];
-    double rc, rc2, rmin2, dr, inv_dr;
+    double rc, rc2, rmin2, dr, inv_dr, scale;  // scale = ntab / (rc - dr)
     int ntab;
 };
 
@@ -152,11 +152,21 @@ __global__ void pair_owner_kernel(int nclus, const long long *__restrict__ head,
 }
 
 __device__ __forceinline__ double table_lerp64(const double2 *__restrict__ tab, const RSBuild &c, double d) {
-    int ind = (int)floor(c.ntab * (d - c.dr) / (c.rc - c.dr));
+    int ind = (int)floor((d - c.dr) * c.scale);
     ind = min(max(ind, 0), c.ntab - 1);
     const double lin = d * c.inv_dr - ind - 1.0;
     const double2 e = tab[ind];
     return e.x + (e.y - e.x) * lin;
+}
+
+// 1/sqrt(d2) for d2 > 0 in FP64: the FP32 estimate refined by two Newton-Raphson steps
+// for the reciprocal square root, y <- y (3 - d2 y^2) / 2 (relative error squared per
+// step: ~1e-7 -> ~1e-14 -> the FP64 rounding level).
+__device__ __forceinline__ double rsqrt64(double d2) {
+    double y = (double)rsqrtf((float)d2);
+    y = y * (1.5 - 0.5 * d2 * y * y);
+    y = y * (1.5 - 0.5 * d2 * y * y);
+    return y;
 }
 
 // Bit masks of the in-range bead pairs of every cluster pair (row i = bead i of I,
@@ -265,7 +275,8 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
             const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
             const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
             const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
-            t = table_lerp64(tab, c, sqrt(dx * dx + dy * dy + dz * dz));
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            t = table_lerp64(tab, c, d2 * rsqrt64(d2));
         }
         out[(size_t)k * CS] = (R)t;
         if (BOTH) out2[(size_t)k * CS] = t;
@@ -411,8 +422,9 @@ __global__ void __launch_bounds__(W * 32) pair_force_kernel(const long long *__r
                 const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
                 const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
                 const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
-                const double d = sqrt(dx * dx + dy * dy + dz * dz);
-                const double a = -table_lerp64(tab, c, d) * qi * qj / d;
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                const double inv_d = rsqrt64(d2);
+                const double a = -table_lerp64(tab, c, d2 * inv_d) * qi * qj * inv_d;
                 fi[0] += a * dx;
                 fi[1] += a * dy;
                 fi[2] += a * dz;
@@ -455,6 +467,7 @@ RSBuild rs_build(const cr_handle *h) {
     c.dr = h->d.dr;
     c.inv_dr = 1.0 / h->d.dr;
     c.ntab = h->d.n_table;
+    c.scale = h->d.n_table / (h->d.rcut - h->d.dr);
     return c;
 }
 
