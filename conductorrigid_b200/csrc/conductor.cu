@@ -15,6 +15,7 @@
 // (distance matrices compared entry by entry), factorised once in FP64 (Cholesky),
 // and applied on the device, one CTA per body.  In flexible GMRES any fixed or varying
 // preconditioner leaves the solution unchanged; only the iteration count moves.
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <tuple>
@@ -242,7 +243,8 @@ int conductor_apply(cr_handle *h, const double *x, double *y) {
     if (!C.ready) return fail(h, CR_NOT_READY, "conductor preconditioner not set up");
     if (h->B == 0) return CR_OK;
     const size_t smem = (size_t)C.max_n * sizeof(double);
-    conductor_apply_kernel<<<h->B, 128, smem, h->stream>>>(h->N, h->B, h->d_body_start, h->d_body_members,
+    const int threads = std::min(256, std::max(64, (C.max_n + 31) / 32 * 32));  // one pass over a body's rows
+    conductor_apply_kernel<<<h->B, threads, smem, h->stream>>>(h->N, h->B, h->d_body_start, h->d_body_members,
                                                            C.d_body_shape, C.d_shape_n, C.d_shape_mat, C.d_shape_vec,
                                                            C.d_kinv, C.d_u, C.d_invs, x, y);
     CR_LAUNCH(h, "conductor_apply_kernel");
