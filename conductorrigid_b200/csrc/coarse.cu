@@ -1072,8 +1072,8 @@ int coarse_prepare(cr_handle *h) {
     }
     const int nrows = (int)rows.size();
     const int K2 = std::max(16, (2 * nmodes + 15) / 16 * 16);
-    // dense: padded order (identity on the padding); sparse: rows of whole float4
-    const int np = sparse ? (nc + 3) / 4 * 4 : (nc + GT - 1) / GT * GT;
+    // dense: padded order (identity on the padding)
+    const int np = sparse ? nc : (nc + GT - 1) / GT * GT;
     const int K = cs.pcg_iters;
     const int nspmv = (nbc + kSpmvWarpsC - 1) / kSpmvWarpsC, nvec = (nbc + kVecThreads - 1) / kVecThreads;
     CR_TRY(grow(h, &cs.kv, cs.cap_kv, (size_t)std::max(nmodes, 1), moved));
@@ -1092,7 +1092,7 @@ int coarse_prepare(cr_handle *h) {
         CR_TRY(grow(h, &cs.Dblk, cs.cap_Dblk, (size_t)nbc * 9, moved));
         CR_TRY(grow(h, &cs.pr, cs.cap_pr, (size_t)np, moved));
         CR_TRY(grow(h, &cs.pz, cs.cap_pz, (size_t)np, moved));
-        CR_TRY(grow(h, &cs.pp, cs.cap_pp, (size_t)np, moved));  // zero beyond nc: read by whole float4 rows
+        CR_TRY(grow(h, &cs.pp, cs.cap_pp, (size_t)np, moved));
         CR_TRY(grow(h, &cs.pq, cs.cap_pq, (size_t)np, moved));
         CR_TRY(grow(h, &cs.pu, cs.cap_pu, (size_t)K2, moved));
         CR_TRY(grow(h, &cs.part_pq, cs.cap_part_pq, (size_t)K * nspmv, moved));
@@ -1118,7 +1118,6 @@ int coarse_prepare(cr_handle *h) {
         CR_CUDA(h, cudaFuncSetAttribute(coarse_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)model_smem));
     CR_CUDA(h, cudaMemsetAsync(cs.F, 0, (size_t)nc * K2 * sizeof(float), h->stream));
-    if (sparse) CR_CUDA(h, cudaMemsetAsync(cs.pp, 0, (size_t)np * sizeof(double), h->stream));
     CR_CUDA(h, cudaMemsetAsync(cs.g, 0, (size_t)np * sizeof(double), h->stream));
     CR_CUDA(h, cudaMemsetAsync(cs.y, 0, (size_t)np * sizeof(double), h->stream));
     if (nmodes > 0) {
