@@ -51,6 +51,7 @@ constexpr int kMaxSparse = 786432;  // coarse unknowns above which the level is 
 constexpr int kMaxModes = 1024;     // half-space wave vectors kept (kc shrinks above)
 constexpr int kMaxModesSparse = 256;  // the same for the sparse form (its CG steps read F twice)
 constexpr int NB = 64;              // Gauss-Jordan block
+constexpr int GT = 128;             // Gauss-Jordan update tile; the padded order is a multiple of it
 constexpr int kChunk = 512;         // beads staged in shared memory per pass
 
 __device__ __forceinline__ double mimgd(double d, double L, double Linv) { return d - L * rint(d * Linv); }
@@ -414,6 +415,10 @@ __global__ void symmetrise_kernel(int n, double *__restrict__ C, int ldc) {
 // Fc = A_*K;  A_i* = (A_i* with A_iK := 0) - Fc_i R  (i not in K);  A_K* = R.
 // FP32 is enough for a preconditioner: the coarse operators met here have condition
 // numbers of 1e2-1e3, so C^-1 carries relative errors ~1e-4 at worst.
+// Symmetry: with S the indices swept so far, A_ij = A_ji when i and j are both in S or both
+// outside it, and A_ij = -A_ji otherwise (the sweep operator's sign rule); so only the
+// 128 x 128 tiles on and below the diagonal are updated, the panels read the missing
+// entries through that rule, and the upper tiles are mirrored at the end.
 
 // Dinv of the pivot block (one CTA of kPivThreads threads, scalar in-place Gauss-Jordan in
 // shared memory; thread t owns entries (t/64 + kPivStride u, t%64)); a pivot that is not
@@ -460,10 +465,12 @@ __global__ void gj_panel_kernel(int k0, int np, const float *__restrict__ A, con
     __shared__ float Ds[NB][NB + 1];
     __shared__ float As[NB][NB + 1];
     const int j0 = blockIdx.x * NB;
+    const int tK = k0 / GT, tj = j0 / GT;
     for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
         const int r = t / NB, c = t % NB;
         Ds[r][c] = Dinv[t];
-        As[r][c] = A[(size_t)(k0 + r) * np + j0 + c];
+        // A_K,j right of the pivot's tile: from the stored A_j,K (both unswept: same sign)
+        As[r][c] = tj > tK ? A[(size_t)(j0 + c) * np + k0 + r] : A[(size_t)(k0 + r) * np + j0 + c];
     }
     __syncthreads();
     const bool diag = j0 == k0;
@@ -481,20 +488,26 @@ __global__ void gj_panel_kernel(int k0, int np, const float *__restrict__ A, con
     }
     for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {  // rows j0.. of the column panel
         const int r = t / NB, c = t % NB;
-        Fc[(size_t)(j0 + r) * NB + c] = A[(size_t)(j0 + r) * np + k0 + c];
+        // A_i,K above the pivot's tile: i swept, K not, so A_i,K = -A_K,i
+        Fc[(size_t)(j0 + r) * NB + c] =
+            tj < tK ? -A[(size_t)(k0 + c) * np + j0 + r] : A[(size_t)(j0 + r) * np + k0 + c];
     }
 }
 
 // A_i* = (A_i*, A_iK := 0) - Fc_i R for i outside K; A_K* = R.  128 x 128 tile per CTA,
 // 8 x 8 outputs per thread (rows and columns {4t..4t+3} and {64+4t..64+4t+3}, so every
 // shared-memory read is a conflict-free float4), the inner dimension in two halves of 32.
-constexpr int GT = 128;  // update tile; the padded order is a multiple of it
 __global__ void __launch_bounds__(256) gj_update_kernel(int k0, int np, float *__restrict__ A,
                                                         const float *__restrict__ R, const float *__restrict__ Fc) {
     __shared__ __align__(16) float Fs[32][GT + 4];
     __shared__ __align__(16) float Rs[32][GT + 4];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int r0 = blockIdx.y * GT, c0 = blockIdx.x * GT;
+    // block b -> lower tile (tr, tc), tc <= tr, b = tr (tr + 1) / 2 + tc
+    int tr = (int)((sqrtf(8.0f * blockIdx.x + 1.0f) - 1.0f) * 0.5f);
+    while ((tr + 1) * (tr + 2) / 2 <= (int)blockIdx.x) ++tr;
+    while (tr * (tr + 1) / 2 > (int)blockIdx.x) --tr;
+    const int tc = blockIdx.x - tr * (tr + 1) / 2;
+    const int r0 = tr * GT, c0 = tc * GT;
     float acc[8][8];
 #pragma unroll
     for (int u = 0; u < 8; ++u)
@@ -546,6 +559,14 @@ __global__ void __launch_bounds__(256) gj_update_kernel(int k0, int np, float *_
             }
         }
     }
+}
+
+// The upper tiles from the lower ones (the inverse is symmetric).
+__global__ void mirror_upper_kernel(int np, float *__restrict__ A) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)np * np) return;
+    const int r = (int)(t / np), c = (int)(t % np);
+    if (r / GT < c / GT) A[t] = A[(size_t)c * np + r];
 }
 
 __global__ void to_float_kernel(long long n, const double *__restrict__ a, float *__restrict__ b) {
@@ -1176,9 +1197,12 @@ int coarse_prepare(cr_handle *h) {
             CR_LAUNCH(h, "gj_pivot_kernel");
             gj_panel_kernel<<<np / NB, 256, 0, h->stream>>>(k0, np, cs.Ci, cs.Dinv, cs.R, cs.Fc);
             CR_LAUNCH(h, "gj_panel_kernel");
-            gj_update_kernel<<<dim3(np / GT, np / GT), 256, 0, h->stream>>>(k0, np, cs.Ci, cs.R, cs.Fc);
+            const int nt = np / GT;
+            gj_update_kernel<<<nt * (nt + 1) / 2, 256, 0, h->stream>>>(k0, np, cs.Ci, cs.R, cs.Fc);
             CR_LAUNCH(h, "gj_update_kernel");
         }
+        mirror_upper_kernel<<<blocks_for((long)np * np, 256), 256, 0, h->stream>>>(np, cs.Ci);
+        CR_LAUNCH(h, "mirror_upper_kernel");
     } else {
         block_jacobi_kernel<<<blocks_for(nbc, 128), 128, 0, h->stream>>>(nbc, cs.phead, cs.pcount, cs.pair_b, cs.Cblk,
                                                                           cs.F, K2, cs.Dblk, h->d_flag);
