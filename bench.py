@@ -467,7 +467,7 @@ def main() -> None:
                          "mixture and the dynamics)")
     ap.add_argument("--coarse-max-dense", type=int, default=12288,
                     help="coarse problems above this many unknowns use the sparse form (--coarse-cg steps of CG on "
-                         "near-pair blocks) or, with --coarse-cg 0, no coarse level")
+                         "near-pair blocks + the low-rank wave term) or, with --coarse-cg 0, no coarse level")
     ap.add_argument("--coarse-cg", type=int, default=0, help="CG steps of the sparse coarse form")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

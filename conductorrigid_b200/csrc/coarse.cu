@@ -680,10 +680,13 @@ __global__ void __launch_bounds__(256) fcol_partial_kernel(int nc, int K2, const
 template <typename T>
 __global__ void fcol_reduce_kernel(int nchunk, int K2, const double *__restrict__ part, int nmodes,
                                    const float4 *__restrict__ kv, T *__restrict__ u) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    // one warp per column: lane l sums chunks l, l+32, ..., then a fixed shuffle tree
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (k >= K2) return;
     double s = 0.0;
-    for (int q = 0; q < nchunk; ++q) s += part[(size_t)q * K2 + k];
+    for (int q = lane; q < nchunk; q += 32) s += part[(size_t)q * K2 + k];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane != 0) return;
     if (kv) s = k < 2 * nmodes ? s * kv[k >> 1].w : 0.0;
     u[k] = (T)s;
 }
@@ -1255,7 +1258,7 @@ int coarse_apply(cr_handle *h, const double *x, double *z) {
                 const int nchunk = (cs.nc + kColRows - 1) / kColRows;
                 fcol_partial_kernel<<<nchunk, 256, 0, h->stream>>>(cs.nc, cs.K2, cs.F, cs.pp, cs.fpart);
                 CR_LAUNCH(h, "fcol_partial_kernel");
-                fcol_reduce_kernel<double><<<blocks_for(cs.K2, 256), 256, 0, h->stream>>>(
+                fcol_reduce_kernel<double><<<blocks_for(32L * cs.K2, 256), 256, 0, h->stream>>>(
                     nchunk, cs.K2, cs.fpart, 0, nullptr, cs.pu);
                 CR_LAUNCH(h, "fcol_reduce_kernel");
             }
@@ -1278,7 +1281,7 @@ int coarse_apply(cr_handle *h, const double *x, double *z) {
         const int nchunk = (cs.nc + kColRows - 1) / kColRows;
         fcol_partial_kernel<<<nchunk, 256, 0, h->stream>>>(cs.nc, cs.K2, cs.F, cs.y, cs.fpart);
         CR_LAUNCH(h, "fcol_partial_kernel");
-        fcol_reduce_kernel<float><<<blocks_for(cs.K2, 256), 256, 0, h->stream>>>(nchunk, cs.K2, cs.fpart, cs.nmodes,
+        fcol_reduce_kernel<float><<<blocks_for(32L * cs.K2, 256), 256, 0, h->stream>>>(nchunk, cs.K2, cs.fpart, cs.nmodes,
                                                                                cs.kv, cs.u);
         CR_LAUNCH(h, "fcol_reduce_kernel");
     }

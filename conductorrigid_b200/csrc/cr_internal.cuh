@@ -170,7 +170,7 @@ struct CoarseSpace {
     int nrows = 0, bs = 128;            // runs; threads per body CTA of the A~ Z y kernel
     size_t model_smem = 0;              // dynamic shared memory of the A~ Z y kernel
     // sparse level (coarse problems above max_dense unknowns): near-pair blocks, PCG
-    int max_dense = 12288, pcg_iters = 0;  // pcg_iters 0: no coarse level above max_dense
+    int max_dense = 12288, pcg_iters = 0;  // above max_dense: pcg_iters CG steps (0: no coarse level)
     bool sparse = false;
     int nspmv = 0, nvec = 0;            // blocks of the PCG kernels (partial sums per block)
     double *Cblk = nullptr;             // [npairs][9] C_ab of each ordered near pair

@@ -184,9 +184,9 @@ int cr_precondition(cr_handle *h, const double *d_x, double *d_y);
  * and 1 when the sparse form (near-pair blocks, CG steps) is in use. */
 int cr_coarse_info(cr_handle *h, int *active, int *n_coarse, long long *n_pairs, int *n_modes, int *sparse);
 /* Coarse problems with more than max_dense unknowns (default 12288) skip the coarse level
- * (pcg_iterations = 0, the default) or use the sparse form (pcg_iterations > 0): self and
- * real-space terms only, 3 x 3 blocks of near body pairs, pcg_iterations block-Jacobi CG
- * steps per application instead of a dense inverse. */
+ * (pcg_iterations = 0, the default) or use the sparse form (pcg_iterations > 0): 3 x 3
+ * blocks of near body pairs plus the low-rank wave-space term, pcg_iterations
+ * block-Jacobi CG steps per application instead of a dense inverse. */
 int cr_set_coarse(cr_handle *h, int max_dense, int pcg_iterations);
 /* Right-hand side [-(r_i - R_b).E0 ; Q_b] (compute_objective, cu:764-813). */
 int cr_objective(cr_handle *h, double *d_rhs);
