@@ -91,3 +91,47 @@ def test_sparse_coarse_solve_converges_to_dense(oracle_lib):
         errs.append(np.linalg.norm(ref.coarse_solve(g) - exact) / np.linalg.norm(exact))
     print(f"\ncoarse CG steps 2 / 8 / 40: relative error {errs[0]:.1e} / {errs[1]:.1e} / {errs[2]:.1e}")
     assert errs[0] > errs[1] > errs[2] and errs[2] < 1e-4
+
+
+def test_lower_tile_gauss_jordan_matches_inverse():
+    """The coarse inverse's blocked Gauss-Jordan restated: 64-wide pivot blocks, only the
+    128 x 128 tiles on and below the diagonal updated (upper tiles never read), panels
+    completed by the sweep operator's sign rule, upper tiles mirrored at the end."""
+    rng = np.random.default_rng(0)
+    n, NB, GT = 384, 64, 128
+    T = n // GT
+    X = rng.standard_normal((n, n))
+    C = X @ X.T + n * np.eye(n)
+    A = C.copy()
+    for tr in range(T):
+        for tc in range(tr + 1, T):
+            A[tr * GT:(tr + 1) * GT, tc * GT:(tc + 1) * GT] = np.nan  # must never be read
+
+    def tile(i):
+        return i // GT
+
+    for k0 in range(0, n, NB):
+        K = slice(k0, k0 + NB)
+        tK = tile(k0)
+        Dinv = np.linalg.inv(A[K, K])
+        AK = np.stack([A[j, K] if tile(j) > tK else A[K, j] for j in range(n)], axis=1)
+        R = Dinv @ AK
+        R[:, K] = Dinv
+        Fc = np.stack([-A[K, i] if tile(i) < tK else A[i, K] for i in range(n)], axis=0)
+        An = A.copy()
+        for tr in range(T):
+            for tc in range(tr + 1):
+                cols = np.arange(tc * GT, (tc + 1) * GT)
+                for i in range(tr * GT, (tr + 1) * GT):
+                    if k0 <= i < k0 + NB:
+                        An[i, cols] = R[i - k0, cols]
+                    else:
+                        old = A[i, cols].copy()
+                        old[(cols >= k0) & (cols < k0 + NB)] = 0.0
+                        An[i, cols] = old - Fc[i] @ R[:, cols]
+        A = An
+    for tr in range(T):
+        for tc in range(tr + 1, T):
+            A[tr * GT:(tr + 1) * GT, tc * GT:(tc + 1) * GT] = A[tc * GT:(tc + 1) * GT, tr * GT:(tr + 1) * GT].T
+    ref = np.linalg.inv(C)
+    assert np.abs(A - ref).max() <= 1e-12 * np.abs(ref).max()
