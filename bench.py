@@ -4,16 +4,21 @@ One step = one full solve of the workload: right-hand side, flexible GMRES to a 
 relative residual of 1e-6, and the bead forces, through the C ABI (cr_compute).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload precision_162k|plain_small|replicas_256|dynamics_420k|mlp|polydisperse_204k]
 
-Our arm times the headline solver (FP32 operator inside FP64-Arnoldi flexible GMRES
-with FP64 refinement, each Arnoldi step a captured CUDA graph; the learned warm start
-when enabled) and, in the same run, the plain FP64 solve of the same method on the same
-B200.  Kernel shares and the roofline come from a profiled (uncaptured) pass of the same
-steps right after the timed region.  Inputs are resident in HBM for
-``value``; ``e2e`` repeats the step through cr_compute_host with host buffers, the
-copies inside the timed region.  Multi-GPU runs are independent replicas (one system
-per rank, no collective on the data path).  ``--impl reference`` times the reference
-method's CPU implementation (the FP64 oracle port) on the host cores.
+The headline arm (FP32 operator inside FP64-Arnoldi flexible GMRES with FP64 refinement,
+two-level preconditioner, each Arnoldi step a captured CUDA graph) is timed beside, in
+the same run on the same B200: the same solver in FP64 (the precision-only ratio), FP64
+with the conductor response only, and the plain FP64 method with the reference's
+diagonal preconditioner.  Every arm's solution is compared with the oracle's (q, Phi,
+F).  Kernel shares and the roofline come from a profiled (uncaptured) pass of the same
+steps right after the timed region.  Inputs are resident in HBM for ``value``; ``e2e``
+repeats the step through cr_compute_host with host buffers, the copies inside the timed
+region.  ``--workload plain_small`` is the 4,200-charge plain-method system (FP64
+throughout), with a measured full CPU solve beside it.  Multi-GPU runs are independent
+replicas (one system per rank, no collective on the data path).  ``--impl reference``
+times the reference method's CPU implementation (the FP64 oracle port) on the host
+cores, with inputs from the oracle-side generator.
 """
 from __future__ import annotations
 
@@ -39,10 +44,10 @@ UNIT = "solves/s"
 RESTART = 50          # headline arm (conductor-response preconditioner)
 RESTART_PLAIN = 300   # plain arm: the reference's diagonal preconditioner stagnates with short restarts
 TOL = 1e-6
-#: operator applications of one plain FP64 solve of the 162k-charge workload (seed 1),
-#: measured on B200 with this repository's FGMRES(50); scales the CPU timings of a
-#: bounded sample of applications to a full solve
-MATVECS_PER_SOLVE_FP64 = {"precision_162k": 3849}
+#: GMRES iterations of one plain FP64 solve (the reference's diagonal preconditioner,
+#: restart 300, true relative residual 1e-6) of the 162k-charge workload (seed 1),
+#: measured on B200; projects the reference arm's sampled CPU iterations to a solve
+ITERATIONS_PLAIN_FP64 = {"precision_162k": 3835}
 
 PROFILE_BYTES_DOC = {
     "spread": "N*(16+s) + G*s (positions and charges in, one real mesh written)",
@@ -148,49 +153,6 @@ def algorithmic_bytes(kind: str, prec_bytes: int, N: int, G: int, pairs: int, cl
     if kind == "scale":
         return (G / 2) * (2 * s * 2 + s)
     return float("nan")
-
-
-def run_reference(args) -> None:
-    """The reference method's CPU implementation (FP64 oracle port) on the host cores."""
-    rank = env_int("RANK", 0)
-    if rank != 0:
-        return
-    import oracle
-    from conductorrigid_b200 import systems
-
-    w = systems.workload(WORKLOAD, seed=1)
-    s, p = w.system, w.params
-    t0 = time.perf_counter()
-    orc = oracle.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
-    setup = time.perf_counter() - t0
-    x = np.random.default_rng(0).standard_normal(s.n_beads + s.n_bodies)
-    n_mv = 1
-    for _ in range(args.warmup):
-        orc.matvec(x)
-    times = []
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        for _ in range(n_mv):
-            orc.matvec(x)
-        times.append((time.perf_counter() - t) / n_mv)
-    t_mv = float(np.median(times))
-    mps = MATVECS_PER_SOLVE_FP64.get(WORKLOAD) or 0
-    solve_s = setup + mps * t_mv if mps else float("nan")
-    value = 1.0 / solve_s if mps else None
-    cores = oracle.lib().orc_num_threads()
-    sample = (f"{args.steps} timed FP64 operator applications of the {s.n_beads}-charge system on {cores} host "
-              f"threads ({t_mv:.3f} s each) plus the neighbour-list setup ({setup:.2f} s), scaled to the "
-              f"{mps} applications of one plain FP64 solve")
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_s * 1e3 if mps else None,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "charges": s.n_beads, "bodies": s.n_bodies, "mesh": p["grid"],
-                   "support": p["support"], "rcut": p["rcut"], "tol": TOL},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
 
 
 def run_op_case(args) -> None:
@@ -442,64 +404,189 @@ def run_polydisperse(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def main() -> None:
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--learned", type=int, default=0)
-    ap.add_argument("--op-case", type=float, default=0.0,
-                    help="profiling case: the workload scaled to this body fraction, --steps operator "
-                         "applications in FP32 (small enough for a full ncu capture)")
-    ap.add_argument("--arms", default="fast,plain,f64c",
-                    help="arms to run: fast (headline), plain (reference preconditioner), f64c (FP64 ablation)")
-    ap.add_argument("--workload", default=WORKLOAD,
-                    choices=[WORKLOAD, "replicas_256", "dynamics_420k", "mlp", "polydisperse_204k"],
-                    help="headline solve (default), 256 batched replicas, or Brownian dynamics")
-    ap.add_argument("--scale", type=float, default=1.0, help="body-count fraction (dynamics; headline profiling cases)")
-    ap.add_argument("--tiling", default="", help="T,MODE: fixed mesh tiling of the headline solver instead of "
-                                                 "cr_autotune (for runs under a profiler)")
-    ap.add_argument("--restart", type=int, default=RESTART, help="FGMRES restart of the headline (fast) arm")
-    ap.add_argument("--precond", default=None, choices=["two_level", "conductor"],
-                    help="preconditioner of the fast arm (default: two_level; conductor for the polydisperse "
-                         "mixture and the dynamics)")
-    ap.add_argument("--coarse-max-dense", type=int, default=12288,
-                    help="coarse problems above this many unknowns use the sparse form (--coarse-cg steps of CG on "
-                         "near-pair blocks + the low-rank wave term) or, with --coarse-cg 0, no coarse level")
-    ap.add_argument("--coarse-cg", type=int, default=0, help="CG steps of the sparse coarse form")
-    args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
-    if args.precond is None:
-        args.precond = "conductor" if args.workload in ("polydisperse_204k", "dynamics_420k") else "two_level"
-    if args.impl == "ours" and args.workload == "replicas_256":
-        run_replicas(args)
-        return
-    if args.impl == "ours" and args.workload == "dynamics_420k":
-        run_dynamics(args)
-        return
-    if args.impl == "ours" and args.workload == "mlp":
-        run_mlp(args)
-        return
-    if args.impl == "ours" and args.workload == "polydisperse_204k":
-        run_polydisperse(args)
-        return
-    if args.op_case > 0:
-        run_op_case(args)
-        return
-    if args.impl == "reference":
-        run_reference(args)
-        return
 
+# ------------------------------------------------------------------ oracle side
+def oracle_solution(name: str, s, p) -> dict:
+    """The oracle's solution of the workload and the oracle's forces at it.
+
+    precision_162k: the committed oracle solution (tests/golden/make_solutions.py: the
+    oracle's operator solved to a true relative residual of 1e-11), its residual
+    re-checked here.  plain_small: the oracle's restatement of the reference's solver
+    (GMRES with the diagonal preconditioner, restart 300) converged to 1e-12 in this run.
+    Forces: the oracle's force pass at those charges (ConductorRigid.cu:1256-1278)."""
+    import oracle
+
+    t0 = time.perf_counter()
+    orc = oracle.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    fixture = ROOT / "tests" / "golden" / f"solution_{name}.npz"
+    if fixture.exists():
+        g = np.load(fixture)
+        if len(g["q"]) != s.n_beads or len(g["phi"]) != s.n_bodies:
+            raise RuntimeError(f"{fixture.name} does not describe this system")
+        q, phi = np.array(g["q"]), np.array(g["phi"])
+        how = f"committed oracle solution ({fixture.name})"
+    else:
+        ref = orc.solve(s.field, restart=300, maxiter=20000, tol=1e-12)
+        q, phi = ref["q"], ref["phi"]
+        how = "oracle GMRES (reference method: diagonal preconditioner, restart 300) to 1e-12 in this run"
+    out = {"q": q, "phi": phi, "force": orc.forces(q, s.field), "oracle": orc, "how": how,
+           "residual": orc.residual(q, phi, s.field)}
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
+def error_vs_oracle(ref: dict, s, q, phi, F) -> dict:
+    """Max-norm errors relative to the largest entry, and the solution's true relative
+    residual under the oracle's operator."""
+    def rel(a, b):
+        return float(np.abs(np.asarray(a) - b).max() / max(np.abs(b).max(), 1e-300))
+
+    return {"q": rel(q, ref["q"]), "phi": rel(phi, ref["phi"]), "force": rel(F, ref["force"]),
+            "oracle_residual": ref["oracle"].residual(q, phi, s.field)}
+
+
+def cpu_gmres_sample(s, p, iterations: int, cycles: int, restart: int = 10) -> dict:
+    """The reference method on the host cores, sampled: the oracle's set-up (tables,
+    neighbour list) and `cycles` complete GMRES(restart) cycles of its restatement of the
+    reference's solver (diagonal preconditioner, ConductorRigid.cu:1051-1151), continuing
+    one solve.  A cycle of `restart` iterations runs restart + 2 operator applications;
+    the time per iteration is the cycle time / restart.  One solve is projected as set-up
+    + `iterations` x that time (operator-dominated: Gram-Schmidt is a few per cent)."""
+    import oracle
+
+    t0 = time.perf_counter()
+    orc = oracle.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    setup = time.perf_counter() - t0
+    b = orc.objective(s.field)
+    x = np.zeros(s.n_beads + s.n_bodies)
+    per_iter = []
+    for _ in range(cycles):
+        t = time.perf_counter()
+        x, it, _ = orc.gmres(b, x0=x, restart=restart, maxiter=restart, tol=1e-300)
+        per_iter.append((time.perf_counter() - t) / max(it, 1))
+    t_it = float(np.median(per_iter))
+    cores = oracle.lib().orc_num_threads()
+    solve_s = setup + iterations * t_it
+    return {"value": 1.0 / solve_s, "unit": UNIT, "cores": cores, "kind": "port", "seconds_per_solve": solve_s,
+            "sample": (f"oracle set-up ({setup:.2f} s) + {cycles} complete GMRES({restart}) cycles of the reference "
+                       f"method (diagonal preconditioner, FP64) on the {s.n_beads}-charge system, {cores} host "
+                       f"threads, {t_it:.3f} s per iteration; projected to the {iterations} iterations the same "
+                       f"method needs to reach 1e-6 (measured on the GPU): extrapolated, not a full solve")}
+
+
+def cpu_full_solve(s, p) -> dict:
+    """One complete solve plus forces of the reference method on the host cores: the
+    oracle's GMRES (diagonal preconditioner, restart 300, CUSP's stopping rule on the
+    left-preconditioned residual, ConductorRigid.cu:1134-1136) to 1e-6, then the force
+    pass.  Measured, not projected."""
+    import oracle
+
+    t0 = time.perf_counter()
+    orc = oracle.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    r = orc.solve(s.field, restart=RESTART_PLAIN, maxiter=20000, tol=TOL)
+    dt = time.perf_counter() - t0
+    cores = oracle.lib().orc_num_threads()
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": cores, "kind": "port", "seconds_per_solve": dt,
+            "iterations": r["iterations"], "true_residual": r["true_rel"],
+            "sample": (f"one measured full FP64 solve + forces of the {s.n_beads}-charge system by the oracle's "
+                       f"reference method (set-up, GMRES({RESTART_PLAIN}) with the diagonal preconditioner to 1e-6, "
+                       f"{r['iterations']} iterations, force pass) on {cores} host threads")}
+
+
+def run_reference(args) -> None:
+    """The reference method's CPU implementation (the FP64 oracle port) on the host cores,
+    on the headline workload; inputs from the oracle-side generator, so that nothing of
+    the CUDA product is loaded.  Each step is one complete GMRES(10) cycle of one
+    continuing solve; the line reports the projected solves/s."""
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return
+    import oracle
+    from oracle import systems as osys
+
+    name = args.workload if args.workload in SOLVE_WORKLOADS else WORKLOAD
+    s, p = osys.workload(name, seed=1)
+    config = {"workload": name, "charges": s.n_beads, "bodies": s.n_bodies, "mesh": p["grid"],
+              "support": p["support"], "rcut": p["rcut"], "tol": TOL, "preconditioner": "diagonal (reference)"}
+    if name not in ITERATIONS_PLAIN_FP64:  # small enough for complete solves: each step one measured solve
+        for _ in range(args.warmup):
+            cpu_full_solve(s, p)
+        runs = [cpu_full_solve(s, p) for _ in range(args.steps)]
+        solve_s = float(np.median([r["seconds_per_solve"] for r in runs]))
+        value = 1.0 / solve_s
+        cb = dict(runs[-1], value=value)
+        cb.pop("seconds_per_solve", None)
+        print(json.dumps({"impl": "reference", "metric": SOLVE_WORKLOADS[name][2], "value": value, "unit": UNIT,
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": solve_s * 1e3, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                          "cpu_baseline": cb,
+                          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    iterations = ITERATIONS_PLAIN_FP64[name]
+    t0 = time.perf_counter()
+    orc = oracle.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    setup = time.perf_counter() - t0
+    b = orc.objective(s.field)
+    x = np.zeros(s.n_beads + s.n_bodies)
+    per_iter = []
+    for k in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        x, it, _ = orc.gmres(b, x0=x, restart=10, maxiter=10, tol=1e-300)
+        if k >= args.warmup:
+            per_iter.append((time.perf_counter() - t) / max(it, 1))
+    t_it = float(np.median(per_iter))
+    solve_s = setup + iterations * t_it
+    value = 1.0 / solve_s
+    cores = oracle.lib().orc_num_threads()
+    sample = (f"oracle set-up ({setup:.2f} s) + {args.steps} timed complete GMRES(10) cycles ({args.warmup} warm-up) "
+              f"of the reference method (diagonal preconditioner, FP64) on the {s.n_beads}-charge system, {cores} "
+              f"host threads, {t_it:.3f} s per iteration; projected to the {iterations} iterations the same method "
+              f"needs to reach 1e-6 (measured on the GPU): extrapolated, not a full solve")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_s * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------- solve workloads
+#: solver arms: precision, preconditioner, restart (None: --restart)
+ARMS = {
+    "fast": ("mixed", None, None),            # FP32 operator, FP64 Krylov; --precond (two-level by default)
+    "f64t": ("fp64", "two_level", RESTART),   # FP64, the same preconditioner: the precision-only ratio
+    "f64c": ("fp64", "conductor", RESTART),   # FP64, conductor response only
+    "plain": ("fp64", "diagonal", RESTART_PLAIN),  # the reference method in FP64
+}
+ARM_LABELS = {
+    "fast": "FP32 operator in FGMRES, FP64 Arnoldi / constraints / refinement",
+    "f64t": "FP64 throughout, same preconditioner as the headline",
+    "f64c": "FP64 throughout, conductor-response preconditioner",
+    "plain": "FP64 throughout, the reference's diagonal preconditioner (plain method)",
+}
+#: workload -> (headline arm, arms, metric)
+SOLVE_WORKLOADS = {
+    "precision_162k": ("fast", ("fast", "f64t", "f64c", "plain"), METRIC),
+    "plain_small": ("plain", ("plain", "f64t", "fast"),
+                    "solves/s of the plain FP64 method (one solve + forces, 1e-6 residual), 4,200 charges"),
+}
+
+
+def run_solve(args) -> None:
     import torch
     import torch.distributed as dist
 
-    from conductorrigid_b200 import _lib, systems
+    from conductorrigid_b200 import _lib, ranks, systems
     from conductorrigid_b200.device import Handle
 
-    from conductorrigid_b200 import ranks
-
+    name = args.workload
+    head_arm, all_arms, metric = SOLVE_WORKLOADS[name]
+    arms = [a for a in all_arms if a in set(args.arms.split(",")) or a == head_arm]
     rank, local, world = ranks.rank_info()
     torch.cuda.set_device(local)
     if world > 1:
@@ -507,48 +594,46 @@ def main() -> None:
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
-    def barrier():
-        ranks.barrier(world)
-
-    def max_over_ranks(v: float) -> float:
-        return ranks.max_over_ranks(v, world, device="cuda")
-
-    w = systems.workload(WORKLOAD, seed=ranks.replica_seed(1, rank), scale=args.scale)
+    w = systems.workload(name, seed=ranks.replica_seed(1, rank), scale=args.scale)
     s, p = w.system, w.params
     if args.scale != 1.0:  # profiling case: fewer bodies at the same mesh spacing
-        full_L = systems.workload(WORKLOAD).system.L[0]
+        full_L = systems.workload(name).system.L[0]
         p = dict(p, grid=systems.smooth_at_least(int(np.ceil(p["grid"] * s.L[0] / full_L)), 4096))
     base = {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")}
     common = dict(field=tuple(s.field), gmres_tol=TOL, maxiter=20000, **base)
     stream = torch.cuda.Stream()
-    h_fast = Handle(_lib.make_params(precision="mixed", learned=bool(args.learned), precond=args.precond,
-                                     restart=args.restart, **common), s.L, stream=stream)
-    h_fast.set_coarse(args.coarse_max_dense, args.coarse_cg)
-    h_plain = Handle(_lib.make_params(precision="fp64", precond="diagonal", restart=RESTART_PLAIN, **common), s.L,
-                     stream=stream)
-    h_f64c = Handle(_lib.make_params(precision="fp64", precond="conductor", restart=RESTART, **common), s.L,
-                    stream=stream)
-    for h in (h_fast, h_plain, h_f64c):
+    handles = {}
+    for a in arms:
+        prec, pc, rs = ARMS[a]
+        h = Handle(_lib.make_params(precision=prec, precond=pc or args.precond, restart=rs or args.restart,
+                                    learned=bool(args.learned) and a == "fast", **common), s.L, stream=stream)
+        h.set_coarse(args.coarse_max_dense, args.coarse_cg)
         h.set_topology(s.body, s.rigid, s.body_charge)
-    pos = h_fast.dev(s.pos)
-    bpos = h_fast.dev(s.body_pos)
+        handles[a] = h
+    hh = handles[head_arm]
+    pos = hh.dev(s.pos)
+    bpos = hh.dev(s.body_pos)
     if args.tiling:  # an explicit tiling (profiling runs: timing-based choices are not valid under a profiler)
         t_edge, t_mode = (int(v) for v in args.tiling.split(","))
-        h_fast.set_tiling(t_edge, t_mode)
+        for h in handles.values():
+            h.set_tiling(t_edge, t_mode)
         tiling = {"tile_edge": t_edge, "spread_mode": t_mode, "mesh_ms": None}
     else:
-        tiling = h_fast.autotune(pos, bpos, reps=5)  # untimed set-up
+        tiling = handles["fast"].autotune(pos, bpos, reps=5) if "fast" in handles else None  # untimed set-up
     q = torch.zeros(s.n_beads, dtype=torch.float64, device="cuda")
     phi = torch.zeros(s.n_bodies, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+    results = {}
 
-    def timed(h, steps, profile=False):
-        """Per-step device time (CUDA events on the solver's stream), L2 flushed before each step."""
-        stats = []
-        total_ms = 0.0
+    def timed(a, steps, profile=False):
+        """Per-step device time (CUDA events on the solver's stream), L2 flushed before each
+        step; the last step's solution is kept for the error check."""
+        h = handles[a]
+        stats, total_ms = [], 0.0
         if profile:
             h.profile(True)
         c0 = h.counters()
+        F = None
         for _ in range(steps):
             with torch.cuda.stream(stream):
                 flush.fill_(1.0)
@@ -565,165 +650,210 @@ def main() -> None:
         prof = h.profile_read() if profile else None
         if profile:
             h.profile(False)
-        launches = c1["kernel_launches"] - c0["kernel_launches"]
-        return total_ms / steps, stats, prof, launches, c1["fft_execs"] - c0["fft_execs"]
+        sol = (q.cpu().numpy(), phi.cpu().numpy(), F.cpu().numpy())
+        return {"ms": total_ms / steps, "stats": stats, "prof": prof, "sol": sol,
+                "launches": c1["kernel_launches"] - c0["kernel_launches"],
+                "ffts": c1["fft_execs"] - c0["fft_execs"]}
 
-    arms = set(args.arms.split(","))
+    def arm_steps(a):
+        if a == "plain" and name == "precision_162k":
+            return max(1, min(args.steps, 2))  # ~10 s per solve
+        return args.steps
+
     # warm-up (untimed)
-    timed(h_fast, args.warmup)
-    if "f64c" in arms:
-        timed(h_f64c, args.warmup)
-    if "plain" in arms:
-        timed(h_plain, 1)  # one plain solve (~14 s) is warm-up enough for its kernels
-
+    for a in arms:
+        timed(a, 1 if (a == "plain" and name == "precision_162k") else args.warmup)
     dev_id = str(local)
     try:
-        uuid = torch.cuda.get_device_properties(local).uuid
-        dev_id = "GPU-" + str(uuid)
+        dev_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     except Exception:
         pass
     clocks = ClockSampler(dev_id)
     torch.cuda.synchronize()
-    barrier()
+    ranks.barrier(world)
     clocks.start()
-    # captured Arnoldi steps (the default with a stream set) need the profiler off
-    ms_fast, st_fast, _, launches, ffts = timed(h_fast, args.steps)
+    results[head_arm] = timed(head_arm, args.steps)
     torch.cuda.synchronize()
-    barrier()
-    ms_f64c, st_f64c = float("nan"), [{"iterations": None, "final_residual": None}]
-    if "f64c" in arms:
-        ms_f64c, st_f64c, _, _, _ = timed(h_f64c, args.steps)
-    torch.cuda.synchronize()
-    barrier()
+    ranks.barrier(world)
     clk = clocks.stop()
-    # per-kernel times: the same steps again, uncaptured, under the in-library CUDA-event profiler
-    ms_fast_prof, _, prof, _, _ = timed(h_fast, args.steps, profile=True)
+    for a in arms:
+        if a != head_arm:
+            results[a] = timed(a, arm_steps(a))
+            torch.cuda.synchronize()
+            ranks.barrier(world)
+    # per-kernel times: the headline steps again, uncaptured, under the in-library profiler
+    prof_run = timed(head_arm, args.steps, profile=True)
+    prof = prof_run["prof"]
     torch.cuda.synchronize()
-    barrier()
-    ms_plain = float("nan")
-    st_plain = [{"iterations": None, "matvecs_fp64": MATVECS_PER_SOLVE_FP64[WORKLOAD], "final_residual": None,
-                 "converged": None}]
-    if "plain" in arms:
-        ms_plain, st_plain, _, _, _ = timed(h_plain, max(1, min(args.steps, 2)))
-    torch.cuda.synchronize()
-    barrier()
-    ms_fast = max_over_ranks(ms_fast)
-    ms_plain = max_over_ranks(ms_plain)
-    ms_f64c = max_over_ranks(ms_f64c)
+    ranks.barrier(world)
+    ms = {a: ranks.max_over_ranks(results[a]["ms"], world, device="cuda") for a in arms}
 
-    # end to end through the public C ABI on host buffers (pinned)
+    # end to end through the public C ABI on host buffers (pinned), the headline arm
     hp = torch.from_numpy(s.pos.copy()).pin_memory()
     hb = torch.from_numpy(s.body_pos.copy()).pin_memory()
     hq = torch.zeros(s.n_beads, dtype=torch.float64).pin_memory()
     hphi = torch.zeros(s.n_bodies, dtype=torch.float64).pin_memory()
     hf = torch.zeros((s.n_beads, 3), dtype=torch.float64).pin_memory()
     e2e_s = []
-    h_fast.compute_host(hp.numpy(), hb.numpy(), hq.numpy(), hphi.numpy(), hf.numpy())  # untimed: host staging
+    hh.compute_host(hp.numpy(), hb.numpy(), hq.numpy(), hphi.numpy(), hf.numpy())  # untimed: host staging
     for _ in range(args.steps):
         hq.zero_()
         hphi.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        h_fast.compute_host(hp.numpy(), hb.numpy(), hq.numpy(), hphi.numpy(), hf.numpy())
+        hh.compute_host(hp.numpy(), hb.numpy(), hq.numpy(), hphi.numpy(), hf.numpy())
         e2e_s.append(time.perf_counter() - t0)
-    e2e_ms = max_over_ranks(1e3 * float(np.mean(e2e_s)))
+    e2e_ms = ranks.max_over_ranks(1e3 * float(np.mean(e2e_s)), world, device="cuda")
     h2d = 8 * (3 * s.n_beads + 3 * s.n_bodies + s.n_beads + s.n_bodies)
     d2h = 8 * (s.n_beads + s.n_bodies + 3 * s.n_beads)
 
-    # roofline of the dominant kernel class in the timed headline solves
-    geo = h_fast.geometry_info()
+    # roofline of the dominant kernel class in the profiled headline steps
+    prec_bytes = 4 if ARMS[head_arm][0] == "mixed" else 8
+    geo = hh.geometry_info()
     G = int(np.prod([p["grid"]] * 3))
     dom = max((k for k in prof if k not in ("geometry",)), key=lambda k: prof[k]["ms"])
     dom_ms = prof[dom]["ms"] / max(prof[dom]["launches"], 1)
-    alg = algorithmic_bytes(dom, 4, s.n_beads, G, geo["real_space_pairs"], geo["cluster_pairs"])
+    alg = algorithmic_bytes(dom, prec_bytes, s.n_beads, G, geo["real_space_pairs"], geo["cluster_pairs"])
     peak, peak_kind = load_peaks()
     achieved = alg / (dom_ms * 1e-3) / 1e9
     traffic = None
     tpath = ROOT / "profiles" / "ncu_traffic.json"
     if tpath.exists():
         try:
-            traffic = json.loads(tpath.read_text()).get(WORKLOAD, {}).get(dom)
+            traffic = json.loads(tpath.read_text()).get(name, {}).get(dom)
         except Exception:
             traffic = None
     total_prof_ms = sum(v["ms"] for v in prof.values())
     shares = {k: round(v["ms"] / total_prof_ms, 4) for k, v in prof.items() if total_prof_ms > 0}
 
-    value = ranks.job_throughput(1.0, ms_fast, world)
-    plain_value = ranks.job_throughput(1.0, ms_plain, world)
+    # errors of every arm's solution against the oracle (rank 0's system, full size only)
+    errors = None
+    if rank == 0 and args.scale == 1.0 and not args.no_oracle:
+        ref = oracle_solution(name, s, p)
+        errors = {"reference": ref["how"], "reference_oracle_residual": ref["residual"],
+                  "bar": "max-norm error relative to the largest entry; target 1e-5 at residual 1e-6"}
+        for a in arms:
+            errors[a] = error_vs_oracle(ref, s, *results[a]["sol"])
+
+    def arm_summary(a):
+        st = results[a]["stats"][-1]
+        d = {"value": ranks.job_throughput(1.0, ms[a], world), "ms_per_step": ms[a], "what": ARM_LABELS[a],
+             "precision": ARMS[a][0], "preconditioner": ARMS[a][1] or args.precond,
+             "restart": ARMS[a][2] or args.restart, "iterations": st["iterations"],
+             "matvecs_fp64": st["matvecs_fp64"], "matvecs_fp32": st["matvecs_fp32"],
+             "final_residual": st["final_residual"], "converged": st["converged"]}
+        if errors is not None:
+            d["error_vs_oracle"] = errors[a]
+        return d
+
+    st_h = results[head_arm]["stats"][-1]
+    value = ranks.job_throughput(1.0, ms[head_arm], world)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_fast, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 operator / f64 Krylov", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "charges": s.n_beads, "bodies": s.n_bodies, "mesh": p["grid"],
-                   "support": p["support"], "rcut": p["rcut"], "xi": p["xi"], "tol": TOL, "restart": args.restart,
-                   "preconditioner": {"two_level": "two-level (conductor response + induced-dipole coarse "
-                                                    "correction)", "conductor": "conductor response"}[args.precond],
-                   "learned": bool(args.learned),
-                   "mesh_tiling": tiling,
-                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every step"},
-        "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain, "preconditioner": "diagonal (reference)",
-                       "restart": RESTART_PLAIN, "iterations": st_plain[-1]["iterations"],
-                       "matvecs_fp64": st_plain[-1]["matvecs_fp64"],
-                       "final_residual": st_plain[-1]["final_residual"], "converged": st_plain[-1]["converged"]},
-        "fp64_conductor": {"value": world * 1e3 / ms_f64c, "ms_per_step": ms_f64c,
-                           "iterations": st_f64c[-1]["iterations"], "final_residual": st_f64c[-1]["final_residual"]},
-        "speedup_vs_plain_fp64": value / plain_value,
-        "solve": {"iterations": st_fast[-1]["iterations"], "refinements": st_fast[-1]["refinements"],
-                  "coarse_level": h_fast.coarse_info() if args.precond == "two_level" else None,
-                  "matvecs_fp32": st_fast[-1]["matvecs_fp32"], "matvecs_fp64": st_fast[-1]["matvecs_fp64"],
-                  "final_residual": st_fast[-1]["final_residual"]},
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms[head_arm], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"mixed": "f32 operator / f64 Krylov", "fp64": "f64"}[ARMS[head_arm][0]],
+        "data": "synthetic (seeded placement)",
+        "config": {"workload": name, "charges": s.n_beads, "bodies": s.n_bodies, "mesh": p["grid"],
+                   "support": p["support"], "rcut": p["rcut"], "xi": p["xi"], "tol": TOL,
+                   "headline_arm": head_arm, "preconditioner": ARMS[head_arm][1] or args.precond,
+                   "restart": ARMS[head_arm][2] or args.restart,
+                   "learned": (bool(args.learned) if head_arm == "fast" else False),
+                   "learned_note": "n/a for a single static solve: the learned start needs a previous solution "
+                                   "(time stepping, dynamics_420k workload)",
+                   "mesh_tiling": tiling, "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MB write) before every step"},
+        "arms": {a: arm_summary(a) for a in arms},
+        "solve": {"iterations": st_h["iterations"], "refinements": st_h["refinements"],
+                  "coarse_level": hh.coarse_info() if (ARMS[head_arm][1] or args.precond) == "two_level" else None,
+                  "matvecs_fp32": st_h["matvecs_fp32"], "matvecs_fp64": st_h["matvecs_fp64"],
+                  "final_residual": st_h["final_residual"]},
+        "error_vs_oracle": errors[head_arm] if errors is not None else None,
         "kernel_share": shares,
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "launches": prof[dom]["launches"], "avg_launch_ms": dom_ms,
                      "measured_over": "a profiled pass of the same steps right after the timed region "
-                                      f"(uncaptured, {ms_fast_prof:.1f} ms per step): captured graph steps "
+                                      f"(uncaptured, {prof_run['ms']:.1f} ms per step): captured graph steps "
                                       "cannot be timed per kernel",
                      "algorithmic_bytes_per_launch": alg},
         "e2e": {"value": world * 1e3 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": int(launches),
-        "captured_arnoldi_steps": h_fast.graph_launches(),
-        "cufft_execs": int(ffts),
+        "gpu_launches": int(results[head_arm]["launches"]),
+        "captured_arnoldi_steps": hh.graph_launches(),
+        "cufft_execs": int(results[head_arm]["ffts"]),
         "clocks": clk,
     }
-    # spread GB/s (named by the metric)
+    if "plain" in arms and head_arm != "plain":
+        line["speedup_vs_plain_fp64"] = ms["plain"] / ms[head_arm]
+    if "f64t" in arms and head_arm == "fast":
+        line["precision_only_speedup"] = ms["f64t"] / ms["fast"]  # same preconditioner, FP64 vs mixed
     if "spread" in prof and prof["spread"]["launches"]:
         sp_ms = prof["spread"]["ms"] / prof["spread"]["launches"]
-        sp_alg = algorithmic_bytes("spread", 4, s.n_beads, G, 0)
+        sp_alg = algorithmic_bytes("spread", prec_bytes, s.n_beads, G, 0)
         line["spread"] = {"achieved_gbs": sp_alg / (sp_ms * 1e-3) / 1e9, "avg_launch_ms": sp_ms,
                           "frac": sp_alg / (sp_ms * 1e-3) / 1e9 / peak}
-
-    if rank == 0 and world == 1 and not args.no_cpu and st_plain[-1]["matvecs_fp64"]:
-        line["cpu_baseline"] = cpu_baseline(s, p, st_plain[-1]["matvecs_fp64"])
+    if rank == 0 and world == 1 and not args.no_cpu and args.scale == 1.0:
+        if name == "plain_small":
+            line["cpu_baseline"] = cpu_full_solve(s, p)
+        else:
+            it_plain = results["plain"]["stats"][-1]["iterations"] if "plain" in arms else ITERATIONS_PLAIN_FP64[name]
+            line["cpu_baseline"] = cpu_gmres_sample(s, p, it_plain, cycles=2)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    for h in (h_fast, h_plain, h_f64c):
+    for h in handles.values():
         h.close()
     if world > 1:
         dist.destroy_process_group()
 
 
-def cpu_baseline(s, p, matvecs_per_solve: int) -> dict:
-    """The FP64 oracle (port of the reference method) on the host cores: a bounded
-    sample of operator applications, scaled to one plain solve."""
-    import oracle
-
-    t0 = time.perf_counter()
-    orc = oracle.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
-    setup = time.perf_counter() - t0
-    x = np.random.default_rng(0).standard_normal(s.n_beads + s.n_bodies)
-    orc.matvec(x)
-    n, t1 = 0, time.perf_counter()
-    while n < 3 or (time.perf_counter() - t1 < 10.0 and n < 20):
-        orc.matvec(x)
-        n += 1
-    t_mv = (time.perf_counter() - t1) / n
-    cores = oracle.lib().orc_num_threads()
-    solve_s = setup + matvecs_per_solve * t_mv
-    return {"value": 1.0 / solve_s, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": (f"{n} FP64 operator applications of the {s.n_beads}-charge system on {cores} host threads "
-                       f"({t_mv:.3f} s each) plus neighbour-list setup ({setup:.2f} s), scaled to the "
-                       f"{matvecs_per_solve} applications of the plain FP64 solve in this run")}
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-oracle", action="store_true", help="skip the errors against the oracle's solution")
+    ap.add_argument("--learned", type=int, default=0)
+    ap.add_argument("--op-case", type=float, default=0.0,
+                    help="profiling case: the workload scaled to this body fraction, --steps operator "
+                         "applications in FP32 (small enough for a full ncu capture)")
+    ap.add_argument("--arms", default="fast,f64t,f64c,plain",
+                    help="arms to run besides the headline one: fast (FP32 operator), f64t (FP64, same "
+                         "preconditioner), f64c (FP64, conductor response), plain (FP64, reference preconditioner)")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=[WORKLOAD, "plain_small", "replicas_256", "dynamics_420k", "mlp", "polydisperse_204k"],
+                    help="headline solve (default), the small plain-method system, 256 batched replicas, Brownian "
+                         "dynamics, the network kernels, or the charged polydisperse mixture")
+    ap.add_argument("--scale", type=float, default=1.0, help="body-count fraction (dynamics; headline profiling cases)")
+    ap.add_argument("--tiling", default="", help="T,MODE: fixed mesh tiling of the headline solver instead of "
+                                                 "cr_autotune (for runs under a profiler)")
+    ap.add_argument("--restart", type=int, default=RESTART, help="FGMRES restart of the headline (fast) arm")
+    ap.add_argument("--precond", default=None, choices=["two_level", "conductor"],
+                    help="preconditioner of the fast arm (default: two_level; conductor for the polydisperse "
+                         "mixture and the dynamics)")
+    ap.add_argument("--coarse-max-dense", type=int, default=12288,
+                    help="coarse problems above this many unknowns use the sparse form (--coarse-cg steps of CG on "
+                         "near-pair blocks + the low-rank wave term) or, with --coarse-cg 0, no coarse level")
+    ap.add_argument("--coarse-cg", type=int, default=0, help="CG steps of the sparse coarse form")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.precond is None:
+        args.precond = "conductor" if args.workload in ("polydisperse_204k", "dynamics_420k") else "two_level"
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    if args.workload == "replicas_256":
+        run_replicas(args)
+    elif args.workload == "dynamics_420k":
+        run_dynamics(args)
+    elif args.workload == "mlp":
+        run_mlp(args)
+    elif args.workload == "polydisperse_204k":
+        run_polydisperse(args)
+    elif args.op_case > 0:
+        run_op_case(args)
+    else:
+        run_solve(args)
 
 
 if __name__ == "__main__":

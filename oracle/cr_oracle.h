@@ -130,6 +130,14 @@ int orc_solve(orc_ctx *c, const double E0[3], double *q_io, double *phi_io, doub
               int restart, int maxiter, double tol, double *true_rel);
 int orc_num_threads(void);
 
+/* Synthetic systems (cr_systems.cc): icosphere vertices, SplitMix64 uniforms and
+ * random sequential addition of non-overlapping spheres in a periodic box. */
+int orc_icosphere_count(int level);
+int orc_icosphere(int level, double *verts);
+int orc_uniform(uint64_t seed, int64_t n, double *out);
+int orc_place_spheres(int n, const double *radii, const double L[3], uint64_t seed, int64_t max_attempts,
+                      double *centres);
+
 #ifdef __cplusplus
 }
 #endif

@@ -127,7 +127,15 @@ def test_solve_matches_oracle(cuda, product_lib, oracle_lib, precision):
     print(f"\n{precision}: iters={st['iterations']} fp64 mv={st['matvecs_fp64']} fp32 mv={st['matvecs_fp32']} "
           f"resid={st['final_residual']:.2e} err q={eq:.2e} phi={ep:.2e} F={ef:.2e}")
     assert st["converged"] == 1 and st["final_residual"] <= 1e-6
-    assert eq < 1e-3 and ep < 1e-3 and ef < 1e-3
+    # The reference's diagonal preconditioner on this 30-body, 1,260-charge system: the
+    # solver stops on the true residual 1e-6, which leaves Phi within 1e-6 but q only
+    # within ~5e-5 and F within ~1e-5 (measured 5.4e-5 / 4.6e-7 / 9.0e-6 in FP64).  The
+    # bead-shell operator is ill-conditioned and the true residual is dominated by the
+    # body rows; the reference's own stopping rule (CUSP's default_monitor on the
+    # left-preconditioned residual, ConductorRigid.cu:1134-1136, which scales bead rows
+    # by 4 pi) is ~13x stricter on the bead rows.  The conductor and two-level
+    # preconditioners meet 1e-5 in all three (below and tests/test_gpu_solve_parity.py).
+    assert ep < 1e-5 and ef < 2e-5 and eq < 1e-4
 
 
 def test_compute_host_matches_device(cuda, product_lib):
@@ -245,7 +253,7 @@ def test_conductor_preconditioned_solve_matches_oracle(cuda, product_lib, oracle
     print(f"\nconductor {precision}: iters={st['iterations']} resid={st['final_residual']:.2e} "
           f"err q={eq:.2e} phi={ep:.2e} F={ef:.2e}")
     assert st["converged"] == 1 and st["final_residual"] <= 1e-6
-    assert eq < 1e-3 and ep < 1e-3 and ef < 1e-3
+    assert eq < 1e-5 and ep < 1e-5 and ef < 1e-5
 
 
 @pytest.mark.parametrize("support", [7, 11])
