@@ -29,6 +29,9 @@ CR_FP32 = 2
 
 PRECISIONS = {"fp64": CR_FP64, "mixed": CR_MIXED, "fp32": CR_FP32}
 
+CR_REALSPACE_ONFLY32 = 1
+CR_REALSPACE_ONFLY64 = 2
+
 CR_PRECOND_DIAGONAL = 0
 CR_PRECOND_CONDUCTOR = 1
 CR_PRECOND_TWO_LEVEL = 2
@@ -143,6 +146,7 @@ _SIGS = {
     "cr_set_topology": ([_P, _I, C.POINTER(C.c_uint32), _I, C.POINTER(C.c_uint8), _D], _I),
     "cr_set_stream": ([_P, _P], _I),
     "cr_set_graphs": ([_P, _I], _I),
+    "cr_set_realspace": ([_P, _I], _I),
     "cr_set_tiling": ([_P, _I, _I], _I),
     "cr_autotune": ([_P, _P, _P, _I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)], _I),
     "cr_graph_launches": ([_P, C.POINTER(C.c_longlong)], _I),
@@ -160,6 +164,7 @@ _SIGS = {
     "cr_apply_M": ([_P, _P, _P, _I], _I),
     "cr_forces": ([_P, _P, _P, _I], _I),
     "cr_energy": ([_P, _P, C.POINTER(C.c_double)], _I),
+    "cr_virial": ([_P, _P, C.POINTER(C.c_double)], _I),
     "cr_neighbor_list": ([_P, C.c_double, _P, _P, _P, C.c_int64, C.POINTER(C.c_int64)], _I),
     "cr_profile": ([_P, _I], _I),
     "cr_profile_read": ([_P, _I, C.POINTER(C.c_int), C.POINTER(C.c_double)], _I),
@@ -177,6 +182,7 @@ _SIGS = {
     "cr_mlp_accumulate_grad": ([_P, _I, _P, _P, C.POINTER(C.c_double), _P], _I),
     "cr_mlp_adam": ([_P, C.c_double, C.c_double, _P], _I),
     "cr_mlp_counters": ([_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], _I),
+    "cr_mlp_set_wait": ([_P, C.c_longlong, _I], _I),
     "cr_set_guess_directions": ([_P, _I, _P], _I),
     "cr_bead_neighbors": ([_P, _P, _P], _I),
     "cr_body_neighbors": ([_P, _P, _P], _I),

@@ -337,6 +337,15 @@ int cr_set_graphs(cr_handle *h, int enable) {
     return CR_OK;
 }
 
+int cr_set_realspace(cr_handle *h, int flags) {
+    if (!h) return CR_BAD_PARAM;
+    if (flags & ~(CR_REALSPACE_ONFLY32 | CR_REALSPACE_ONFLY64)) return fail(h, CR_BAD_PARAM, "unknown real-space flags");
+    if (h->stream) CR_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->rs_onfly = flags;
+    h->geo_gen++;  // captured Arnoldi steps hold the old kernels: capture again
+    return CR_OK;
+}
+
 int cr_graph_launches(const cr_handle *h, long long *launches) {
     if (!h || !launches) return CR_BAD_PARAM;
     *launches = h->graph_launches;
@@ -487,6 +496,17 @@ int cr_energy(cr_handle *h, const double *d_q, double *energy) {
     CR_LAUNCH(h, "half_dot_kernel");
     CR_CUDA(h, cudaMemcpyAsync(energy, h->d_tmp_n2, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_energy");
+}
+
+int cr_virial(cr_handle *h, const double *d_q, double *virial) {
+    CR_TRY(need_geometry(h));
+    if (!virial) return fail(h, CR_BAD_PARAM, "null output");
+    for (int e = 0; e < 13; ++e) virial[e] = 0.0;
+    if (h->N == 0) return CR_OK;
+    if (!d_q) return fail(h, CR_BAD_PARAM, "null vector");
+    CR_TRY(cast_charges(h, h->m64, d_q));
+    CR_TRY(real_space_virial(h, d_q, virial));
+    return wave_virial(h, virial + 6);
 }
 
 int cr_apply_M(cr_handle *h, const double *d_q, double *d_Mq, int precision) {

@@ -100,6 +100,9 @@ struct RealSpace {
     float *acc32 = nullptr;         // [nclus*32] charges in cluster order
     double *acc64 = nullptr;
     double *freal = nullptr;        // [3N] real-space forces
+    float4 *boff = nullptr;         // [nclus*32] bead offsets from their cluster centre (FP32)
+    float4 *pshift = nullptr;       // [npairs] centre offset of the pair (minimum image), .w = 1 when
+                                    // bead separations need no further image
 };
 
 // GMRES workspace (FP64).
@@ -275,6 +278,8 @@ struct cr_handle {
     double *d_bf = nullptr, *d_bt = nullptr, *d_moves = nullptr;
     // solver graphs: capture one Arnoldi step per geometry when a stream is set
     int use_graphs = 1;
+    // real-space kernel values: CR_REALSPACE_* flags, evaluated on the fly instead of stored
+    int rs_onfly = 0;
     long long geo_gen = 0;
     long long graph_launches = 0;
     // learned guess: caller directions for the next solve [CR_MAX_GUESS_DIRECTIONS][N+B]
@@ -360,6 +365,11 @@ int realspace_alloc(cr_handle *h);
 void realspace_free(cr_handle *h);
 // Clusters and cluster pairs of the current positions.
 int realspace_build(cr_handle *h);
+// Virial tensors (xx, xy, xz, yy, yz, zz) of the FP64 charges q64 at the current geometry:
+// real-space part into out[0..5]; wave-space part of the charges in m64.q into out[0..5]
+// and the wave energy into out[6].
+int real_space_virial(cr_handle *h, const double *q64, double *out);
+int wave_virial(cr_handle *h, double *out);
 int realspace_prepare(cr_handle *h, int precision);
 int mesh_set_tile(cr_handle *h, int T);
 int neighbor_list_build(cr_handle *h, double r_list, int *d_count, int64_t *d_head, int *d_list,

@@ -345,6 +345,59 @@ __global__ void scale_init_kernel(R *scale, int Nx, int Ny, int Nz, double Lx, d
     scale[idx] = (R)(j0 * j0 * exp(-etak2 / (4.0 * xi * xi)) / k2 / ((double)Nx * Ny * Nz));
 }
 
+// Wave-space virial of U_k = 1/2 quadW sum_k S(k) |H(k)|^2 (H the spread mesh's
+// transform, S the influence function, the sum over the full spectrum: modes of the half
+// spectrum with 0 < kz < Nz/2 count twice).  Under the affine strain r -> (1 + e) r of
+// positions and box, with the shell radius fixed, -dU_k/de_ab = sum_k E_k (delta_ab +
+// g(k) k_a k_b / k^2), g = d ln S / d ln k = 2 k cot k - 4 - k^2 / (2 xi^2) for the
+// continuous kernel j0(k)^2 exp(-k^2 / 4 xi^2) / k^2 (the Gaussian splitting factors of
+// the spread and of S combine to it).  Per block: the six tensor components and E_k summed
+// into partial[block][7] (the seventh the wave energy itself).
+__global__ void wave_virial_kernel(const double2 *__restrict__ spec, const double *__restrict__ scale, int Nx,
+                                   int Ny, int Nz, double Lx, double Ly, double Lz, double xi, double half_quadW,
+                                   double *__restrict__ partial) {
+    const int Nzh = Nz / 2 + 1;
+    const long n = (long)Nx * Ny * Nzh;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        const int k = (int)(idx % Nzh);
+        const int j = (int)((idx / Nzh) % Ny);
+        const int i = (int)(idx / ((long)Nzh * Ny));
+        if (i == 0 && j == 0 && k == 0) continue;
+        const double kx = ((i < (Nx + 1) / 2) ? i : i - Nx) * 2.0 * kPi / Lx;
+        const double ky = ((j < (Ny + 1) / 2) ? j : j - Ny) * 2.0 * kPi / Ly;
+        const double kz = ((k < (Nz + 1) / 2) ? k : k - Nz) * 2.0 * kPi / Lz;
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        const double2 hk = spec[idx];
+        const double w = (k == 0 || (Nz % 2 == 0 && k == Nz / 2)) ? 1.0 : 2.0;
+        const double E = half_quadW * w * scale[idx] * (hk.x * hk.x + hk.y * hk.y);
+        const double kk = sqrt(k2);
+        const double sk = sin(kk), ck = cos(kk);
+        const double cot_term = fabs(sk) > 1e-300 ? 2.0 * kk * ck / sk : 0.0;  // E = 0 where sin k = 0
+        const double g = (cot_term - 4.0 - k2 / (2.0 * xi * xi)) / k2;
+        acc[0] += E * (1.0 + g * kx * kx);
+        acc[1] += E * g * kx * ky;
+        acc[2] += E * g * kx * kz;
+        acc[3] += E * (1.0 + g * ky * ky);
+        acc[4] += E * g * ky * kz;
+        acc[5] += E * (1.0 + g * kz * kz);
+        acc[6] += E;
+    }
+    __shared__ double red[8][7];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = 0; c < 7; ++c) {
+        double v = acc[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][c] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        double t = 0.0;
+        for (int v = 0; v < (int)(blockDim.x >> 5); ++v) t += red[v][threadIdx.x];
+        partial[(size_t)blockIdx.x * 7 + threadIdx.x] = t;
+    }
+}
+
 template <typename R> __global__ void cast_kernel(const double *__restrict__ in, R *__restrict__ out, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (R)in[i];
@@ -563,6 +616,37 @@ template <typename R> int wave_force(cr_handle *h, MeshBuffers<R> &m) {
         CR_LAUNCH(h, "contract_force_tiles_kernel");
         return CR_OK;
     }));
+    return CR_OK;
+}
+
+// Wave-space virial (FP64) of the charges already cast into m64.q: spread, forward
+// transform, then the per-mode sums of wave_virial_kernel; out[0..5] the tensor (xx, xy,
+// xz, yy, yz, zz), out[6] the wave energy.
+int wave_virial(cr_handle *h, double *out) {
+    MeshBuffers<double> &m = h->m64;
+    CR_TRY(spread_only(h, m));
+    CR_CUFFT(h, cufftSetStream(m.plan_fwd, h->stream));
+    CR_CUFFT(h, fft_forward(m.plan_fwd, m.grid, m.spec));
+    ++h->fft_execs;
+    constexpr int kBlocks = 296;  // 2 per SM; partials summed in block order on the host
+    std::vector<double> part((size_t)kBlocks * 7);
+    double *d_part = nullptr;
+    CR_TRY(dalloc(h, &d_part, part.size()));
+    wave_virial_kernel<<<kBlocks, 256, 0, h->stream>>>(reinterpret_cast<const double2 *>(m.spec), m.scale,
+                                                       h->d.grid[0], h->d.grid[1], h->d.grid[2], h->L[0], h->L[1],
+                                                       h->L[2], h->user.xi, 0.5 * h->d.quadW, d_part);
+    int st = check_cuda(h, cudaGetLastError(), "wave_virial_kernel");
+    if (st == CR_OK) {
+        ++h->launches;
+        st = check_cuda(h, cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                           h->stream), "wave virial partials");
+    }
+    if (st == CR_OK) st = check_cuda(h, cudaStreamSynchronize(h->stream), "wave virial");
+    dfree(&d_part);
+    if (st != CR_OK) return st;
+    for (int c = 0; c < 7; ++c) out[c] = 0.0;
+    for (int b = 0; b < kBlocks; ++b)
+        for (int c = 0; c < 7; ++c) out[c] += part[(size_t)b * 7 + c];
     return CR_OK;
 }
 

@@ -143,9 +143,9 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Wait for the barrier phase `parity` to complete; gives up after ~2^31 cycles (about a
-// second) and returns false.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// Wait for the barrier phase `parity` to complete; gives up after `limit` cycles (2^31 by
+// default, about a second) and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
     const uint32_t a = smem_u32(bar);
     const long long t0 = clock64();
     while (true) {
@@ -157,7 +157,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > (1ll << 31)) return false;
+        if (clock64() - t0 > limit) return false;
     }
 }
 
@@ -210,7 +210,7 @@ template <bool TRAIN>
 __global__ void __launch_bounds__(128, 1)
     mlp_kernel(int n, const uint16_t *__restrict__ X, const float *__restrict__ target, float inv_n,
                const float *__restrict__ params, float *__restrict__ y_out, float *__restrict__ grad,
-               float *__restrict__ stats, int *__restrict__ err) {
+               float *__restrict__ stats, int *__restrict__ err, long long wait_limit, int withhold_first) {
     extern __shared__ __align__(1024) uint8_t smem[];
     using Lay = typename std::conditional<TRAIN, TrainLayout, InferLayout>::type;
     constexpr uint32_t NCOL = TRAIN ? 512 : 256;  // one CTA per SM (shared memory)
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(128, 1)
     int done_tiles = 0;
 
     auto sync_wait = [&]() -> bool {
-        const bool ok = mbar_wait(bar, phase);
+        const bool ok = mbar_wait(bar, phase, wait_limit);
         phase ^= 1u;
         tc_after();
         return __syncthreads_or(!ok) == 0;
@@ -295,7 +295,10 @@ __global__ void __launch_bounds__(128, 1)
         }
         handoff();
         // ---- MMA1: Z1 = X W1^T ----
-        if (tid == 0) {
+        // (withhold_first: a test hook that issues neither these MMAs nor their commit on the
+        // CTA's first tile, so nothing arrives on the barrier and its bounded wait runs out
+        // with no tensor-core work in flight)
+        if (tid == 0 && !(withhold_first && tile == (int)blockIdx.x)) {
             tc_after();
             mma_chain(tm + TC_Z1, s_base + Lay::x, TM, s_base + Lay::w1, H, H, F / 16, false);
             mma_commit(bar);
@@ -468,6 +471,8 @@ struct cr_mlp {
     int n_sm = 148;
     float *d_param = nullptr, *d_grad = nullptr, *d_m = nullptr, *d_v = nullptr, *d_stats = nullptr;
     int *d_err = nullptr;
+    long long wait_limit = 1ll << 31;  // clock cycles of every bounded barrier wait
+    int withhold_first = 0;            // test hook: the next launch withholds its first MMAs
     long long adam_steps = 0;
     long long launches = 0;
     std::string last_error;
@@ -605,7 +610,9 @@ int cr_mlp_forward(cr_mlp *h, int n, const uint16_t *d_x, float *d_y, void *stre
     const int ntiles = (n + crmlp::TM - 1) / crmlp::TM;
     const int grid = std::min(ntiles, h->n_sm);
     crmlp::mlp_kernel<false><<<grid, 128, crmlp::InferLayout::bytes, s>>>(n, d_x, nullptr, 0.f, h->d_param, d_y,
-                                                                            nullptr, nullptr, h->d_err);
+                                                                            nullptr, nullptr, h->d_err,
+                                                                            h->wait_limit, h->withhold_first);
+    h->withhold_first = 0;
     ++h->launches;
     MLP_CUDA(h, cudaGetLastError());
     return check_err(h, s);
@@ -620,7 +627,9 @@ int cr_mlp_accumulate_grad(cr_mlp *h, int n, const uint16_t *d_x, const float *d
         const int ntiles = (n + crmlp::TM - 1) / crmlp::TM;
         const int grid = std::min(ntiles, h->n_sm);
         crmlp::mlp_kernel<true><<<grid, 128, crmlp::TrainLayout::bytes, s>>>(n, d_x, d_t, 1.f / n, h->d_param,
-                                                                               nullptr, h->d_grad, h->d_stats, h->d_err);
+                                                                               nullptr, h->d_grad, h->d_stats, h->d_err,
+                                                                               h->wait_limit, h->withhold_first);
+        h->withhold_first = 0;
         ++h->launches;
         MLP_CUDA(h, cudaGetLastError());
     }
@@ -644,6 +653,13 @@ int cr_mlp_adam(cr_mlp *h, double lr, double clip, void *stream) {
         (float)c2, (float)clip);
     ++h->launches;
     MLP_CUDA(h, cudaGetLastError());
+    return CR_OK;
+}
+
+int cr_mlp_set_wait(cr_mlp *h, long long max_cycles, int withhold_next) {
+    if (!h || max_cycles < 1000) return mlp_fail(h, CR_BAD_PARAM, "wait limit below 1000 cycles");
+    h->wait_limit = max_cycles;
+    h->withhold_first = withhold_next ? 1 : 0;
     return CR_OK;
 }
 

@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <type_traits>
+#include <vector>
 
 #include "cr_internal.cuh"
 
@@ -180,7 +181,8 @@ __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_
                                  const int *__restrict__ members, const double4 *__restrict__ pos,
                                  const float4 *__restrict__ pos32, RSBuild c, float3 L32, float3 Linv32, float rc2,
                                  float band, float low, unsigned *__restrict__ masks, int *__restrict__ nnz,
-                                 unsigned long long *__restrict__ bits) {
+                                 unsigned long long *__restrict__ bits, const double4 *__restrict__ centre,
+                                 const double4 *__restrict__ extent, float4 *__restrict__ pshift) {
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (p >= npairs) return;
@@ -226,6 +228,14 @@ __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_
     if (lane == 0) {
         nnz[p] = n * CS;  // stored slots: longest row times 32 lanes
         atomicAdd(bits, (unsigned long long)tot);
+        // offset of the cluster centres under the minimum image, and whether the bead
+        // offsets then need no further image: rc + 2 (e_I + e_J) < L/2 along every axis
+        const double4 cI = centre[I], cJ = centre[J], eI = extent[I], eJ = extent[J];
+        const bool direct = c.rc + 2.0 * (eI.x + eJ.x) < 0.5 * c.L[0] - 1e-3 &&
+                            c.rc + 2.0 * (eI.y + eJ.y) < 0.5 * c.L[1] - 1e-3 &&
+                            c.rc + 2.0 * (eI.z + eJ.z) < 0.5 * c.L[2] - 1e-3;
+        pshift[p] = make_float4((float)mimg(cJ.x - cI.x, c.L[0], c.Linv[0]), (float)mimg(cJ.y - cI.y, c.L[1], c.Linv[1]),
+                                (float)mimg(cJ.z - cI.z, c.L[2], c.Linv[2]), direct ? 1.f : 0.f);
     }
 }
 
@@ -375,6 +385,192 @@ __global__ void __launch_bounds__(W * 32, sizeof(R) == 4 ? 6 : 1) pair_spmv_kern
 
 constexpr int kSpmvWarps = 8;
 
+// Bead offsets from their cluster's centre in FP32 (minimum image; 0 for padding).
+__global__ void cluster_offsets_kernel(int n, const int *__restrict__ members, const double4 *__restrict__ pos,
+                                       const double4 *__restrict__ centre, RSBuild c, float4 *__restrict__ off) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = members[k];
+    float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (i >= 0) {
+        const double4 p = pos[i], cc = centre[k / CS];
+        o.x = (float)mimg(p.x - cc.x, c.L[0], c.Linv[0]);
+        o.y = (float)mimg(p.y - cc.y, c.L[1], c.Linv[1]);
+        o.z = (float)mimg(p.z - cc.z, c.L[2], c.Linv[2]);
+    }
+    off[k] = o;
+}
+
+// Tabulated kernel in FP32 from the shared-memory table: index floor((d - dr) Ntable /
+// (rc - dr)) clamped into the table, weight d/dr - index - 1 (ConductorRigid.cu:549-554).
+__device__ __forceinline__ float table_lerp32(const float2 *__restrict__ tab, float d2, int ntab, float scale,
+                                              float dr, float inv_dr) {
+    const float d = d2 * rsqrtf(d2);
+    int ind = (int)((d - dr) * scale);  // truncation = floor for d >= dr; FP32 rounding below dr gives 0
+    ind = min(max(ind, 0), ntab - 1);
+    const float lin = fmaf(d, inv_dr, -(float)(ind + 1));
+    const float2 e = tab[ind];
+    return fmaf(e.y - e.x, lin, e.x);
+}
+
+// The FP32 product y_I = sum_J B_IJ x_J with the kernel values evaluated on the fly
+// instead of streamed: the same cluster pairs, bit masks, lane/warp mapping and sum
+// order as pair_spmv_kernel, the table in shared memory.  Per pair the offset of the
+// cluster centres under the minimum image comes from the mask pass; when
+// rc + 2 (e_I + e_J) < L/2 along every axis (e the clusters' half extents) every
+// in-range bead pair's separation is the plain difference of the bead offsets (a bead
+// lies within e of its centre, so that difference is within rc + 2 (e_I + e_J) of zero
+// and no other image can be nearer), otherwise each separation gets its own minimum
+// image.
+template <int W>
+__global__ void __launch_bounds__(W * 32, 6) pair_otf32_kernel(const long long *__restrict__ head,
+                                                               const int *__restrict__ count,
+                                                               const int *__restrict__ pair_j,
+                                                               const int *__restrict__ members,
+                                                               const unsigned *__restrict__ masks,
+                                                               const float4 *__restrict__ boff,
+                                                               const float4 *__restrict__ pshift, RSBuild c,
+                                                               const float2 *__restrict__ tab, float scale,
+                                                               const float *__restrict__ qc,
+                                                               const float *__restrict__ q,
+                                                               const float *__restrict__ phik, double selfc,
+                                                               const double *__restrict__ phi_body,
+                                                               const uint32_t *__restrict__ body,
+                                                               double *__restrict__ out) {
+    extern __shared__ float2 stab[];
+    __shared__ float part[W][CS];
+    for (int k = threadIdx.x; k <= c.ntab; k += W * 32) stab[k] = tab[k];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int I = blockIdx.x;
+    const float4 oi = boff[I * CS + lane];
+    const long long h0 = head[I];
+    const int n = count[I];
+    const float dr = (float)c.dr, inv_dr = (float)c.inv_dr;
+    const float3 L32 = make_float3((float)c.L[0], (float)c.L[1], (float)c.L[2]);
+    const float3 Li32 = make_float3((float)c.Linv[0], (float)c.Linv[1], (float)c.Linv[2]);
+    __syncthreads();
+    float y = 0.f;
+    for (int k = w; k < n; k += W) {
+        const long long p = h0 + k;
+        const int J = pair_j[p];
+        const unsigned m = masks[p * CS + lane];
+        const float4 oj = boff[J * CS + lane];
+        const float qj = qc[J * CS + lane];
+        const float4 sh = pshift[p];
+        const bool direct = sh.w != 0.f;
+        const float ax = oi.x - sh.x, ay = oi.y - sh.y, az = oi.z - sh.z;
+        const unsigned steps = __reduce_max_sync(0xffffffffu, (unsigned)__popc(m));
+        unsigned mm = m;
+        if (direct) {
+            for (unsigned t = 0; t < steps; ++t) {
+                const bool has = mm != 0;
+                const int j = has ? __ffs(mm) - 1 : 0;
+                mm &= mm - 1;
+                const float bx = __shfl_sync(0xffffffffu, oj.x, j);
+                const float by = __shfl_sync(0xffffffffu, oj.y, j);
+                const float bz = __shfl_sync(0xffffffffu, oj.z, j);
+                const float qq = __shfl_sync(0xffffffffu, qj, j);
+                if (has) {
+                    const float dx = ax - bx, dy = ay - by, dz = az - bz;
+                    y = fmaf(table_lerp32(stab, dx * dx + dy * dy + dz * dz, c.ntab, scale, dr, inv_dr), qq, y);
+                }
+            }
+        } else {
+            for (unsigned t = 0; t < steps; ++t) {
+                const bool has = mm != 0;
+                const int j = has ? __ffs(mm) - 1 : 0;
+                mm &= mm - 1;
+                const float bx = __shfl_sync(0xffffffffu, oj.x, j);
+                const float by = __shfl_sync(0xffffffffu, oj.y, j);
+                const float bz = __shfl_sync(0xffffffffu, oj.z, j);
+                const float qq = __shfl_sync(0xffffffffu, qj, j);
+                if (has) {
+                    float dx = ax - bx, dy = ay - by, dz = az - bz;
+                    dx -= L32.x * rintf(dx * Li32.x);
+                    dy -= L32.y * rintf(dy * Li32.y);
+                    dz -= L32.z * rintf(dz * Li32.z);
+                    y = fmaf(table_lerp32(stab, dx * dx + dy * dy + dz * dz, c.ntab, scale, dr, inv_dr), qq, y);
+                }
+            }
+        }
+    }
+    part[w][lane] = y;
+    __syncthreads();
+    if (w == 0) {
+        float tot = 0.f;
+#pragma unroll
+        for (int v = 0; v < W; ++v) tot += part[v][lane];
+        const int bi = members[I * CS + lane];
+        if (bi >= 0) {
+            const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)tot;
+            out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+        }
+    }
+}
+
+// The FP64 product with the values evaluated on the fly: the arithmetic of
+// pair_values_kernel (FP64 minimum image, reciprocal square root by Newton steps, the
+// FP64 table lerp) and the sum order of pair_spmv_kernel, so the result equals the
+// streamed FP64 product bit for bit.
+template <int W>
+__global__ void __launch_bounds__(W * 32) pair_otf64_kernel(const long long *__restrict__ head,
+                                                            const int *__restrict__ count,
+                                                            const int *__restrict__ pair_j,
+                                                            const int *__restrict__ members,
+                                                            const unsigned *__restrict__ masks,
+                                                            const double4 *__restrict__ pos,
+                                                            const double2 *__restrict__ tab, RSBuild c,
+                                                            const double *__restrict__ qc,
+                                                            const double *__restrict__ q,
+                                                            const double *__restrict__ phik, double selfc,
+                                                            const double *__restrict__ phi_body,
+                                                            const uint32_t *__restrict__ body,
+                                                            double *__restrict__ out) {
+    __shared__ double part[W][CS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int I = blockIdx.x;
+    const int bi = members[I * CS + lane];
+    const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
+    const long long h0 = head[I];
+    const int n = count[I];
+    double y = 0.0;
+    for (int k = w; k < n; k += W) {
+        const long long p = h0 + k;
+        const int J = pair_j[p];
+        const unsigned m = masks[p * CS + lane];
+        const int bj = members[J * CS + lane];
+        const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
+        const double qjl = qc[J * CS + lane];
+        const unsigned steps = __reduce_max_sync(0xffffffffu, (unsigned)__popc(m));
+        unsigned mm = m;
+        for (unsigned t = 0; t < steps; ++t) {
+            const bool has = mm != 0;
+            const int j = has ? __ffs(mm) - 1 : 0;
+            mm &= mm - 1;
+            const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
+            const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
+            const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
+            const double qj = __shfl_sync(0xffffffffu, qjl, j);
+            if (has) {
+                const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
+                const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
+                const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                y += table_lerp64(tab, c, d2 * rsqrt64(d2)) * qj;
+            }
+        }
+    }
+    part[w][lane] = y;
+    __syncthreads();
+    if (w == 0 && bi >= 0) {
+        double tot = 0.0;
+#pragma unroll
+        for (int v = 0; v < W; ++v) tot += part[v][lane];
+        const double total = phik[bi] + selfc * q[bi] + tot;
+        out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+    }
+}
+
 // Real-space forces over the cluster pairs, on the fly in FP64: F_i += -T'(d) q_i q_j
 // r_ij / d (ConductorRigid.cu:637-654); every ordered pair (I, J) is in the list.  One
 // CTA per cluster I: warp w takes I's pairs w, w+W, ..., lane i accumulates bead i's
@@ -443,6 +639,76 @@ __global__ void __launch_bounds__(W * 32) pair_force_kernel(const long long *__r
     }
 }
 
+// Real-space virial -dU_real/de_ab = 1/2 sum_{i != j} r_ij,a F_ij,b with the pair force
+// F_ij = -T'(d) q_i q_j r_ij / d of pair_force_kernel (the same pairs, gradient table and
+// FP64 arithmetic).  One CTA per cluster I writes its six components (xx, xy, xz, yy,
+// yz, zz) to partial[I][6]; the host adds the clusters in order.
+template <int W>
+__global__ void __launch_bounds__(W * 32) pair_virial_kernel(const long long *__restrict__ head,
+                                                             const int *__restrict__ count,
+                                                             const int *__restrict__ pair_j,
+                                                             const int *__restrict__ members,
+                                                             const unsigned *__restrict__ masks,
+                                                             const double4 *__restrict__ pos,
+                                                             const double *__restrict__ q,
+                                                             const double2 *__restrict__ tab, RSBuild c,
+                                                             double *__restrict__ partial) {
+    __shared__ double red[W][6];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int I = blockIdx.x;
+    const int bi = members[I * CS + lane];
+    const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
+    const double qi = bi >= 0 ? q[bi] : 0.0;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    const long long h0 = head[I];
+    const int n = count[I];
+    for (int k = w; k < n; k += W) {
+        const long long p = h0 + k;
+        const int J = pair_j[p];
+        const unsigned m = masks[p * CS + lane];
+        const int bj = members[J * CS + lane];
+        const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
+        const double qjl = bj >= 0 ? q[bj] : 0.0;
+        const unsigned steps = __reduce_max_sync(0xffffffffu, (unsigned)__popc(m));
+        unsigned mm = m;
+        for (unsigned t = 0; t < steps; ++t) {
+            const bool has = mm != 0;
+            const int j = has ? __ffs(mm) - 1 : 0;
+            mm &= mm - 1;
+            const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
+            const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
+            const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
+            const double qj = __shfl_sync(0xffffffffu, qjl, j);
+            if (has) {
+                const double dx = mimg(pi.x - xj, c.L[0], c.Linv[0]);
+                const double dy = mimg(pi.y - yj, c.L[1], c.Linv[1]);
+                const double dz = mimg(pi.z - zj, c.L[2], c.Linv[2]);
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                const double inv_d = rsqrt64(d2);
+                const double a = -table_lerp64(tab, c, d2 * inv_d) * qi * qj * inv_d;
+                v[0] += a * dx * dx;
+                v[1] += a * dx * dy;
+                v[2] += a * dx * dz;
+                v[3] += a * dy * dy;
+                v[4] += a * dy * dz;
+                v[5] += a * dz * dz;
+            }
+        }
+    }
+    for (int e = 0; e < 6; ++e) {
+        double t = v[e];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (lane == 0) red[w][e] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double t = 0.0;
+#pragma unroll
+        for (int u = 0; u < W; ++u) t += red[u][threadIdx.x];
+        partial[(size_t)I * 6 + threadIdx.x] = 0.5 * t;
+    }
+}
+
 // force_i = wave force_i + q_i E0 + real-space force_i
 template <typename R>
 __global__ void force_combine_kernel(int N, const R *__restrict__ fk, const double *__restrict__ q, double Ex,
@@ -498,10 +764,19 @@ template <typename R> int realspace_reserve(cr_handle *h) {
 // Packed values of precision R for the current cluster pairs (once per solve).  A solve
 // that runs an FP32 operator also needs FP64 values (its true residuals), so in those
 // modes the first request builds both in one pass.
+// Shared memory of the FP32 table (value, next value) of the on-the-fly product; tables
+// beyond the default 48 KB of dynamic shared memory (rc > 6.1) keep the stored values.
+size_t onfly32_smem(const cr_handle *h) { return (size_t)(h->d.n_table + 1) * sizeof(float2); }
+
+template <typename R> bool onfly(const cr_handle *h) {
+    if (sizeof(R) == 4) return (h->rs_onfly & CR_REALSPACE_ONFLY32) && onfly32_smem(h) <= 48 * 1024;
+    return h->rs_onfly & CR_REALSPACE_ONFLY64;
+}
+
 template <typename R> int realspace_blocks(cr_handle *h) {
     RealSpace &r = h->rs;
-    if (valid_of<R>(r) || h->N == 0) return CR_OK;
-    if (h->user.precision != CR_FP64 && !r.valid32 && !r.valid64) {
+    if (valid_of<R>(r) || h->N == 0 || onfly<R>(h)) return CR_OK;
+    if (h->user.precision != CR_FP64 && !r.valid32 && !r.valid64 && !onfly<float>(h) && !onfly<double>(h)) {
         CR_TRY(realspace_reserve<float>(h));
         CR_TRY(realspace_reserve<double>(h));
         pair_values_kernel<float, double><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
@@ -546,6 +821,8 @@ void realspace_free(cr_handle *h) {
     dfree(&r.acc64);
     dfree(&r.freal);
     dfree(&r.bits);
+    dfree(&r.boff);
+    dfree(&r.pshift);
     r.pair_cap = 0;
     r.nnz = 0;
     r.blocks32_cap = r.blocks64_cap = 0;
@@ -569,6 +846,7 @@ int realspace_alloc(cr_handle *h) {
     CR_TRY(dalloc(h, &r.acc64, nc * CS));
     CR_TRY(dalloc(h, &r.freal, 3 * (size_t)std::max(h->N, 1)));
     CR_TRY(dalloc(h, &r.bits, 1));
+    CR_TRY(dalloc(h, &r.boff, nc * CS));
     return CR_OK;
 }
 
@@ -590,6 +868,8 @@ int realspace_build(cr_handle *h) {
     const int nb = blocks_for((long)r.nclus * 32, 256);
     cluster_kernel<<<nb, 256, 0, s>>>(N, r.nclus, r.sorted, h->m64.pos, c, r.members, r.centre, r.extent);
     CR_LAUNCH(h, "cluster_kernel");
+    cluster_offsets_kernel<<<nb, 256, 0, s>>>(r.nclus * CS, r.members, h->m64.pos, r.centre, c, r.boff);
+    CR_LAUNCH(h, "cluster_offsets_kernel");
     pair_search_kernel<false><<<nb, 256, 0, s>>>(r.nclus, r.centre, r.extent, c, r.count, nullptr, nullptr);
     CR_LAUNCH(h, "pair_search_kernel");
     bytes = h->sort_tmp_bytes;
@@ -607,6 +887,7 @@ int realspace_build(cr_handle *h) {
         CR_TRY(dalloc(h, &r.masks, (size_t)cap * CS));
         CR_TRY(dalloc(h, &r.nnz_pair, (size_t)cap));
         CR_TRY(dalloc(h, &r.voff, (size_t)cap));
+        CR_TRY(dalloc(h, &r.pshift, (size_t)cap));
         r.pair_cap = cap;
         // scan scratch for npairs entries
         size_t b = 0;
@@ -631,7 +912,8 @@ int realspace_build(cr_handle *h) {
                                             make_float3((float)h->L[0], (float)h->L[1], (float)h->L[2]),
                                             make_float3((float)(1.0 / h->L[0]), (float)(1.0 / h->L[1]),
                                                         (float)(1.0 / h->L[2])),
-                                            (float)c.rc2, band, low, r.masks, r.nnz_pair, r.bits);
+                                            (float)c.rc2, band, low, r.masks, r.nnz_pair, r.bits, r.centre,
+                                            r.extent, r.pshift);
     }
     CR_LAUNCH(h, "pair_mask_kernel");
     bytes = h->sort_tmp_bytes;
@@ -664,6 +946,21 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
                                                                                          m.q, qc);
     CR_LAUNCH(h, "gather_cluster_kernel");
     constexpr int W = kSpmvWarps;
+    if (onfly<R>(h)) {
+        if constexpr (sizeof(R) == 4) {
+            pair_otf32_kernel<W><<<r.nclus, W * 32, onfly32_smem(h), h->stream>>>(
+                r.head, r.count, r.pair_j, r.members, r.masks, r.boff, r.pshift, rs_build(h), h->m32.phiq,
+                (float)(h->d.n_table / (h->d.rcut - h->d.dr)), qc, m.q, m.phi, h->d.selfcoeff, phi_body, h->d_body,
+                out);
+            CR_LAUNCH(h, "pair_otf32_kernel");
+        } else {
+            pair_otf64_kernel<W><<<r.nclus, W * 32, 0, h->stream>>>(r.head, r.count, r.pair_j, r.members, r.masks,
+                                                                    h->m64.pos, h->m64.phiq, rs_build(h), qc, m.q,
+                                                                    m.phi, h->d.selfcoeff, phi_body, h->d_body, out);
+            CR_LAUNCH(h, "pair_otf64_kernel");
+        }
+        return CR_OK;
+    }
     pair_spmv_kernel<R, W, 16><<<r.nclus, W * 32, 0, h->stream>>>(
         r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, m.phi,
         h->d.selfcoeff, phi_body, h->d_body, out);
@@ -683,6 +980,29 @@ template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, cons
     force_combine_kernel<R><<<blocks_for(N, 256), 256, 0, h->stream>>>(N, m.force, q64, h->field[0], h->field[1],
                                                                        h->field[2], r.freal, force_out);
     CR_LAUNCH(h, "force_combine_kernel");
+    return CR_OK;
+}
+
+int real_space_virial(cr_handle *h, const double *q64, double *out) {
+    for (int e = 0; e < 6; ++e) out[e] = 0.0;
+    if (h->N == 0) return CR_OK;
+    RealSpace &r = h->rs;
+    std::vector<double> part((size_t)r.nclus * 6);
+    double *d_part = nullptr;
+    CR_TRY(dalloc(h, &d_part, part.size()));
+    pair_virial_kernel<kSpmvWarps><<<r.nclus, kSpmvWarps * 32, 0, h->stream>>>(
+        r.head, r.count, r.pair_j, r.members, r.masks, h->m64.pos, q64, h->m64.gradphiq, rs_build(h), d_part);
+    int st = check_cuda(h, cudaGetLastError(), "pair_virial_kernel");
+    if (st == CR_OK) {
+        ++h->launches;
+        st = check_cuda(h, cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                           h->stream), "real-space virial partials");
+    }
+    if (st == CR_OK) st = check_cuda(h, cudaStreamSynchronize(h->stream), "real-space virial");
+    dfree(&d_part);
+    if (st != CR_OK) return st;
+    for (int I = 0; I < r.nclus; ++I)
+        for (int e = 0; e < 6; ++e) out[e] += part[(size_t)I * 6 + e];
     return CR_OK;
 }
 

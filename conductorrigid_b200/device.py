@@ -65,6 +65,11 @@ class Handle:
     def set_graphs(self, enable: bool):
         self._check(_lib.lib().cr_set_graphs(self.h, int(bool(enable))), "cr_set_graphs")
 
+    def set_realspace(self, flags: int):
+        """CR_REALSPACE_ONFLY32 / CR_REALSPACE_ONFLY64: evaluate the real-space kernel values
+        of the FP32 / FP64 products on the fly instead of storing them per geometry."""
+        self._check(_lib.lib().cr_set_realspace(self.h, int(flags)), "cr_set_realspace")
+
     def graph_launches(self) -> int:
         v = C.c_longlong(0)
         self._check(_lib.lib().cr_graph_launches(self.h, C.byref(v)), "cr_graph_launches")
@@ -172,6 +177,19 @@ class Handle:
         u = C.c_double(0.0)
         self._check(_lib.lib().cr_energy(self.h, _ptr(q), C.byref(u)), "cr_energy")
         return u.value
+
+    def virial(self, q) -> dict:
+        """Virial tensors -dU/de of U = 1/2 q.(M q) at the current positions: real-space and
+        wave-space parts as 3x3 arrays, and the wave-space energy."""
+        q = self.dev(q)
+        v = (C.c_double * 13)()
+        self._check(_lib.lib().cr_virial(self.h, _ptr(q), v), "cr_virial")
+        a = np.array(v[:])
+
+        def tensor(c):
+            return np.array([[c[0], c[1], c[2]], [c[1], c[3], c[4]], [c[2], c[4], c[5]]])
+
+        return {"real": tensor(a[0:6]), "wave": tensor(a[6:12]), "wave_energy": float(a[12])}
 
     def neighbor_list(self, r_list: float):
         t = self.torch

@@ -93,6 +93,11 @@ class Network:
         self.adam(lr, clip)
         return loss
 
+    def set_wait(self, max_cycles: int = 1 << 31, withhold_next: bool = False):
+        """Cycle limit of the kernels' bounded barrier waits; withhold_next makes the next
+        launch withhold its first MMAs so that its waits run out (timeout-path test hook)."""
+        self._check(_lib.lib().cr_mlp_set_wait(self.h, int(max_cycles), int(bool(withhold_next))), "cr_mlp_set_wait")
+
     def counters(self) -> dict:
         a, b = C.c_longlong(0), C.c_longlong(0)
         self._check(_lib.lib().cr_mlp_counters(self.h, C.byref(a), C.byref(b)), "cr_mlp_counters")

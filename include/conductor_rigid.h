@@ -156,6 +156,17 @@ int cr_set_tiling(cr_handle *h, int tile_edge, int spread_mode);
 int cr_autotune(cr_handle *h, const double *d_pos, const double *d_body_pos, int reps, int *tile_edge,
                 int *spread_mode, float *best_ms);
 int cr_set_graphs(cr_handle *h, int enable);
+/* Real-space part of the operator (ConductorRigid.cu:469-567 evaluates the tabulated
+ * kernel per neighbour in every product).  Per geometry the in-range bead pairs are
+ * found once (32-bead clusters, per cluster pair a 32 x 32 bit mask); the kernel values
+ * T(d) of those pairs are then either stored once per geometry and streamed by every
+ * product, or evaluated again in every product from the positions (the table in shared
+ * memory in FP32).  flags: CR_REALSPACE_ONFLY32 evaluates the FP32 products on the fly,
+ * CR_REALSPACE_ONFLY64 the FP64 products (bit-identical to the stored FP64 values'
+ * product); 0 stores both.  Takes effect at the next product. */
+#define CR_REALSPACE_ONFLY32 1
+#define CR_REALSPACE_ONFLY64 2
+int cr_set_realspace(cr_handle *h, int flags);
 int cr_graph_launches(const cr_handle *h, long long *launches);
 
 /* ---- the step (gpu_ComputeForce, ConductorRigid.cu:1153-1286) ----
@@ -202,6 +213,18 @@ int cr_apply_M(cr_handle *h, const double *d_q, double *d_Mq, int precision);
  * last cr_set_positions / cr_compute (FP64).  Not computed by the reference, whose force
  * pass leaves the energy slot at zero (ConductorRigid.cu:464,661). */
 int cr_energy(cr_handle *h, const double *d_q, double *energy);
+/* Virial of the electrostatic energy U = 1/2 q.(M q) of bead charges d_q[N] at the
+ * positions of the last cr_set_positions / cr_compute (FP64): W_ab = -dU/de_ab under the
+ * affine strain r -> (1 + e) r of the bead positions and the box, with the charges and
+ * the unit shell radius fixed.  virial[13] (host): [0..5] the real-space tensor
+ * 1/2 sum_{i != j} r_ij,a F_ij,b over the real-space pair forces, [6..11] the
+ * wave-space tensor (per-mode energies of the spread mesh's spectrum with the strain
+ * derivative of the shell kernel j0(k)^2 exp(-k^2/4 xi^2)/k^2), [12] the wave-space
+ * energy; components in the order xx, xy, xz, yy, yz, zz.  The external field's term
+ * -q_i E0.(r_i - R_b) depends on intra-body vectors only and is not included.  Not
+ * computed by the reference, which leaves HOOMD's virial untouched
+ * (ConductorRigid.cu:464,661). */
+int cr_virial(cr_handle *h, const double *d_q, double *virial);
 /* Bead forces for charges q (force pass, ConductorRigid.cu:1256-1278). */
 int cr_forces(cr_handle *h, const double *d_q, double *d_force, int precision);
 /* Full neighbour list within r_list of the current positions (the pair set of the
@@ -286,6 +309,14 @@ int cr_mlp_forward(cr_mlp *net, int n, const uint16_t *d_x, float *d_y, void *st
 int cr_mlp_accumulate_grad(cr_mlp *net, int n, const uint16_t *d_x, const float *d_t, double *loss, void *stream);
 int cr_mlp_adam(cr_mlp *net, double lr, double clip, void *stream);
 int cr_mlp_counters(const cr_mlp *net, long long *kernel_launches, long long *adam_steps);
+/* Failure detection of the bounded waits.  max_cycles: the clock-cycle limit of every
+ * wait of the network's kernels on a tensor-core barrier (default 2^31, about a second
+ * at 2 GHz; at least 1000).  withhold_next != 0 makes the next forward or training
+ * launch issue neither the first tile's MMAs nor their commit in every CTA, so nothing
+ * arrives on the barrier: each CTA's wait runs out, the CTA frees its tensor memory and
+ * exits, and the call returns CR_TIMEOUT; the network stays usable (a test hook for the
+ * timeout path: nothing faults or hangs, no tensor-core work is left in flight). */
+int cr_mlp_set_wait(cr_mlp *net, long long max_cycles, int withhold_next);
 
 /* ---- learned guess for time stepping ----
  * No counterpart in the reference (its solve starts from the previous step's charges,
@@ -347,11 +378,15 @@ int cr_batch_compute(int n, cr_handle *const *handles, const double *const *d_po
  * d_grid[Nx*Ny*Nz] out (overwritten).  It allocates nothing: its scratch is one
  * file-scope device array of CR_NOALLOC_SCRATCH_BYTES that every GPU loading the
  * library holds until exit, located per device with cudaGetSymbolAddress on the first
- * call on that device (make that first call before any stream capture).  At most
- * CR_NOALLOC_MAX_BEADS beads, CR_NOALLOC_MAX_TILES 8^3-node mesh tiles and support 16;
- * larger inputs are rejected with CR_BAD_PARAM and a message in
- * cr_noalloc_last_error().  All calls share the array, so calls that overlap on the GPU
- * race and must be serialised by the caller.  Synchronises `stream` before returning. */
+ * call on that device (make that first call before any stream capture).  The address
+ * is kept for the life of the process: after cudaDeviceReset on a device, do not call
+ * this entry point on that device again.  At most CR_NOALLOC_MAX_BEADS beads,
+ * CR_NOALLOC_MAX_TILES 8^3-node mesh tiles and support 16; larger inputs are rejected
+ * with CR_BAD_PARAM and a message in cr_noalloc_last_error().  All calls share the
+ * array, so calls that overlap on the GPU race and must be serialised by the caller.
+ * Every call reads a position-check flag back to the host after its first kernel and
+ * waits for the end of its work on `stream` before returning, so each call blocks the
+ * calling thread until its spreading has finished. */
 #define CR_NOALLOC_MAX_BEADS 262144
 #define CR_NOALLOC_MAX_TILES 32768
 #define CR_NOALLOC_SCRATCH_BYTES 6291456

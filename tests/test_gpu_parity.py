@@ -274,3 +274,33 @@ def test_operator_matches_oracle_other_supports(cuda, product_lib, oracle_lib, s
     assert rel(h.apply_operator(x, product_lib.CR_FP32), orc.matvec(x)) < 2e-5
     assert rel(h.forces(q), orc.forces(q, s.field)) < 1e-11
     h.close()
+
+
+@pytest.mark.parametrize("flags", [0, 1, 2, 3])
+@pytest.mark.parametrize("case", ["plain_small", "small_box"])
+def test_realspace_modes_match_oracle(cuda, product_lib, oracle_lib, flags, case):
+    """Stored and on-the-fly real-space values give the oracle's operator; the FP64
+    on-the-fly product equals the stored one bit for bit.  The small box (rc = 0.45 L)
+    takes the per-separation minimum image of the on-the-fly FP32 product."""
+    import math
+
+    from conductorrigid_b200 import systems
+
+    w = systems.workload("plain_small", scale=1.0 if case == "plain_small" else 0.1)
+    s, p = w.system, w.params
+    rcut = p["rcut"] if case == "plain_small" else 0.45 * float(s.L[0])
+    xi = p["xi"] if case == "plain_small" else math.sqrt(-math.log(1e-5)) / rcut
+    grid = p["grid"] if case == "plain_small" else 32
+    base = dict(xi=xi, errortol=p["errortol"], grid=grid, support=p["support"], rcut=rcut)
+    h = make_handle(product_lib, s, base)
+    h.set_realspace(flags)
+    orc = oracle_lib.Oracle(s, xi, p["errortol"], grid, p["support"], rcut)
+    x = np.random.default_rng(17).standard_normal(s.n_beads + s.n_bodies)
+    ref = orc.matvec(x)
+    y64 = h.apply_operator(x)
+    assert rel(y64, ref) < 1e-11
+    assert rel(h.apply_operator(x, product_lib.CR_FP32), ref) < 2e-5
+    h.set_realspace(0)
+    y64s = h.apply_operator(x)
+    assert bool((y64 == y64s).all()), "FP64 on-the-fly and stored products differ"
+    h.close()
