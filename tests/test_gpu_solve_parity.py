@@ -13,7 +13,10 @@ Reference solutions:
   * the full 162k-charge headline system (1000 spheres x 162, 128^3, P = 11): the
     committed oracle solution tests/golden/solution_precision_162k.npz (residual
     1e-11 under the oracle's operator, re-checked here), with the forces recomputed by
-    the oracle's force pass at those charges (cu:1256-1278).
+    the oracle's force pass at those charges (cu:1256-1278);
+  * the full charged polydisperse mixture (1000 spheres a = 1 x 42 and 1000 a = 2 x 162
+    charges, Q = +-1, 256^3, P = 11): the committed oracle solution
+    tests/golden/solution_polydisperse_204k.npz, checked the same way.
 """
 from pathlib import Path
 
@@ -161,3 +164,29 @@ def test_headline_solve_full_size(headline, product_lib, cuda, precision):
     stream = cuda.cuda.Stream()
     q, phi, F, st = solve_gpu(product_lib, s, base, precision, "two_level", stream=stream)
     check(f"162k {precision} two_level", orc, s, ref, q, phi, F, st)
+
+
+@pytest.fixture(scope="module")
+def polydisperse(cuda, product_lib, oracle_lib):
+    """The full charged polydisperse mixture (204,000 charges, 256^3, P = 11) with the
+    committed oracle solution."""
+    from conductorrigid_b200 import systems
+
+    w = systems.workload("polydisperse_204k", seed=1)
+    s, p = w.system, w.params
+    base = {k: p[k] for k in ("xi", "errortol", "grid", "support", "rcut")}
+    g = np.load(GOLD / "solution_polydisperse_204k.npz")
+    orc = oracle_lib.Oracle(s, p["xi"], p["errortol"], p["grid"], p["support"], p["rcut"])
+    r = orc.residual(g["q"], g["phi"], s.field)
+    assert r < 2e-11, f"stored oracle solution has residual {r:.2e} under the oracle's operator"
+    ref = {"q": g["q"], "phi": g["phi"], "force": orc.forces(g["q"], s.field)}
+    return s, base, orc, ref
+
+
+@pytest.mark.parametrize("precond", ["conductor", "two_level"])
+def test_polydisperse_solve_full_size(polydisperse, product_lib, cuda, precond):
+    """Charged bodies (Q = +-1) of two sizes: the mixed solver at residual 1e-6."""
+    s, base, orc, ref = polydisperse
+    stream = cuda.cuda.Stream()
+    q, phi, F, st = solve_gpu(product_lib, s, base, "mixed", precond, stream=stream)
+    check(f"204k mixed {precond}", orc, s, ref, q, phi, F, st)
