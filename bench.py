@@ -227,10 +227,13 @@ def run_replicas(args) -> None:
 
 
 def run_dynamics(args) -> None:
-    """Rigid-body Brownian steps of the 420k-charge suspension: the plain solver warm-started
-    from the previous step against the learned start (network trained online on the first
-    half of the steps), both on one trajectory; per-step device time includes, for the
-    learned arm, the features, network inference and training."""
+    """Rigid-body Brownian steps of the 420k-charge suspension, three solvers on one
+    trajectory: the plain solver warm-started from the previous step (it moves the
+    bodies), the learned start (guess directions with the network trained online on the
+    first --train-solves solves), and the learned start plus the learned preconditioner
+    correction (its network trained online on the same solves, then used by every solve
+    whose initial-residual test it passes).  Per-step device time includes, for the learned
+    arms, the features, network inference and training."""
     import torch
 
     from conductorrigid_b200 import _lib, systems
@@ -243,28 +246,40 @@ def run_dynamics(args) -> None:
                   rcut=p["rcut"], gmres_tol=TOL, restart=RESTART, maxiter=20000, precision="mixed",
                   precond=args.precond)
     steps = args.warmup + args.steps
-    train = min(200, max(1, steps // 2))
-    out, guess = paired_run(_lib.make_params(**common), _lib.make_params(learned=True, **common), s,
-                            np.ones(s.n_bodies), steps, train_solves=train, seed=1,
-                            coarse=(args.coarse_max_dense, args.coarse_cg))
+    train = args.train_solves if args.train_solves > 0 else min(200, max(1, steps // 2))
+    out, guess, corr = paired_run(_lib.make_params(**common), _lib.make_params(learned=True, **common), s,
+                                  np.ones(s.n_bodies), steps, train_solves=train, seed=1,
+                                  coarse=(args.coarse_max_dense, args.coarse_cg), corrected=True)
     tail = out[max(train + 1, args.warmup):]
 
     def arm(name):
         ms = float(np.mean([o[name]["step_ms"] for o in tail]))
-        return {"iterations": round(float(np.mean([o[name]["iterations"] for o in tail])), 1),
-                "ms_per_step": round(ms, 2), "solves_per_s": round(1e3 / ms, 3),
-                "ns_per_day": round(1e3 / ms * 86400 * 1e-3, 1)}
+        d = {"iterations": round(float(np.mean([o[name]["iterations"] for o in tail])), 1),
+             "ms_per_step": round(ms, 2), "solves_per_s": round(1e3 / ms, 3),
+             "ns_per_day": round(1e3 / ms * 86400 * 1e-3, 1),
+             "converged": int(sum(o[name]["converged"] for o in tail))}
+        if name == "corrected":
+            d["solves_using_correction"] = int(sum(o[name]["used_learned_correction"] for o in tail))
+            red = [o[name]["correction_reduction"] for o in tail if o[name]["correction_reduction"][0] >= 0]
+            if red:
+                d["initial_step_reduction_plain_vs_corrected"] = [round(float(np.mean([r[0] for r in red])), 4),
+                                                                  round(float(np.mean([r[1] for r in red])), 4)]
+        return d
 
     line = {
-        "metric": "dynamics: GMRES iterations per step and solves/s, learned start vs plain warm start",
+        "metric": "dynamics: GMRES iterations per step and solves/s, learned start (+ learned preconditioner "
+                  "correction) vs plain warm start",
         "value": arm("learned")["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": len(tail),
         "warmup": len(out) - len(tail), "higher_is_better": True,
-        "learned": arm("learned"), "plain_warm_start": arm("plain"), "trained_solves": guess.trained,
+        "learned": arm("learned"), "corrected": arm("corrected"), "plain_warm_start": arm("plain"),
+        "trained_solves": guess.trained, "correction_trained_solves": corr.trained,
         "preconditioner": args.precond, "coarse_cg": args.coarse_cg,
         "heldout_explained": round(float(np.mean(guess.heldout[-len(tail):])) if guess.heldout else 0.0, 3),
-        "dtype": "f32 operator, f64 Krylov; bf16 network", "data": "synthetic (seeded placement, relaxed)",
+        "correction_heldout_explained": round(float(np.mean(corr.heldout[-20:])) if corr.heldout else 0.0, 3),
+        "dtype": "f32 operator, f64 Krylov; bf16 networks", "data": "synthetic (seeded placement, relaxed)",
         "config": {"workload": f"dynamics_420k scale {args.scale}: {s.n_bodies} spheres x 42, phi 0.35, "
-                               f"mesh {grid}^3, P=9, dt 1e-3, kT 1, steric repulsion k=1000 gap 0.1",
+                               f"mesh {grid}^3, P=9, dt 1e-3, kT 1, steric repulsion k=1000 gap 0.1, "
+                               f"{steps} steps, networks trained on the first {train} solves",
                    "ns_per_day_unit": "reduced time units per day (dt = 1e-3)"},
     }
     print(json.dumps(line), flush=True)
@@ -836,6 +851,8 @@ def main() -> None:
                     help="coarse problems above this many unknowns use the sparse form (--coarse-cg steps of CG on "
                          "near-pair blocks + the low-rank wave term) or, with --coarse-cg 0, no coarse level")
     ap.add_argument("--coarse-cg", type=int, default=0, help="CG steps of the sparse coarse form")
+    ap.add_argument("--train-solves", type=int, default=0,
+                    help="dynamics: solves the networks are trained on (default min(200, steps/2))")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.precond is None:

@@ -98,10 +98,16 @@ class CrSolveStats(C.Structure):
         ("final_residual", C.c_double),
         ("solve_ms", C.c_double),
         ("learned_residual", C.c_double),
+        ("used_learned_correction", C.c_int),
+        ("correction_reduction", C.c_double * 2),
     ]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
 
 
 class CrGeometryInfo(C.Structure):
@@ -147,6 +153,8 @@ _SIGS = {
     "cr_set_stream": ([_P, _P], _I),
     "cr_set_graphs": ([_P, _I], _I),
     "cr_set_realspace": ([_P, _I], _I),
+    "cr_set_correction": ([_P, _P, C.c_double], _I),
+    "cr_correction_samples": ([_P, _I, _P, _P, C.POINTER(C.c_int)], _I),
     "cr_set_tiling": ([_P, _I, _I], _I),
     "cr_autotune": ([_P, _P, _P, _I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)], _I),
     "cr_graph_launches": ([_P, C.POINTER(C.c_longlong)], _I),

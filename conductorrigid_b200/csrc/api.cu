@@ -59,6 +59,7 @@ void prof_end(cr_handle *h, long token) {
 namespace {
 
 void free_all(cr_handle *h) {
+    correction_free(h);
     conductor_free(h);
     coarse_free(h);
     mesh_free(h->m64);
@@ -335,6 +336,26 @@ int cr_set_graphs(cr_handle *h, int enable) {
     if (!h) return CR_BAD_PARAM;
     h->use_graphs = enable ? 1 : 0;
     return CR_OK;
+}
+
+int cr_set_correction(cr_handle *h, cr_mlp *net, double weight) {
+    if (!h) return CR_BAD_PARAM;
+    if (!std::isfinite(weight)) return fail(h, CR_BAD_PARAM, "non-finite correction weight");
+    if (h->stream) CR_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->corr.net = net;
+    h->corr.weight = weight;
+    h->corr.active = 0;
+    return CR_OK;
+}
+
+int cr_correction_samples(cr_handle *h, int max_dirs, uint16_t *d_x, float *d_t, int *rows) {
+    if (!h || !rows || max_dirs < 0) return CR_BAD_PARAM;
+    *rows = 0;
+    if (!h->corr.net) return fail(h, CR_NOT_READY, "no correction network set");
+    if (!h->geo.valid) return fail(h, CR_NOT_READY, "no solve on this handle yet");
+    if (max_dirs > 0 && (!d_x || !d_t)) return fail(h, CR_BAD_PARAM, "null output");
+    if ((uintptr_t)d_x % 16) return fail(h, CR_BAD_PARAM, "feature rows must be 16-byte aligned");
+    return correction_samples(h, max_dirs, d_x, d_t, rows);
 }
 
 int cr_set_realspace(cr_handle *h, int flags) {

@@ -105,6 +105,22 @@ struct RealSpace {
                                     // bead separations need no further image
 };
 
+// Learned correction of the preconditioner (correction.cu).
+struct Correction {
+    cr_mlp *net = nullptr;              // the caller's network (not owned); null: no correction
+    double weight = 1.0;
+    int active = 0;                     // used by the current solve (decided per solve)
+    double last_rho[2] = {-1.0, -1.0};  // one-step residual reduction without / with it
+    uint16_t *x = nullptr;              // [N][48] BF16 feature rows
+    float *y = nullptr;                 // [N] network output
+    int *nbr = nullptr;                 // [B][8] nearest bodies
+    double4 *mom = nullptr;             // [B] mean and induced dipole of the preconditioned vector
+    double *ss = nullptr;               // [2] squared norms of z and v
+    double *zp = nullptr, *zc = nullptr;  // [N+B] scratch
+    int cap_n = -1, cap_b = -1;
+    long long nbr_gen = -1;
+};
+
 // GMRES workspace (FP64).
 struct Krylov {
     int n = 0, m = 0;
@@ -121,6 +137,7 @@ struct Krylov {
     double *yvec = nullptr;     // [m] least-squares coefficients
     double *h_pinned = nullptr; // pinned host mirror of hcol
     int nblocks = 0;
+    int last_cols = 0;          // Z columns filled by the last cycle
     // captured Arnoldi step (CUDA graph): device-side Hessenberg bookkeeping
     double *H = nullptr;        // [(m+1) * m] row-major Hessenberg, rotated in place
     double *cs = nullptr, *sn = nullptr;  // [m] Givens rotations
@@ -131,6 +148,7 @@ struct Krylov {
     double *h_hg = nullptr;     // pinned [(m+1)*m + (m+1)]: H and g at the end of a cycle
     cudaGraphExec_t exec[2] = {nullptr, nullptr};  // per operator precision (FP64, FP32)
     long long exec_gen[2] = {-1, -1};              // geometry generation captured
+    int exec_corr[2] = {0, 0};                     // learned correction inside the captured step
     long long exec_kernels[2] = {0, 0}, exec_ffts[2] = {0, 0};  // work per launch
 };
 
@@ -259,6 +277,7 @@ struct cr_handle {
     cr::Geometry geo;
     cr::RealSpace rs;
     cr::Krylov kry;
+    cr::Correction corr;
 
     // scratch
     double *d_tmp_n = nullptr;        // [N+B]
@@ -393,6 +412,15 @@ void coarse_free(cr_handle *h);
 int apply_operator(cr_handle *h, const double *x, double *y, int precision);
 // Solve A x = b (x holds the warm start).
 int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st);
+// learned correction of the preconditioner (correction.cu)
+int correction_prepare(cr_handle *h);
+void correction_free(cr_handle *h);
+int correction_add(cr_handle *h, const double *v, double *z);
+int precondition_step(cr_handle *h, const double *v, double *z);
+int correction_decide(cr_handle *h, int precision, const double *r, double *w);
+int correction_samples(cr_handle *h, int max_dirs, uint16_t *d_x, float *d_t, int *rows);
+// out[0..k) = V[0..k)^T w over the N + B unknowns (device result)
+int dots(cr_handle *h, int k, const double *V, const double *w, double *out);
 int body_force_torque(cr_handle *h, const double *pos, const double *bpos, const double *force, double *bf,
                       double *bt);
 int brownian_step(cr_handle *h, const cr_brownian_params *bp, long long step, const double *radius,

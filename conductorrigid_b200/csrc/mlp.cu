@@ -523,6 +523,28 @@ int check_err(cr_mlp *h, cudaStream_t s) {
 
 }  // namespace
 
+namespace cr {
+
+// Inference without the host-side error check (for use inside a solve, also while a
+// stream is being captured): the kernel records a wait that ran out in the network's
+// error flag, which mlp_check reads later.
+int mlp_forward_async(cr_mlp *h, int n, const uint16_t *d_x, float *d_y, cudaStream_t s) {
+    if (!h || n <= 0) return CR_OK;
+    const int ntiles = (n + crmlp::TM - 1) / crmlp::TM;
+    const int grid = std::min(ntiles, h->n_sm);
+    crmlp::mlp_kernel<false><<<grid, 128, crmlp::InferLayout::bytes, s>>>(n, d_x, nullptr, 0.f, h->d_param, d_y,
+                                                                            nullptr, nullptr, h->d_err,
+                                                                            h->wait_limit, 0);
+    ++h->launches;
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CR_OK : CR_CUDA_ERROR;
+}
+
+// CR_TIMEOUT if a wait of an earlier asynchronous launch ran out (clears the flag).
+int mlp_check(cr_mlp *h, cudaStream_t s) { return check_err(h, s); }
+
+}  // namespace cr
+
 extern "C" {
 
 int cr_mlp_create(uint64_t seed, cr_mlp **out) {

@@ -259,7 +259,9 @@ __global__ void phi_refit_kernel(int N, int B, const int *__restrict__ start, co
 
 int vec_blocks(int n) { return std::max(1, std::min(4 * 148, blocks_for(n, 256))); }
 
-// hcol[0..k) = V[0..k)^T w   (device result)
+}  // namespace
+
+// out[0..k) = V[0..k)^T w over the n = N + B unknowns (device result, fixed sum order)
 int dots(cr_handle *h, int k, const double *V, const double *w, double *out) {
     ProfScope ps(h, PROF_KRYLOV);
     Krylov &K = h->kry;
@@ -269,6 +271,8 @@ int dots(cr_handle *h, int k, const double *V, const double *w, double *out) {
     CR_LAUNCH(h, "reduce_partials_kernel");
     return CR_OK;
 }
+
+namespace {
 
 int norm(cr_handle *h, const double *v, double *result) {
     Krylov &K = h->kry;
@@ -300,7 +304,7 @@ int record_step(cr_handle *h, int precision) {
     OpCount none;
     gather_col_kernel<<<nb, 256, 0, s>>>(n, K.V, st, K.sin);
     CR_LAUNCH(h, "gather_col_kernel");
-    CR_TRY(precondition(h, K.sin, K.sz));
+    CR_TRY(precondition_step(h, K.sin, K.sz));
     scatter_col_kernel<<<nb, 256, 0, s>>>(n, m, K.sz, st, K.Z);
     CR_LAUNCH(h, "scatter_col_kernel");
     CR_TRY(op_apply(h, precision, K.sz, K.w, none));
@@ -329,8 +333,9 @@ int record_step(cr_handle *h, int precision) {
 int capture_step(cr_handle *h, int precision) {
     Krylov &K = h->kry;
     const int slot = precision == CR_FP64 ? 0 : 1;
-    if (K.exec[slot] && K.exec_gen[slot] == h->geo_gen) return CR_OK;
+    if (K.exec[slot] && K.exec_gen[slot] == h->geo_gen && K.exec_corr[slot] == h->corr.active) return CR_OK;
     CR_TRY(realspace_prepare(h, precision));  // allocations and one-off work stay outside the graph
+    if (h->corr.active) CR_TRY(correction_prepare(h));
     const long long l0 = h->launches, f0 = h->fft_execs;
     CR_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     const int st = record_step(h, precision);
@@ -364,6 +369,7 @@ int capture_step(cr_handle *h, int precision) {
     }
     cudaGraphDestroy(graph);
     K.exec_gen[slot] = h->geo_gen;
+    K.exec_corr[slot] = h->corr.active;
     return CR_OK;
 }
 
@@ -443,7 +449,7 @@ int fgmres(cr_handle *h, int precision, double *x, const double *b, int r_mode, 
         for (; j < m && it < maxit && !stop; ++j) {
             double *vj = K.V + (size_t)j * n;
             double *zj = K.Z + (size_t)j * n;
-            CR_TRY(precondition(h, vj, zj));
+            CR_TRY(precondition_step(h, vj, zj));
             CR_TRY(op_apply(h, precision, zj, K.w, oc));
             // classical Gram-Schmidt, twice
             CR_TRY(dots(h, j + 1, K.V, K.w, K.hcol));
@@ -490,6 +496,7 @@ int fgmres(cr_handle *h, int precision, double *x, const double *b, int r_mode, 
         CR_CUDA(h, cudaMemcpyAsync(K.yvec, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         update_kernel<<<nb, 256, 0, h->stream>>>(n, j, K.Z, K.yvec, x);
         CR_LAUNCH(h, "update_kernel");
+        K.last_cols = j;
         ++*restarts;
         if (single_cycle) {
             // the caller recomputes the residual in higher precision
@@ -682,6 +689,15 @@ int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {
         s.learned_residual = bnorm > 0 ? rnorm / bnorm : rnorm;
         // the guess counts as used when it lowered the initial residual
         s.used_learned_guess = s.learned_residual < 0.999 * s.initial_residual ? 1 : 0;
+    }
+    // learned correction of the preconditioner: used in this solve only if it reduces the
+    // initial residual more than the plain preconditioner in one step
+    h->corr.active = 0;
+    if (h->corr.net) {
+        CR_TRY(correction_decide(h, h->user.precision == CR_FP64 ? CR_FP64 : CR_FP32, K.r, K.w));
+        s.used_learned_correction = h->corr.active;
+        s.correction_reduction[0] = h->corr.last_rho[0];
+        s.correction_reduction[1] = h->corr.last_rho[1];
     }
     int status = CR_OK;
     if (h->user.precision != CR_MIXED) {

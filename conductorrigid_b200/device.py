@@ -70,6 +70,19 @@ class Handle:
         of the FP32 / FP64 products on the fly instead of storing them per geometry."""
         self._check(_lib.lib().cr_set_realspace(self.h, int(flags)), "cr_set_realspace")
 
+    def set_correction(self, net, weight: float = 1.0):
+        """Learned preconditioner correction from `net` (a learned.Network; None removes it)."""
+        self._check(_lib.lib().cr_set_correction(self.h, net.h if net is not None else None, C.c_double(weight)),
+                    "cr_set_correction")
+
+    def correction_samples(self, max_dirs: int, x, t) -> int:
+        """Training rows of the correction from the last solve into x [rows, 48] (int16 BF16
+        bits) and t [rows] (float32); returns the number of rows written."""
+        rows = C.c_int(0)
+        self._check(_lib.lib().cr_correction_samples(self.h, int(max_dirs), _ptr(x), _ptr(t), C.byref(rows)),
+                    "cr_correction_samples")
+        return rows.value
+
     def graph_launches(self) -> int:
         v = C.c_longlong(0)
         self._check(_lib.lib().cr_graph_launches(self.h, C.byref(v)), "cr_graph_launches")

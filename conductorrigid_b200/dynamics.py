@@ -144,6 +144,52 @@ class LearnedGuess:
         return loss
 
 
+class LearnedCorrection:
+    """The learned correction of the preconditioner on one handle, trained online.
+
+    After each of the first `train_solves` solves the handle writes training rows from
+    that solve's stored Krylov directions (cr_correction_samples: the features of
+    (A z_j, P A z_j) and the targets (z_j - P A z_j) / s), the network is scored on them
+    before it sees them (held-out explained fraction) and then trained on them; once
+    trained it is switched on with `weight`.  Each solve still decides for itself whether
+    to use it (its one-step reduction of the initial residual must beat the plain
+    preconditioner's)."""
+
+    def __init__(self, handle, *, train_solves=200, dirs=4, passes=2, lr=1e-3, weight=1.0, seed=2):
+        import torch
+
+        self.torch = torch
+        self.h = handle
+        self.net = Network(seed=seed)
+        self.train_solves = train_solves
+        self.dirs, self.passes, self.lr, self.weight = dirs, passes, lr, weight
+        self.x = torch.empty(dirs * handle.N, FEATURES, dtype=torch.int16, device="cuda")
+        self.t = torch.empty(dirs * handle.N, dtype=torch.float32, device="cuda")
+        self.trained = 0
+        self.losses, self.heldout = [], []
+        handle.set_correction(self.net, 0.0)  # weight 0: rows can be drawn, nothing is applied yet
+
+    def learn(self):
+        if self.trained >= self.train_solves:
+            return None
+        rows = self.h.correction_samples(self.dirs, self.x, self.t)
+        if rows == 0:
+            return None
+        x, t = self.x[:rows], self.t[:rows]
+        power = float(t.double().pow(2).mean().item())
+        if self.trained > 0 and power > 0:
+            y = self.net.forward(x).double()
+            self.heldout.append(1.0 - float((y - t.double()).pow(2).mean().item()) / power)
+        loss = None
+        for _ in range(self.passes):
+            loss = self.net.train_step(x, t, lr=self.lr)
+        self.losses.append(loss)
+        self.trained += 1
+        if self.trained >= self.train_solves:
+            self.h.set_correction(self.net, self.weight)
+        return loss
+
+
 def relax(handle, pos, bpos, radius, steps, *, repulsion=1000.0, contact_gap=0.1, dt=1e-3, kT=1.0, viscosity=1.0,
           seed=1):
     """Brownian steps under the steric repulsion alone (no solves): opens the near-contact
@@ -202,59 +248,75 @@ class BrownianRun:
 
 def paired_run(params_plain, params_learned, system, radius, steps, *, train_solves=None, seed=1, dt=1e-3,
                use_network=True, use_transport=True, passes=4, lr=1e-3, repulsion=1000.0, contact_gap=0.1,
-               relax_steps=300, mode="lsq", coarse=None):
-    """Two solvers on ONE trajectory: the plain solver (warm start from its own previous
+               relax_steps=300, mode="lsq", coarse=None, corrected=False, correction_weight=1.0):
+    """Solvers on ONE trajectory: the plain solver (warm start from its own previous
     solution) moves the bodies; the learned solver solves the same configurations from its
-    own previous solution plus the guess directions.  Returns per-step stats of both.
-    ``coarse`` = (max_dense, cg_steps) sets both handles' two-level coarse level."""
+    own previous solution plus the guess directions; with ``corrected`` a third solver does
+    the same as the learned one and also applies the learned preconditioner correction
+    (trained online on its own solves during the first ``train_solves``).  Returns per-step
+    stats of every arm, the learned guess and the correction (or None).
+    ``coarse`` = (max_dense, cg_steps) sets every handle's two-level coarse level."""
     import torch
 
     from .device import Handle
 
     stream = torch.cuda.Stream()  # a stream of their own: the solvers capture their Arnoldi steps
-    hp = Handle(params_plain, system.L, stream=stream)
-    hp.set_topology(system.body, system.rigid, system.body_charge)
-    hl = Handle(params_learned, system.L, stream=stream)
-    hl.set_topology(system.body, system.rigid, system.body_charge)
-    if coarse is not None:
-        for h in (hp, hl):
+    handles = [Handle(params_plain, system.L, stream=stream), Handle(params_learned, system.L, stream=stream)]
+    if corrected:
+        handles.append(Handle(params_learned, system.L, stream=stream))
+    for h in handles:
+        h.set_topology(system.body, system.rigid, system.body_charge)
+        if coarse is not None:
             h.set_coarse(*coarse)
     with torch.cuda.stream(stream):
-        return _paired_loop(hp, hl, system, radius, steps, train_solves, seed, dt, use_network, use_transport,
-                            passes, lr, repulsion, contact_gap, relax_steps, mode)
+        return _paired_loop(handles, system, radius, steps, train_solves, seed, dt, use_network, use_transport,
+                            passes, lr, repulsion, contact_gap, relax_steps, mode, correction_weight)
 
 
-def _paired_loop(hp, hl, system, radius, steps, train_solves, seed, dt, use_network, use_transport, passes, lr,
-                 repulsion, contact_gap, relax_steps, mode):
+def _paired_loop(handles, system, radius, steps, train_solves, seed, dt, use_network, use_transport, passes, lr,
+                 repulsion, contact_gap, relax_steps, mode, correction_weight):
     import torch
 
+    hp, hl = handles[0], handles[1]
+    hc = handles[2] if len(handles) > 2 else None
+    n_train = train_solves if train_solves is not None else steps
     run = BrownianRun(hp, system, radius, dt=dt, seed=seed, repulsion=repulsion, contact_gap=contact_gap,
                       relax_steps=relax_steps)
-    guess = LearnedGuess(hl, radius, train_solves=train_solves if train_solves is not None else steps,
-                         use_network=use_network, use_transport=use_transport, passes=passes, lr=lr, seed=seed)
-    ql = torch.zeros(hl.N, dtype=torch.float64, device="cuda")
-    pl = torch.zeros(hl.B, dtype=torch.float64, device="cuda")
+    arms = [("learned", hl, LearnedGuess(hl, radius, train_solves=n_train, use_network=use_network,
+                                         use_transport=use_transport, passes=passes, lr=lr, seed=seed))]
+    corr = None
+    if hc is not None:
+        arms.append(("corrected", hc, LearnedGuess(hc, radius, train_solves=n_train, use_network=use_network,
+                                                   use_transport=use_transport, passes=passes, lr=lr, seed=seed)))
+        corr = LearnedCorrection(hc, train_solves=n_train, lr=lr, weight=correction_weight, seed=seed + 1)
+    state = {name: [torch.zeros(h.N, dtype=torch.float64, device="cuda"),
+                    torch.zeros(h.B, dtype=torch.float64, device="cuda"), None] for name, h, _ in arms}
     out = []
-    prev = None
     for k in range(steps):
         pos, bpos = run.pos.clone(), run.bpos.clone()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        if prev is not None:
-            nd = guess.prepare(prev[2], prev[0], prev[1], pos, bpos, None if mode == "add" else prev[3])
-            if mode == "add":
-                # unit-weight corrections on top of the warm start
-                for j in range(nd):
-                    ql += guess.dirs[j, :hl.N]
-                _lib.lib().cr_set_guess_directions(hl.h, 0, None)
-        _, stl = hl.compute(pos, bpos, ql, pl)
-        stl["train_loss"] = guess.learn(ql)
-        e1.record()
-        e1.synchronize()
-        stl["step_ms"] = e0.elapsed_time(e1)
-        prev = (pos, bpos, ql.clone(), pl.clone())
-        stp = run.step()
-        out.append({"plain": stp, "learned": stl})
-    hp.close()
-    hl.close()
-    return out, guess
+        rec = {}
+        for name, h, guess in arms:
+            q, ph, prev = state[name]
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if prev is not None:
+                nd = guess.prepare(prev[2], prev[0], prev[1], pos, bpos, None if mode == "add" else prev[3])
+                if mode == "add":
+                    # unit-weight corrections on top of the warm start
+                    for j in range(nd):
+                        q += guess.dirs[j, :h.N]
+                    _lib.lib().cr_set_guess_directions(h.h, 0, None)
+            _, st = h.compute(pos, bpos, q, ph)
+            st["train_loss"] = guess.learn(q)
+            if name == "corrected":
+                st["correction_loss"] = corr.learn()
+            e1.record()
+            e1.synchronize()
+            st["step_ms"] = e0.elapsed_time(e1)
+            state[name][2] = (pos, bpos, q.clone(), ph.clone())
+            rec[name] = st
+        rec["plain"] = run.step()
+        out.append(rec)
+    for h in handles:
+        h.close()
+    return out, arms[0][2], corr

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define CR_ABI_VERSION 3
+#define CR_ABI_VERSION 4
 
 typedef enum {
     CR_OK = 0,
@@ -106,6 +106,9 @@ typedef struct {
     double solve_ms;          /* device time of the solve (CUDA events) */
     double learned_residual;  /* with learned = 1: relative residual of the start after the
                                  guess directions and the potential refit */
+    int used_learned_correction;     /* 1 when the learned preconditioner correction was used */
+    double correction_reduction[2];  /* one-step residual reduction of the initial residual
+                                        without / with the correction (-1: not tried) */
 } cr_solve_stats;
 
 typedef struct cr_handle cr_handle;
@@ -354,6 +357,29 @@ int cr_feature_pack(cr_handle *h, int n, const float *d_feat, const float *d_mu,
                     uint16_t *d_x);
 int cr_guess_target(cr_handle *h, const double *d_q, const double *d_q_prev, double scale, float *d_t);
 int cr_neutral_direction(cr_handle *h, const void *d_v, int v_is_fp32, double scale, double *d_dir);
+
+/* ---- the learned correction of the preconditioner ----
+ * No counterpart in the reference, whose GMRES applies the fixed diagonal scaling of
+ * Precondition (ConductorRigid.cu:1023-1044) to every Krylov vector.  With a network set,
+ * every flexible-GMRES step of a solve preconditions its Krylov vector v with
+ * z' = P v + weight * s * y, P the handle's preconditioner, s the RMS of P v and y the
+ * network's per-bead output for 48 features of (v, P v) (the vectors at unit RMS, the own
+ * body's mean and induced dipole of P v, the field direction, and for the 8 nearest bodies
+ * their direction, proximity, mean of P v and the potential of their induced dipole).
+ * Before a solve uses it, the correction is tried on the solve's initial residual r: it
+ * is used only if min_a ||r - a A P' r|| < min_a ||r - a A P r|| (P' with the
+ * correction), otherwise the solve falls back to the plain preconditioner;
+ * cr_solve_stats reports the choice and both reductions.  The network is the caller's
+ * (cr_mlp_create); net = NULL removes it, weight = 0 keeps it set without applying it.
+ * Flexible GMRES keeps the fixed point and the true-residual stopping test whatever the
+ * network outputs.
+ * cr_correction_samples writes training rows from the last solve on this handle: for up
+ * to max_dirs stored preconditioned Krylov directions z_j of its last cycle, the features
+ * of (w, P w), w = A z_j (FP64), into d_x [rows][48] (BF16, 16-byte aligned) and the
+ * targets (z_j - P w) / s into d_t [rows]; *rows = directions used x N.  Train the network
+ * on them with cr_mlp_accumulate_grad / cr_mlp_adam. */
+int cr_set_correction(cr_handle *h, cr_mlp *net, double weight);
+int cr_correction_samples(cr_handle *h, int max_dirs, uint16_t *d_x, float *d_t, int *rows);
 
 /* ---- batched independent systems ----
  * No counterpart in the reference (one system per force compute).  Solves n independent

@@ -142,8 +142,8 @@ def test_learned_guess_in_time_stepping(cuda, product_lib):
 
     s = systems_small(0.10)
     steps, train = 24, 12
-    out, guess = paired_run(_params(s), _params(s, learned=True), s, np.ones(s.n_bodies), steps,
-                            train_solves=train, seed=7)
+    out, guess, _ = paired_run(_params(s), _params(s, learned=True), s, np.ones(s.n_bodies), steps,
+                               train_solves=train, seed=7)
     for k, o in enumerate(out):
         print(f"step {k:3d} plain it {o['plain']['iterations']:4d} r0 {o['plain']['initial_residual']:.2e} | "
               f"learned it {o['learned']['iterations']:4d} r0 {o['learned']['initial_residual']:.2e} "
@@ -165,3 +165,60 @@ def systems_small(phi):
     from conductorrigid_b200 import systems
 
     return systems.spheres(np.ones(150), 1, phi, (0.0, 0.0, 1.0), seed=5)
+
+
+def test_learned_correction_in_time_stepping(cuda, product_lib):
+    """The third arm: learned start plus the learned preconditioner correction, trained
+    online.  Every solve converges; a solve that used the correction had passed its
+    initial-residual test (one-step reduction below the plain preconditioner's)."""
+    from conductorrigid_b200.dynamics import paired_run
+
+    s = systems_small(0.20)
+    steps, train = 16, 8
+    out, guess, corr = paired_run(_params(s), _params(s, learned=True), s, np.ones(s.n_bodies), steps,
+                                  train_solves=train, seed=3, corrected=True)
+    assert corr.trained == train and len(corr.losses) == train
+    for k, o in enumerate(out):
+        c = o["corrected"]
+        print(f"step {k:3d} plain it {o['plain']['iterations']:4d} learned it {o['learned']['iterations']:4d} "
+              f"corrected it {c['iterations']:4d} used {c['used_learned_correction']} "
+              f"reduction {c['correction_reduction'][0]:.3f} -> {c['correction_reduction'][1]:.3f}")
+        assert c["converged"] == 1 and o["learned"]["converged"] == 1
+        if c["used_learned_correction"]:
+            assert c["correction_reduction"][1] < c["correction_reduction"][0]
+    for o in out[:train]:
+        assert o["corrected"]["used_learned_correction"] == 0  # weight 0 while training
+    for o in out[train:]:
+        assert o["corrected"]["correction_reduction"][0] >= 0  # tried on every solve after training
+    print("correction held-out explained", np.round(corr.heldout, 3).tolist())
+
+
+def test_learned_correction_falls_back(cuda, product_lib):
+    """An untrained network at a large weight makes the first step worse than the plain
+    preconditioner: the solve falls back to the plain preconditioner and reaches the
+    solution of a solve without any correction."""
+    from conductorrigid_b200.device import Handle
+    from conductorrigid_b200.learned import Network
+
+    s = systems_small(0.20)
+    ref = Handle(_params(s), s.L)
+    ref.set_topology(s.body, s.rigid, s.body_charge)
+    q0 = ref.dev(np.zeros(s.n_beads))
+    p0 = ref.dev(np.zeros(s.n_bodies))
+    ref.compute(s.pos, s.body_pos, q0, p0)
+    net = Network(seed=11)
+    h = Handle(_params(s), s.L)
+    h.set_topology(s.body, s.rigid, s.body_charge)
+    h.set_correction(net, 1000.0)
+    q = h.dev(np.zeros(s.n_beads))
+    phi = h.dev(np.zeros(s.n_bodies))
+    _, st = h.compute(s.pos, s.body_pos, q, phi)
+    print("reductions plain / corrected:", st["correction_reduction"])
+    assert st["used_learned_correction"] == 0
+    assert st["correction_reduction"][1] > st["correction_reduction"][0] >= 0
+    assert st["converged"] == 1
+    assert float((q - q0).abs().max() / q0.abs().max()) < 1e-5
+    h.set_correction(None)
+    ref.close()
+    h.close()
+    net.close()
