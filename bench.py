@@ -172,6 +172,7 @@ def run_op_case(args) -> None:
     base = dict(xi=p["xi"], errortol=p["errortol"], grid=grid, support=p["support"], rcut=p["rcut"])
     h = Handle(_lib.make_params(field=tuple(s.field), precond="conductor", **base), s.L)
     h.set_topology(s.body, s.rigid, s.body_charge)
+    h.set_realspace(args.realspace)
     h.set_positions(s.pos, s.body_pos)
     x = torch.randn(s.n_beads + s.n_bodies, dtype=torch.float64, device="cuda")
     for _ in range(args.warmup + args.steps):
@@ -627,6 +628,7 @@ def run_solve(args) -> None:
         h = Handle(_lib.make_params(precision=prec, precond=pc or args.precond, restart=rs or args.restart,
                                     learned=bool(args.learned) and a == "fast", **common), s.L, stream=stream)
         h.set_coarse(args.coarse_max_dense, args.coarse_cg)
+        h.set_realspace(args.realspace)
         h.set_topology(s.body, s.rigid, s.body_charge)
         handles[a] = h
     hh = handles[head_arm]
@@ -858,6 +860,8 @@ def main() -> None:
                     help="coarse problems above this many unknowns use the sparse form (--coarse-cg steps of CG on "
                          "near-pair blocks + the low-rank wave term) or, with --coarse-cg 0, no coarse level")
     ap.add_argument("--coarse-cg", type=int, default=0, help="CG steps of the sparse coarse form")
+    ap.add_argument("--realspace", type=int, default=0,
+                    help="real-space kernel values evaluated on the fly: 1 FP32, 2 FP64, 3 both (default 0: stored)")
     ap.add_argument("--train-solves", type=int, default=0,
                     help="dynamics: solves the networks are trained on (default min(200, steps/2))")
     args = ap.parse_args()
