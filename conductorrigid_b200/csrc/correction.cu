@@ -24,10 +24,11 @@
 // (w, P w).
 //
 // Fallback: before a solve uses the correction it is tried on the solve's initial
-// residual r: the one-step residual reductions min_a ||r - a A P r|| and
-// min_a ||r - a A P' r|| (P' = P plus the correction) are compared, and the correction
-// is used in that solve only if it reduces the residual more than the plain
-// preconditioner; otherwise the solve runs with the plain preconditioner alone.
+// residual r: the one-step least-squares residual over span{A P r} is compared with the
+// one over span{A P r, A c} (c the correction of r), and the correction is used in that
+// solve only if it lowers that residual by at least 1 % -- at the scale the least-squares
+// fit gives it;
+// otherwise the solve runs with the plain preconditioner alone.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -272,7 +273,8 @@ int correction_add(cr_handle *h, const double *v, double *z) {
     CR_TRY(correction_features(h, v, z, c.x));
     if (mlp_forward_async(c.net, h->N, c.x, c.y, h->stream) != CR_OK)
         return fail(h, CR_CUDA_ERROR, "learned correction: network launch failed");
-    corr_apply_kernel<<<blocks_for(h->N, 256), 256, 0, h->stream>>>(h->N, h->N + h->B, c.weight, c.ss, c.y, z);
+    corr_apply_kernel<<<blocks_for(h->N, 256), 256, 0, h->stream>>>(h->N, h->N + h->B, c.weight * c.scale, c.ss,
+                                                                     c.y, z);
     CR_LAUNCH(h, "corr_apply_kernel");
     return CR_OK;
 }
@@ -285,34 +287,61 @@ int precondition_step(cr_handle *h, const double *v, double *z) {
     return CR_OK;
 }
 
-// Decide for this solve (residual r, operator precision `precision`): the one-step
-// residual reduction with and without the correction (see the file header).
+// Decide for this solve (residual r, operator precision `precision`): with zp = P r and
+// c the network's correction of r (at the caller's weight), the one-step least-squares
+// residual over span{A zp} and over span{A zp, A c}.  The correction is used only if the
+// second is smaller by at least 1 %, and then with the fitted scale: the solve's steps apply
+// zp + (a_c / a_p) c, (a_p, a_c) the least-squares coefficients.
 int correction_decide(cr_handle *h, int precision, const double *r, double *w) {
     Correction &c = h->corr;
     c.active = 0;
+    c.scale = 1.0;
     c.last_rho[0] = c.last_rho[1] = -1.0;
     if (!c.net || c.weight == 0.0 || h->N == 0) return CR_OK;
     CR_TRY(correction_prepare(h));
+    const int n = h->N + h->B;
     CR_TRY(precondition(h, r, c.zp));
-    CR_CUDA(h, cudaMemcpyAsync(c.zc, c.zp, (size_t)(h->N + h->B) * sizeof(double), cudaMemcpyDeviceToDevice,
-                               h->stream));
-    CR_TRY(correction_add(h, r, c.zc));
+    CR_CUDA(h, cudaMemsetAsync(c.zc, 0, (size_t)n * sizeof(double), h->stream));
+    CR_TRY(correction_features(h, r, c.zp, c.x));  // the correction alone, into zc
+    if (mlp_forward_async(c.net, h->N, c.x, c.y, h->stream) != CR_OK)
+        return fail(h, CR_CUDA_ERROR, "learned correction: network launch failed");
+    corr_apply_kernel<<<blocks_for(h->N, 256), 256, 0, h->stream>>>(h->N, n, c.weight, c.ss, c.y, c.zc);
+    CR_LAUNCH(h, "corr_apply_kernel");
     Krylov &K = h->kry;
+    double *wp = w, *wc = K.d;  // A zp and A c (K.d is free before the solve's refinement)
+    CR_TRY(apply_operator(h, c.zp, wp, precision));
+    CR_TRY(apply_operator(h, c.zc, wc, precision));
     CR_TRY(dots(h, 1, r, r, K.hcol));
-    double rho[2];
-    for (int t = 0; t < 2; ++t) {
-        CR_TRY(apply_operator(h, t == 0 ? c.zp : c.zc, w, precision));
-        CR_TRY(dots(h, 1, w, r, K.hcol + 1));
-        CR_TRY(dots(h, 1, w, w, K.hcol + 2));
-        CR_CUDA(h, cudaMemcpyAsync(K.h_pinned, K.hcol, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        CR_CUDA(h, cudaStreamSynchronize(h->stream));
-        const double rr = K.h_pinned[0], wr = K.h_pinned[1], ww = K.h_pinned[2];
-        rho[t] = (rr > 0 && ww > 0) ? std::max(0.0, 1.0 - wr * wr / (rr * ww)) : 1.0;
-    }
+    CR_TRY(dots(h, 1, wp, r, K.hcol + 1));
+    CR_TRY(dots(h, 1, wc, r, K.hcol + 2));
+    double g[3];
+    CR_TRY(dots(h, 1, wp, wp, K.hcol + 3));
+    CR_TRY(dots(h, 1, wp, wc, K.hcol + 4));
+    CR_TRY(dots(h, 1, wc, wc, K.hcol + 5));
+    CR_CUDA(h, cudaMemcpyAsync(K.h_pinned, K.hcol, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CR_CUDA(h, cudaStreamSynchronize(h->stream));
     if (mlp_check(c.net, h->stream) != CR_OK) return fail(h, CR_TIMEOUT, "learned correction: network wait ran out");
-    c.last_rho[0] = std::sqrt(rho[0]);
-    c.last_rho[1] = std::sqrt(rho[1]);
-    c.active = std::isfinite(rho[1]) && rho[1] < rho[0] ? 1 : 0;
+    const double rr = K.h_pinned[0], pr = K.h_pinned[1], cr = K.h_pinned[2];
+    g[0] = K.h_pinned[3];
+    g[1] = K.h_pinned[4];
+    g[2] = K.h_pinned[5];
+    if (!(rr > 0) || !(g[0] > 0)) return CR_OK;
+    const double rho_p = std::max(0.0, 1.0 - pr * pr / (rr * g[0]));
+    c.last_rho[0] = std::sqrt(rho_p);
+    const double det = g[0] * g[2] - g[1] * g[1];
+    if (!(det > 1e-12 * g[0] * g[2])) {  // the correction adds no new direction
+        c.last_rho[1] = c.last_rho[0];
+        return CR_OK;
+    }
+    const double ap = (g[2] * pr - g[1] * cr) / det, ac = (g[0] * cr - g[1] * pr) / det;
+    const double rho_c = std::max(0.0, 1.0 - (ap * pr + ac * cr) / rr);
+    c.last_rho[1] = std::sqrt(rho_c);
+    // a direction unrelated to r lowers the least-squares residual by ~1/n only: the
+    // correction must lower it by at least 1 % to be used
+    if (std::isfinite(rho_c) && ap != 0.0 && std::isfinite(ac / ap) && c.last_rho[1] < 0.99 * c.last_rho[0]) {
+        c.active = 1;
+        c.scale = ac / ap;
+    }
     return CR_OK;
 }
 

@@ -109,6 +109,7 @@ struct RealSpace {
 struct Correction {
     cr_mlp *net = nullptr;              // the caller's network (not owned); null: no correction
     double weight = 1.0;
+    double scale = 1.0;                 // fitted scale of the correction in the current solve
     int active = 0;                     // used by the current solve (decided per solve)
     double last_rho[2] = {-1.0, -1.0};  // one-step residual reduction without / with it
     uint16_t *x = nullptr;              // [N][48] BF16 feature rows

@@ -366,10 +366,11 @@ int cr_neutral_direction(cr_handle *h, const void *d_v, int v_is_fp32, double sc
  * network's per-bead output for 48 features of (v, P v) (the vectors at unit RMS, the own
  * body's mean and induced dipole of P v, the field direction, and for the 8 nearest bodies
  * their direction, proximity, mean of P v and the potential of their induced dipole).
- * Before a solve uses it, the correction is tried on the solve's initial residual r: it
- * is used only if min_a ||r - a A P' r|| < min_a ||r - a A P r|| (P' with the
- * correction), otherwise the solve falls back to the plain preconditioner;
- * cr_solve_stats reports the choice and both reductions.  The network is the caller's
+ * Before a solve uses it, the correction c of the solve's initial residual r is tried:
+ * it is used only if the least-squares residual of r over span{A P r, A c} is at least
+ * 1 % below the one over span{A P r} alone, and then at the scale that fit gives it (z' = P v +
+ * (a_c / a_p) weight s y); otherwise the solve falls back to the plain preconditioner.
+ * cr_solve_stats reports the choice and both relative residuals.  The network is the caller's
  * (cr_mlp_create); net = NULL removes it, weight = 0 keeps it set without applying it.
  * Flexible GMRES keeps the fixed point and the true-residual stopping test whatever the
  * network outputs.

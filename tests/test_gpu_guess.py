@@ -185,7 +185,7 @@ def test_learned_correction_in_time_stepping(cuda, product_lib):
               f"reduction {c['correction_reduction'][0]:.3f} -> {c['correction_reduction'][1]:.3f}")
         assert c["converged"] == 1 and o["learned"]["converged"] == 1
         if c["used_learned_correction"]:
-            assert c["correction_reduction"][1] < c["correction_reduction"][0]
+            assert c["correction_reduction"][1] < 0.99 * c["correction_reduction"][0]
     for o in out[:train]:
         assert o["corrected"]["used_learned_correction"] == 0  # weight 0 while training
     for o in out[train:]:
@@ -194,9 +194,10 @@ def test_learned_correction_in_time_stepping(cuda, product_lib):
 
 
 def test_learned_correction_falls_back(cuda, product_lib):
-    """An untrained network at a large weight makes the first step worse than the plain
-    preconditioner: the solve falls back to the plain preconditioner and reaches the
-    solution of a solve without any correction."""
+    """An untrained network's correction is a direction unrelated to the residual: even at
+    its least-squares scale it lowers the first step's residual by far less than the 1 %
+    a correction must gain, so the solve falls back to the plain preconditioner and
+    reaches the solution of a solve without any correction."""
     from conductorrigid_b200.device import Handle
     from conductorrigid_b200.learned import Network
 
@@ -215,7 +216,7 @@ def test_learned_correction_falls_back(cuda, product_lib):
     _, st = h.compute(s.pos, s.body_pos, q, phi)
     print("reductions plain / corrected:", st["correction_reduction"])
     assert st["used_learned_correction"] == 0
-    assert st["correction_reduction"][1] > st["correction_reduction"][0] >= 0
+    assert 0.99 * st["correction_reduction"][0] <= st["correction_reduction"][1] <= st["correction_reduction"][0]
     assert st["converged"] == 1
     assert float((q - q0).abs().max() / q0.abs().max()) < 1e-5
     h.set_correction(None)

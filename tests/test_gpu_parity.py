@@ -306,3 +306,24 @@ def test_realspace_modes_match_oracle(cuda, product_lib, oracle_lib, flags, case
     y64s = h.apply_operator(x)
     assert rel(y64, y64s.cpu().numpy()) < 1e-13, "FP64 on-the-fly and stored products differ"
     h.close()
+
+
+def test_operator_matches_oracle_at_the_cutoff(cuda, product_lib, oracle_lib):
+    """The polydisperse mixture scaled down: spheres of radius 2 carry antipodal beads at
+    exactly the cutoff distance 4, so the in-range decision of those pairs must round as
+    the oracle's does (the tabulated kernel is 5.8e-6 there, not zero)."""
+    from conductorrigid_b200 import systems
+
+    w = systems.workload("polydisperse_204k", scale=0.05)
+    s, p = w.system, w.params
+    grid = systems.smooth_at_least(int(np.ceil(256 * s.L[0] / systems.workload("polydisperse_204k").system.L[0])),
+                                   4096)
+    base = dict(xi=p["xi"], errortol=p["errortol"], grid=grid, support=p["support"], rcut=p["rcut"])
+    h = make_handle(product_lib, s, base)
+    orc = oracle_lib.Oracle(s, p["xi"], p["errortol"], grid, p["support"], p["rcut"])
+    x = np.random.default_rng(23).standard_normal(s.n_beads + s.n_bodies)
+    ref = orc.matvec(x)
+    assert rel(h.apply_operator(x), ref) < 1e-11
+    assert rel(h.apply_operator(x, product_lib.CR_FP32), ref) < 2e-5
+    assert rel(h.objective(), orc.objective(s.field)) < 1e-14
+    h.close()
