@@ -143,11 +143,11 @@ __global__ void __launch_bounds__(256) spread_tiles_kernel(
 
 // Spread for a compile-time support PT (tile edge 8, halo buffer edge BD = 8 + PT - 1):
 // thread t < BD*BD owns the buffer column (y, z) = (t / BD, t % BD) in registers.  Beads
-// of the tile are taken 32 at a time: lane l of warp 0 computes the Gaussian factors of
-// bead l of the batch into shared memory (x factors already shifted to the column's
-// x index and scaled by prefac q), then every thread adds the beads whose window covers
-// its column.  No shared-memory atomics; within a tile the summation order is fixed.
-// The columns are added to the mesh once at the end.
+// of the tile are taken 32 at a time: the first threads stage the batch's bead data, then
+// all threads compute the batch's 32 x 3P Gaussian factors into shared memory (x factors
+// already shifted to the column's x index and scaled by prefac q), then every thread adds
+// the beads whose window covers its column.  No shared-memory atomics; within a tile the
+// summation order is fixed.  The columns are added to the mesh once at the end.
 template <typename R, int PT>
 __global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32) spread_columns_kernel(
     const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
@@ -156,7 +156,9 @@ __global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32) 
     constexpr int P = PT, T = 8, BD = T + PT - 1;
     __shared__ R sx[32][BD];     // shifted, scaled x factors
     __shared__ R sy[32][P], sz[32][P];
-    __shared__ int soy[32], soz[32];
+    __shared__ R sp[32][3], sc[32];
+    __shared__ int4 sst[32];
+    __shared__ int sox[32], soy[32], soz[32];
     const int tile = blockIdx.x;
     const int b0 = tile_start[tile], b1 = tile_start[tile + 1];
     if (b0 == b1) return;
@@ -169,30 +171,43 @@ __global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32) 
     for (int x = 0; x < BD; ++x) col[x] = (R)0;
     for (int base = b0; base < b1; base += 32) {
         const int nb = min(32, b1 - base);
-        if (t < 32) {
-            const int l = t;
-            if (l < nb) {
-                const int i = tile_beads[base + l];
-                const typename Prec<R>::R4 p = pos[i];
-                const int4 st = wstart[i];
-                const int ox = wrapmod(st.x, ms.Ng[0]) - tx * T;
-                const int oy = wrapmod(st.y, ms.Ng[1]) - ty * T;
-                const int oz = wrapmod(st.z, ms.Ng[2]) - tz * T;
-                const bool ok = ox >= 0 && ox < T && oy >= 0 && oy < T && oz >= 0 && oz < T;
-                const R c = ok ? prefac * q[i] : (R)0;
-#pragma unroll
-                for (int x = 0; x < BD; ++x) sx[l][x] = (R)0;
-#pragma unroll
-                for (int a = 0; a < P; ++a) {
-                    const R rx = wc.h[0] * (R)(st.x + a) - wc.halfL[0] - p.x;
-                    const R ry = wc.h[1] * (R)(st.y + a) - wc.halfL[1] - p.y;
-                    const R rz = wc.h[2] * (R)(st.z + a) - wc.halfL[2] - p.z;
-                    if (ok) sx[l][ox + a] = c * dexp(-wc.xiterm * rx * rx * wc.inv_eta[0]);
-                    sy[l][a] = dexp(-wc.xiterm * ry * ry * wc.inv_eta[1]);
-                    sz[l][a] = dexp(-wc.xiterm * rz * rz * wc.inv_eta[2]);
-                }
-                soy[l] = ok ? oy : -BD;  // a bead outside its tile touches no column
-                soz[l] = oz;
+        // bead data of the batch, and cleared x-factor rows
+        if (t < nb) {
+            const int i = tile_beads[base + t];
+            const typename Prec<R>::R4 p = pos[i];
+            const int4 st = wstart[i];
+            const int ox = wrapmod(st.x, ms.Ng[0]) - tx * T;
+            const int oy = wrapmod(st.y, ms.Ng[1]) - ty * T;
+            const int oz = wrapmod(st.z, ms.Ng[2]) - tz * T;
+            const bool ok = ox >= 0 && ox < T && oy >= 0 && oy < T && oz >= 0 && oz < T;
+            sp[t][0] = p.x;
+            sp[t][1] = p.y;
+            sp[t][2] = p.z;
+            sst[t] = st;
+            sc[t] = ok ? prefac * q[i] : (R)0;
+            sox[t] = ok ? ox : -1;   // a bead outside its tile writes no x factor...
+            soy[t] = ok ? oy : -BD;  // ...and touches no column
+            soz[t] = oz;
+        }
+        for (int e = t; e < nb * BD; e += blockDim.x) (&sx[0][0])[e] = (R)0;
+        __syncthreads();
+        // the batch's Gaussian factors, all threads: entry e = (bead l, dimension d, node a)
+        for (int e = t; e < nb * 3 * P; e += blockDim.x) {
+            const int l = e / (3 * P), rem = e - l * 3 * P;
+            const int d = rem / P, a = rem - d * P;
+            // (selected, not indexed, so the parameter block stays in registers)
+            const int st = d == 0 ? sst[l].x : (d == 1 ? sst[l].y : sst[l].z);
+            const R hd = d == 0 ? wc.h[0] : (d == 1 ? wc.h[1] : wc.h[2]);
+            const R half = d == 0 ? wc.halfL[0] : (d == 1 ? wc.halfL[1] : wc.halfL[2]);
+            const R ie = d == 0 ? wc.inv_eta[0] : (d == 1 ? wc.inv_eta[1] : wc.inv_eta[2]);
+            const R r = hd * (R)(st + a) - half - sp[l][d];
+            const R w = dexp(-wc.xiterm * r * r * ie);
+            if (d == 0) {
+                if (sox[l] >= 0) sx[l][sox[l] + a] = sc[l] * w;
+            } else if (d == 1) {
+                sy[l][a] = w;
+            } else {
+                sz[l][a] = w;
             }
         }
         __syncthreads();

@@ -391,110 +391,6 @@ __global__ void __launch_bounds__(W * 32, sizeof(R) == 4 ? 6 : 1) pair_spmv_kern
 
 constexpr int kSpmvWarps = 8;
 
-// The FP32 product of pair_spmv_kernel, software-pipelined across pairs: while a warp
-// consumes the first U slots of pair k it already has the first U slots of its next pair
-// k + W in flight (two bursts per warp instead of one), so the loads that a warp keeps
-// outstanding no longer drain at every pair boundary.  Slots beyond the first U of a
-// pair (rows longer than U) are loaded and consumed in further bursts as before.  Same
-// lanes, sum order and result as pair_spmv_kernel.
-template <int W, int U>
-__global__ void __launch_bounds__(W * 32, 4) pair_spmv_pipe_kernel(const long long *__restrict__ head,
-                                                                  const int *__restrict__ count,
-                                                                  const int *__restrict__ pair_j,
-                                                                  const int *__restrict__ members,
-                                                                  const unsigned *__restrict__ masks,
-                                                                  const long long *__restrict__ voff,
-                                                                  const int *__restrict__ slots,
-                                                                  const float *__restrict__ vals,
-                                                                  const float *__restrict__ qc,
-                                                                  const float *__restrict__ q,
-                                                                  const float *__restrict__ phik, double selfc,
-                                                                  const double *__restrict__ phi_body,
-                                                                  const uint32_t *__restrict__ body,
-                                                                  double *__restrict__ out) {
-    __shared__ float part[W][CS];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int I = blockIdx.x;
-    float yI = 0.f;
-    const long long h0 = head[I];
-    const int n = count[I];
-    // current pair: mask row, charge of bead `lane` of J, slots, value base, first burst
-    unsigned m = 0;
-    float xJ = 0.f;
-    int rows = 0;
-    const float *v = vals;
-    float t[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) t[u] = 0.f;
-    if (w < n) {
-        const long long p = h0 + w;
-        m = masks[p * CS + lane];
-        xJ = qc[pair_j[p] * CS + lane];
-        rows = slots[p] / CS;
-        v = vals + voff[p] + lane;
-        const int own = __popc(m);
-#pragma unroll
-        for (int u = 0; u < U; ++u) t[u] = u < own ? __ldg(v + (size_t)u * CS) : 0.f;
-    }
-    for (int k = w; k < n; k += W) {
-        // next pair: metadata and its first burst, issued before the current pair is used
-        unsigned mn = 0;
-        float xn = 0.f;
-        int rn = 0;
-        const float *vn = vals;
-        float tn[U];
-        if (k + W < n) {
-            const long long p = h0 + k + W;
-            mn = masks[p * CS + lane];
-            xn = qc[pair_j[p] * CS + lane];
-            rn = slots[p] / CS;
-            vn = vals + voff[p] + lane;
-            const int ownn = __popc(mn);
-#pragma unroll
-            for (int u = 0; u < U; ++u) tn[u] = u < ownn ? __ldg(vn + (size_t)u * CS) : 0.f;
-        } else {
-#pragma unroll
-            for (int u = 0; u < U; ++u) tn[u] = 0.f;
-        }
-        const int own = __popc(m);
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int j = m ? __ffs(m) - 1 : 0;
-            m &= m - 1;
-            yI += t[u] * __shfl_sync(0xffffffffu, xJ, j);
-        }
-        for (int base = U; base < rows; base += U) {
-            float r[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) r[u] = base + u < own ? __ldg(v + (size_t)(base + u) * CS) : 0.f;
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int j = m ? __ffs(m) - 1 : 0;
-                m &= m - 1;
-                yI += r[u] * __shfl_sync(0xffffffffu, xJ, j);
-            }
-        }
-        m = mn;
-        xJ = xn;
-        rows = rn;
-        v = vn;
-#pragma unroll
-        for (int u = 0; u < U; ++u) t[u] = tn[u];
-    }
-    part[w][lane] = yI;
-    __syncthreads();
-    if (w == 0) {
-        float tot = 0.f;
-#pragma unroll
-        for (int u = 0; u < W; ++u) tot += part[u][lane];
-        const int bi = members[I * CS + lane];
-        if (bi >= 0) {
-            const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)tot;
-            out[bi] = phi_body ? phi_body[body[bi]] - total : total;
-        }
-    }
-}
-
 // Bead offsets from their cluster's centre in FP32 (minimum image; 0 for padding).
 __global__ void cluster_offsets_kernel(int n, const int *__restrict__ members, const double4 *__restrict__ pos,
                                        const double4 *__restrict__ centre, RSBuild c, float4 *__restrict__ off) {
@@ -1069,13 +965,6 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
                                                                     m.phi, h->d.selfcoeff, phi_body, h->d_body, out);
             CR_LAUNCH(h, "pair_otf64_kernel");
         }
-        return CR_OK;
-    }
-    if constexpr (sizeof(R) == 4) {
-        pair_spmv_pipe_kernel<W, 16><<<r.nclus, W * 32, 0, h->stream>>>(
-            r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, m.phi,
-            h->d.selfcoeff, phi_body, h->d_body, out);
-        CR_LAUNCH(h, "pair_spmv_pipe_kernel");
         return CR_OK;
     }
     pair_spmv_kernel<R, W, 16><<<r.nclus, W * 32, 0, h->stream>>>(
