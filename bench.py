@@ -816,6 +816,13 @@ def run_solve(args) -> None:
         sp_alg = algorithmic_bytes("spread", prec_bytes, s.n_beads, G, 0)
         line["spread"] = {"achieved_gbs": sp_alg / (sp_ms * 1e-3) / 1e9, "avg_launch_ms": sp_ms,
                           "frac": sp_alg / (sp_ms * 1e-3) / 1e9 / peak}
+    # spread and contract are bound by instruction issue and shared memory, not HBM: their
+    # work rate is N P^3 weighted node updates per launch
+    updates = float(s.n_beads) * p["support"] ** 3
+    for k in ("spread", "contract"):
+        if k in prof and prof[k]["launches"]:
+            ms_k = prof[k]["ms"] / prof[k]["launches"]
+            line.setdefault(k, {"avg_launch_ms": ms_k})["weighted_updates_per_s"] = updates / (ms_k * 1e-3)
     if rank == 0 and world == 1 and not args.no_cpu and args.scale == 1.0:
         if name == "plain_small":
             line["cpu_baseline"] = cpu_full_solve(s, p)
