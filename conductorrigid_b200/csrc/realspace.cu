@@ -137,7 +137,10 @@ __global__ void pair_search_kernel(int nclus, const double4 *__restrict__ centre
     for (int base = 0; base < nclus; base += 32) {
         const int J = base + lane;
         bool hit = false;
-        if (J < nclus) hit = J == I || box_gap2(ci, ei, centre[J], extent[J], c) < c.rc2;
+        // a bead pair at exactly the cutoff can make two clusters' box gap equal rc: the
+        // test is widened by a relative 1e-9 so that rounding never drops such a cluster
+        // pair (the masks then decide every bead pair exactly)
+        if (J < nclus) hit = J == I || box_gap2(ci, ei, centre[J], extent[J], c) < c.rc2 * (1.0 + 1e-9);
         const unsigned mask = __ballot_sync(0xffffffffu, hit);
         if (FILL && hit) pair_j[h0 + n + __popc(mask & ((1u << lane) - 1u))] = J;
         n += __popc(mask);
