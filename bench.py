@@ -193,7 +193,8 @@ def run_replicas(args) -> None:
 
     R = Replicas(systems.replica_specs(256, seed=1), precond=args.precond)
     R.warm()
-    policy_rates = R.tune_batch(16)  # untimed set-up: tiling policy by batch throughput
+    nt = args.batch_threads
+    policy_rates = R.tune_batch(nt)  # untimed set-up: tiling policy by batch throughput
 
     def timed(fn):
         R.reset()
@@ -206,8 +207,8 @@ def run_replicas(args) -> None:
         return e0.elapsed_time(e1), st
 
     for _ in range(args.warmup):
-        timed(lambda: R.solve_batched(16))
-    ms = [timed(lambda: R.solve_batched(16)) for _ in range(args.steps)]
+        timed(lambda: R.solve_batched(nt))
+    ms = [timed(lambda: R.solve_batched(nt)) for _ in range(args.steps)]
     ms_loop, st_loop = timed(R.solve_looped)
     t_batch = statistics.median(m for m, _ in ms)
     st = ms[-1][1]
@@ -219,7 +220,7 @@ def run_replicas(args) -> None:
         "iterations_mean": round(float(np.mean([s["iterations"] for s in st])), 1),
         "iterations_max": int(max(s["iterations"] for s in st)),
         "converged": int(sum(s["converged"] for s in st)), "replicas": R.n, "charges": R.n_charges,
-        "tiling_policy": R.best_policy, "tiling_policy_rates": {k: round(v, 1) for k, v in policy_rates.items()},
+        "host_threads": nt, "tiling_policy": R.best_policy, "tiling_policy_rates": {k: round(v, 1) for k, v in policy_rates.items()},
         "isolated_autotune_tiles": {str(t): sum(1 for c in R.tilings if c["tile_edge"] == t) for t in (4, 6, 8, 12, 16)},
         "dtype": "f32 operator, f64 Krylov", "data": "synthetic (seeded replica generator)",
         "config": {"workload": "replicas_256: N_body~U[20,400], phi~U[0.05,0.35], |E0|=1, 2 nodes/unit, P=9",
@@ -869,6 +870,8 @@ def main() -> None:
     ap.add_argument("--coarse-cg", type=int, default=0, help="CG steps of the sparse coarse form")
     ap.add_argument("--realspace", type=int, default=0,
                     help="real-space kernel values evaluated on the fly: 1 FP32, 2 FP64, 3 both (default 0: stored)")
+    ap.add_argument("--batch-threads", type=int, default=16,
+                    help="replicas: host threads (one stream each) of the batched solve")
     ap.add_argument("--train-solves", type=int, default=0,
                     help="dynamics: solves the networks are trained on (default min(200, steps/2))")
     args = ap.parse_args()
