@@ -869,7 +869,8 @@ def main() -> None:
                          "near-pair blocks + the low-rank wave term) or, with --coarse-cg 0, no coarse level")
     ap.add_argument("--coarse-cg", type=int, default=0, help="CG steps of the sparse coarse form")
     ap.add_argument("--realspace", type=int, default=0,
-                    help="real-space kernel values evaluated on the fly: 1 FP32, 2 FP64, 3 both (default 0: stored)")
+                    help="real-space kernel values evaluated on the fly: 1 FP32, 2 FP64, 3 both; 4: stored values "
+                         "streamed through shared memory (default 0: stored, read by one CTA per cluster)")
     ap.add_argument("--batch-threads", type=int, default=16,
                     help="replicas: host threads (one stream each) of the batched solve")
     ap.add_argument("--train-solves", type=int, default=0,

@@ -31,6 +31,7 @@ PRECISIONS = {"fp64": CR_FP64, "mixed": CR_MIXED, "fp32": CR_FP32}
 
 CR_REALSPACE_ONFLY32 = 1
 CR_REALSPACE_ONFLY64 = 2
+CR_REALSPACE_STREAM = 4
 
 CR_PRECOND_DIAGONAL = 0
 CR_PRECOND_CONDUCTOR = 1
@@ -153,6 +154,7 @@ _SIGS = {
     "cr_set_stream": ([_P, _P], _I),
     "cr_set_graphs": ([_P, _I], _I),
     "cr_set_realspace": ([_P, _I], _I),
+    "cr_set_wait_limit": ([_P, C.c_longlong, _I], _I),
     "cr_set_correction": ([_P, _P, C.c_double], _I),
     "cr_correction_samples": ([_P, _I, _P, _P, C.POINTER(C.c_int)], _I),
     "cr_set_tiling": ([_P, _I, _I], _I),

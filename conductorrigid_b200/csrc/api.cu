@@ -219,6 +219,11 @@ int cr_create(const cr_params *p, const double L[3], cr_handle **out) {
         delete h;
         return CR_CUDA_ERROR;
     }
+    if (cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || h->n_sm <= 0) {
+        cudaGetLastError();
+        delete h;
+        return CR_CUDA_ERROR;
+    }
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
     *out = h;
@@ -360,10 +365,20 @@ int cr_correction_samples(cr_handle *h, int max_dirs, uint16_t *d_x, float *d_t,
 
 int cr_set_realspace(cr_handle *h, int flags) {
     if (!h) return CR_BAD_PARAM;
-    if (flags & ~(CR_REALSPACE_ONFLY32 | CR_REALSPACE_ONFLY64)) return fail(h, CR_BAD_PARAM, "unknown real-space flags");
+    if (flags & ~(CR_REALSPACE_ONFLY32 | CR_REALSPACE_ONFLY64 | CR_REALSPACE_STREAM))
+        return fail(h, CR_BAD_PARAM, "unknown real-space flags");
     if (h->stream) CR_CUDA(h, cudaStreamSynchronize(h->stream));
     h->rs_onfly = flags;
     h->geo_gen++;  // captured Arnoldi steps hold the old kernels: capture again
+    return CR_OK;
+}
+
+int cr_set_wait_limit(cr_handle *h, long long cycles, int withhold_next) {
+    if (!h) return CR_BAD_PARAM;
+    if (h->stream) CR_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->rs.wait_limit = cycles > 0 ? cycles : (1LL << 31);
+    h->rs.withhold_next = withhold_next ? 1 : 0;
+    h->geo_gen++;  // captured Arnoldi steps hold the old limit: capture again
     return CR_OK;
 }
 
@@ -430,7 +445,8 @@ int cr_apply_operator(cr_handle *h, const double *d_x, double *d_y, int precisio
     if (h->N == 0) return CR_OK;
     if (!d_x || !d_y) return fail(h, CR_BAD_PARAM, "null vector");
     CR_TRY(apply_operator(h, d_x, d_y, precision));
-    return check_cuda(h, cudaStreamSynchronize(h->stream), "cr_apply_operator");
+    CR_TRY(check_cuda(h, cudaStreamSynchronize(h->stream), "cr_apply_operator"));
+    return realspace_check(h);
 }
 
 int cr_precondition(cr_handle *h, const double *d_x, double *d_y) {
@@ -644,7 +660,10 @@ int cr_compute(cr_handle *h, const double *d_pos, const double *d_body_pos, doub
     if (B) CR_CUDA(h, cudaMemcpyAsync(K.x + N, d_phi, B * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     CR_CUDA(h, cudaEventRecord(h->ev0, h->stream));
     const int sst = solve(h, K.x, K.b, &st);
-    if (sst != CR_OK && sst != CR_NOT_CONVERGED) return sst;
+    if (sst != CR_OK && sst != CR_NOT_CONVERGED) {
+        const int rc = realspace_check(h);  // a wait that ran out explains a failed solve
+        return rc != CR_OK ? rc : sst;
+    }
     CR_CUDA(h, cudaEventRecord(h->ev1, h->stream));
     CR_CUDA(h, cudaMemcpyAsync(d_q, K.x, N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     if (B) CR_CUDA(h, cudaMemcpyAsync(d_phi, K.x + N, B * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
@@ -653,6 +672,7 @@ int cr_compute(cr_handle *h, const double *d_pos, const double *d_body_pos, doub
     CR_TRY(wave_force(h, h->m64));
     CR_TRY(real_space_force(h, h->m64, K.x, d_force));
     CR_CUDA(h, cudaStreamSynchronize(h->stream));
+    CR_TRY(realspace_check(h));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     st.solve_ms = ms;

@@ -99,10 +99,25 @@ struct RealSpace {
     bool valid32 = false, valid64 = false;
     float *acc32 = nullptr;         // [nclus*32] charges in cluster order
     double *acc64 = nullptr;
+    float *ysum32 = nullptr;        // [nclus*32] sums of the streamed product (cleared after use)
+    double *ysum64 = nullptr;
     double *freal = nullptr;        // [3N] real-space forces
     float4 *boff = nullptr;         // [nclus*32] bead offsets from their cluster centre (FP32)
     float4 *pshift = nullptr;       // [npairs] centre offset of the pair (minimum image), .w = 1 when
                                     // bead separations need no further image
+    // streamed product (one per operator precision): the CTAs' cluster ranges and chunks
+    struct StreamPlan {
+        int ctas = 0;
+        int *cl0 = nullptr;             // [ctas+1] first cluster of each CTA
+        long long *cbase = nullptr;     // [ctas+1] first chunk of each CTA
+        long long *cstart = nullptr;    // [chunks] absolute first byte of each chunk
+        long long cap = 0;              // capacity of cstart
+        bool valid = false;
+    };
+    StreamPlan plan32, plan64;
+    int *err = nullptr;             // device error word of the streamed product (1: a wait ran out)
+    long long wait_limit = 1LL << 31;  // cycles of one bounded wait (about a second)
+    int withhold_next = 0;          // the next streamed product issues no copies (test of the waits)
 };
 
 // Learned correction of the preconditioner (correction.cu).
@@ -300,6 +315,7 @@ struct cr_handle {
     int use_graphs = 1;
     // real-space kernel values: CR_REALSPACE_* flags, evaluated on the fly instead of stored
     int rs_onfly = 0;
+    int n_sm = 0;                     // multiprocessors of the device
     long long geo_gen = 0;
     long long graph_launches = 0;
     // learned guess: caller directions for the next solve [CR_MAX_GUESS_DIRECTIONS][N+B]
@@ -391,6 +407,9 @@ int realspace_build(cr_handle *h);
 int real_space_virial(cr_handle *h, const double *q64, double *out);
 int wave_virial(cr_handle *h, double *out);
 int realspace_prepare(cr_handle *h, int precision);
+// CR_TIMEOUT (and the error word cleared) when a bounded wait of the streamed product ran
+// out since the last check; synchronises the stream.
+int realspace_check(cr_handle *h);
 int mesh_set_tile(cr_handle *h, int T);
 int neighbor_list_build(cr_handle *h, double r_list, int *d_count, int64_t *d_head, int *d_list,
                         int64_t capacity, int64_t *total);

@@ -17,13 +17,16 @@
 //    ConductorRigid.cu:549-554, evaluated in FP64 and stored in the operator
 //    precision (the 32x32 blocks of a 4-unit cutoff are only 20-35% full, so the mask
 //    keeps the streamed bytes near one value per interacting pair).  The values of a
-//    pair are stored lane-interleaved: the k-th value of row i at k*32 + i, rows padded
-//    with zeros to the pair's longest row, so that every load is one coalesced warp
-//    load;
+//    pair are stored in row groups: rows in groups of 8 lanes, each group padded with
+//    zeros to its longest row, the k-th value of a row in slot k of its group (8
+//    consecutive values, one 32-byte sector in FP32), so that every load of a warp is
+//    four whole sectors;
 //  * the product y_I = sum_J B_IJ x_J, the pairs of cluster I split over the warps of
-//    one CTA: lane i takes the k-th set bit j of its row, multiplies the k-th value by
-//    x_J[j] fetched with a warp shuffle; the partial sums are added in warp order, so
-//    there are no atomics and the sum order is fixed.
+//    one CTA: lane i takes the k-th set bit j of its row (from the highest column
+//    down), multiplies the k-th value by x_J[j] fetched with a warp shuffle; the
+//    partial sums are added in warp order, so there are no atomics and the sum order
+//    is fixed.  An alternative product streams the values through shared memory with
+//    bulk copies (pair_stream_kernel, CR_REALSPACE_STREAM).
 //
 // The force pass (once per solve) evaluates the gradient table on the fly over the same
 // cluster pairs in FP64.
@@ -182,8 +185,43 @@ __device__ __forceinline__ double dist2_exact(const double4 &a, const double4 &b
     return __dadd_rn(__dadd_rn(__dmul_rn(e[0], e[0]), __dmul_rn(e[1], e[1])), __dmul_rn(e[2], e[2]));
 }
 
+#ifndef CR_RS_GROUP
+#define CR_RS_GROUP 8
+#endif
+// Stored layout of one cluster pair's values: its 32 rows in groups of RG lanes; group g
+// holds rows_g slots (its longest row) of RG values, the k-th value of row i at
+// off_g + k*RG + (i mod RG), the groups one after the other.  RG = 32 is the plain
+// lane-interleaved layout (one 128-byte line per FP32 slot); smaller groups pad less.
+constexpr int RG = CR_RS_GROUP;
+static_assert(RG == 8 || RG == 16 || RG == 32, "row group of 8, 16 or 32 lanes");
+
+struct RowGroup {
+    int rows;   // slots of this lane's group
+    int off;    // position of this lane's slot 0 within the pair's values
+    int total;  // stored slots of the pair
+};
+
+__device__ __forceinline__ RowGroup row_group(unsigned m, int lane) {
+    if (RG == CS) {
+        const int rows = (int)__reduce_max_sync(0xffffffffu, (unsigned)__popc(m));
+        return RowGroup{rows, lane, rows * CS};
+    }
+    int rg = __popc(m);
+#pragma unroll
+    for (int o = 1; o < RG; o <<= 1) rg = max(rg, __shfl_xor_sync(0xffffffffu, rg, o));
+    RowGroup g{rg, lane & (RG - 1), 0};
+#pragma unroll
+    for (int k = 0; k < CS / RG; ++k) {
+        const int sz = __shfl_sync(0xffffffffu, rg, k * RG) * RG;
+        if (k < lane / RG) g.off += sz;
+        g.total += sz;
+    }
+    return g;
+}
+
 // Bit masks of the in-range bead pairs of every cluster pair (row i = bead i of I,
-// bit j = bead j of J) and the stored slots of the pair (32 x its longest row).
+// bit j = bead j of J) and the stored slots of the pair (per group of RG rows, RG times
+// the group's longest row).
 // The test runs on the FP32 copies of the positions; only a pair whose FP32 squared
 // distance lies within `band` of rc^2 (or below 2 dr^2 + band) is decided again in FP64,
 // exactly as the oracle decides it.  `band` is ten times a bound on the FP32 error of
@@ -229,13 +267,10 @@ __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_
         }
     }
     masks[p * CS + lane] = m;
-    int n = __popc(m), tot = n;
-    for (int o = 16; o > 0; o >>= 1) {
-        n = max(n, __shfl_xor_sync(0xffffffffu, n, o));
-        tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    }
+    const int stored = row_group(m, lane).total;
+    const int tot = (int)__reduce_add_sync(0xffffffffu, (unsigned)__popc(m));
     if (lane == 0) {
-        nnz[p] = n * CS;  // stored slots: longest row times 32 lanes
+        nnz[p] = stored;
         atomicAdd(bits, (unsigned long long)tot);
         // offset of the cluster centres under the minimum image, and whether the bead
         // offsets then need no further image: rc + 2 (e_I + e_J) < L/2 along every axis
@@ -248,24 +283,32 @@ __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_
     }
 }
 
-__device__ __forceinline__ int warp_exclusive_scan(int v, int lane) {
-    int incl = v;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    return incl - v;
+// The stored values of a row, and every product that must reproduce their sums, walk the
+// row's set bits from the highest column down: the position of the highest set bit is
+// one `bfind` (0xffffffff for an empty row, which a shuffle reads as lane 31 against a
+// zero value), and clearing it is one mask of the bits below it (`bmsk.clamp` of width
+// 0xffffffff keeps every bit, so an empty row stays empty).
+__device__ __forceinline__ int top_bit(unsigned m) {
+    int j;
+    asm("bfind.u32 %0, %1;" : "=r"(j) : "r"(m));
+    return j;
+}
+__device__ __forceinline__ unsigned below_bit(unsigned m, int j) {
+    unsigned k;
+    asm("bmsk.clamp.b32 %0, 0, %1;" : "=r"(k) : "r"(j));
+    return m & k;
 }
 
-// Values T(d_ij) of the set mask bits in the operator precision, lane-interleaved:
-// the k-th set bit of row i at voff + k*32 + i, zeros after the row's last bit.
+// Values T(d_ij) of the set mask bits in the operator precision, in the row-group
+// layout: the k-th set bit of row i, counted from the highest column down, in slot k of
+// the row, zeros after the row's last bit up to its group's longest row.
 // With R2 = double (and R = float) one pass writes both precisions' values.
 template <typename R, typename R2 = void>
 __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
                                    const int *__restrict__ members, const double4 *__restrict__ pos,
                                    const double2 *__restrict__ tab, RSBuild c, const unsigned *__restrict__ masks,
-                                   const long long *__restrict__ voff, const int *__restrict__ slots,
-                                   R *__restrict__ vals, double *__restrict__ vals2 = nullptr) {
+                                   const long long *__restrict__ voff, R *__restrict__ vals,
+                                   double *__restrict__ vals2 = nullptr) {
     constexpr bool BOTH = std::is_same<R2, double>::value;
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -276,16 +319,17 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
     const double4 pi = bi >= 0 ? pos[bi] : make_double4(0, 0, 0, 0);
     const double4 pjl = bj >= 0 ? pos[bj] : make_double4(0, 0, 0, 0);
     const unsigned m = masks[p * CS + lane];
-    R *out = vals + voff[p] + lane;
-    double *out2 = BOTH ? vals2 + voff[p] + lane : nullptr;
-    // lane i walks its own set bits (the k-th bit j at step k), fetching bead j's position
-    // from lane j; lanes past their last bit write the zero padding of the slot
-    const int rows = slots[p] / CS;
+    const RowGroup g = row_group(m, lane);
+    R *out = vals + voff[p] + g.off;
+    double *out2 = BOTH ? vals2 + voff[p] + g.off : nullptr;
+    // lane i walks its own set bits from the top (the k-th bit j at step k), fetching bead
+    // j's position from lane j; lanes past their last bit write the zero padding of the slot
+    const int rows = (int)__reduce_max_sync(0xffffffffu, (unsigned)g.rows);
     unsigned mm = m;
     for (int k = 0; k < rows; ++k) {
         const bool has = mm != 0;
-        const int j = has ? __ffs(mm) - 1 : 0;
-        mm &= mm - 1;
+        const int j = top_bit(mm) & 31;
+        mm = below_bit(mm, j);
         const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
         const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
         const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
@@ -297,8 +341,10 @@ __global__ void pair_values_kernel(long long npairs, const int *__restrict__ pai
             const double d2 = dx * dx + dy * dy + dz * dz;
             t = table_lerp64(tab, c, d2 * rsqrt64(d2));
         }
-        out[(size_t)k * CS] = (R)t;
-        if (BOTH) out2[(size_t)k * CS] = t;
+        if (k < g.rows) {
+            out[(size_t)k * RG] = (R)t;
+            if (BOTH) out2[(size_t)k * RG] = t;
+        }
     }
 }
 
@@ -316,8 +362,8 @@ __global__ void gather_cluster_kernel(int n, const int *__restrict__ members, co
 // y_I = sum_J B_IJ x_J for cluster I (one CTA of W warps), combined with the wave-space
 // part and the self term: out_i = Phi_body(i) - (phik_i + self q_i + y_i), or the bare
 // sum when phi_body is NULL.  Warp w takes pairs w, w+W, ...; lane i consumes the set
-// bits of its mask row in order, the k-th against the coalesced load of slot k, with
-// x_J[j] from a shuffle.  Up to U slots are loaded before they are used; the next
+// bits of its mask row from the top, the k-th against the coalesced load of slot k, with
+// x_J[j] from a shuffle (per slot: load, bfind, bmsk, and, shuffle, multiply-add).  Up to U slots are loaded before they are used; the next
 // pair's metadata is fetched while the current one is summed.  The W partial sums are
 // added in warp order, so the result does not depend on scheduling.
 // FP32: six CTAs per SM (at most 40 registers; 48 warps of loads in flight, 0.864 ->
@@ -338,47 +384,67 @@ __global__ void __launch_bounds__(W * 32, sizeof(R) == 4 ? 6 : 1) pair_spmv_kern
     __shared__ R part[W][CS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int I = blockIdx.x;
-    R yI = 0;
+    R yI = 0, yI2 = 0;  // FP32: odd slots into a second sum (half the dependent-add chain)
     const long long h0 = head[I];
     const int n = count[I];
-    int J = 0, rows = 0;
+    int J = 0;
     unsigned m0 = 0;
     long long off = 0;
     R xJ = 0;
+    long long offn = 0;  // values offset and stored slots of the pair after the next one
+    int sln = 0;
     if (w < n) {
         J = pair_j[h0 + w];
         m0 = masks[(h0 + w) * CS + lane];
         off = voff[h0 + w];
-        rows = slots[h0 + w] / CS;
         xJ = qc[J * CS + lane];
     }
+    if (w + W < n) {
+        offn = voff[h0 + w + W];
+        sln = slots[h0 + w + W];
+    }
     for (int k = w; k < n; k += W) {
-        const R *v = vals + off + lane;
         unsigned m = m0;
+        const RowGroup g = row_group(m, lane);
+        const R *v = vals + off + g.off;
+        const int rcur = RG == CS ? g.rows : (int)__reduce_max_sync(0xffffffffu, (unsigned)g.rows);
         const R xcur = xJ;
-        const int rcur = rows;
         if (k + W < n) {
+            // the next pair's values into L2 while this pair is summed (one bulk prefetch;
+            // offsets and sizes are multiples of 32 bytes)
+            if (lane == 0 && sln > 0)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(vals + offn),
+                             "r"((unsigned)(sln * sizeof(R)))
+                             : "memory");
             const long long p1 = h0 + k + W;
             J = pair_j[p1];
             m0 = masks[p1 * CS + lane];
-            off = voff[p1];
-            rows = slots[p1] / CS;
+            off = offn;
             xJ = qc[J * CS + lane];
+            if (k + 2 * W < n) {
+                offn = voff[p1 + W];
+                sln = slots[p1 + W];
+            }
         }
-        const int own = __popc(m);  // slots past the end of this lane's row hold zeros: skip them
+        // slots past the end of a lane's row hold zeros and its walk then reads lane 31
         for (int base = 0; base < rcur; base += U) {
             R t[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) t[u] = base + u < own ? __ldg(v + (size_t)(base + u) * CS) : (R)0;
+            for (int u = 0; u < U; ++u) t[u] = base + u < g.rows ? __ldg(v + (size_t)(base + u) * RG) : (R)0;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int j = m ? __ffs(m) - 1 : 0;
-                m &= m - 1;
-                yI += t[u] * __shfl_sync(0xffffffffu, xcur, j);
+                const int j = top_bit(m);
+                m = below_bit(m, j);
+                const R xj = __shfl_sync(0xffffffffu, xcur, j);
+                if (sizeof(R) == 4 && (u & 1)) {
+                    yI2 += t[u] * xj;
+                } else {
+                    yI += t[u] * xj;
+                }
             }
         }
     }
-    part[w][lane] = yI;
+    part[w][lane] = yI + yI2;
     __syncthreads();
     if (w == 0) {
         R tot = 0;
@@ -389,6 +455,339 @@ __global__ void __launch_bounds__(W * 32, sizeof(R) == 4 ? 6 : 1) pair_spmv_kern
             const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)tot;
             out[bi] = phi_body ? phi_body[body[bi]] - total : total;
         }
+    }
+}
+
+// ---- streamed product: a bulk-copy producer warp per CTA ------------------------------
+//
+// The direct product above keeps at most U slots of loads in flight per warp, as many as
+// its registers hold.  Here a CTA owns a contiguous range of clusters (balanced by
+// stored bytes) and one producer thread streams the range's values through a ring of
+// shared-memory stages with cp.async.bulk (no multicast), each stage's completion
+// signalled on its mbarrier by the byte count; the consumer warps read the values from
+// shared memory.  A stage holds one chunk: the pairs whose values start in one 8 KB
+// window of the range, so a chunk never splits a pair and spans at most 8 KB plus one
+// pair.  Every consumer warp waits for every chunk in order and releases it (one arrival
+// per warp on the stage's empty barrier) once its later pairs all start in later chunks;
+// the warp holding the oldest chunk never waits on another warp, so the ring always
+// moves.  The pairs of a cluster go to the consumer warps in turn and each warp adds its
+// partial sums of a cluster to the cluster's 32 sums with one coalesced atomic add
+// (stream_finish_kernel then forms the rows and clears the sums).  Every wait is
+// bounded: a wait that runs out (or finds that another warp's did) sets the abort flag
+// and the error word; the consumers then skip the remaining pairs, and the producer
+// stops issuing and, as always before it returns, waits for its copies in flight.
+constexpr int kStreamStages = 4;
+constexpr int kStreamChunk = 16384;  // bytes per stage
+constexpr int kStreamShift = 13;     // 8 KB windows
+constexpr int kStreamWarps = 8;      // consumer warps per CTA, plus one producer warp
+constexpr int kStreamCtasPerSm = 3;
+static_assert((1 << kStreamShift) + CS * CS * 8 <= kStreamChunk, "a stage holds a window plus one FP64 pair");
+constexpr long long kDrainLimit = 1LL << 33;  // cycles; copies in flight always complete
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool bar_ready(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Wait for phase `parity` of the barrier; false after `limit` cycles, or at once when
+// `abort` is set (null: no abort check).
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, long long limit, const volatile int *abort) {
+    const long long t0 = clock64();
+    while (!bar_ready(bar, parity)) {
+        if ((abort && *abort) || clock64() - t0 > limit) return false;
+    }
+    return true;
+}
+
+template <typename R, int NW>
+__global__ void __launch_bounds__((NW + 1) * 32, kStreamCtasPerSm) pair_stream_kernel(
+    int nclus, const int *__restrict__ cl0, const long long *__restrict__ cbase,
+    const long long *__restrict__ cstart, long long total_vals, const long long *__restrict__ head,
+    const int *__restrict__ count, const int *__restrict__ pair_j, const unsigned *__restrict__ masks,
+    const long long *__restrict__ voff, const R *__restrict__ vals, const R *__restrict__ qc,
+    R *__restrict__ ysum, long long limit, int withhold, int *__restrict__ err) {
+    constexpr int S = kStreamStages, U = 16;
+    constexpr long long E = sizeof(R);
+    extern __shared__ __align__(128) unsigned char ring[];  // S stages of kStreamChunk bytes
+    __shared__ __align__(8) uint64_t full[S], empty[S];
+    __shared__ long long cst[S];  // absolute first byte of the chunk held by each stage
+    __shared__ int abort_word;
+    volatile int *abort_flag = &abort_word;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int I0 = cl0[blockIdx.x], I1 = cl0[blockIdx.x + 1];
+    if (I0 >= I1) return;  // no clusters: the whole CTA leaves before any barrier
+    const long long nch = cbase[blockIdx.x + 1] - cbase[blockIdx.x];
+    const long long *cs = cstart + cbase[blockIdx.x];
+    const long long B0 = voff[head[I0]] * E;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[s])), "r"(NW) : "memory");
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (w == NW) {  // producer warp: lane 0 issues, the warp fetches chunk bounds 32 at a time
+        if (withhold) return;  // a test of the bounded waits: nothing is issued, nothing arrives
+        const long long B1 = (I1 < nclus ? voff[head[I1]] : total_vals) * E;
+        long long issued = 0;
+        bool ok = true;
+        for (long long base = 0; base < nch && ok; base += 32) {
+            const long long cl = base + lane;
+            const long long lo_l = cl < nch ? cs[cl] : 0;
+            const long long hi_l = cl + 1 < nch ? cs[cl + 1] : B1;
+            const int nb = (int)min(32LL, nch - base);
+            for (int l = 0; l < nb && ok; ++l) {
+                const long long c = base + l;
+                const long long lo = __shfl_sync(0xffffffffu, lo_l, l);
+                const long long hi = __shfl_sync(0xffffffffu, hi_l, l);
+                const int s = (int)(c % S);
+                if (lane == 0) {
+                    if (c >= S)
+                        ok = bar_wait(smem_addr(&empty[s]), (uint32_t)((c / S - 1) & 1), limit, abort_flag);
+                    if (ok) {
+                        cst[s] = lo;
+                        const uint32_t bytes = (uint32_t)(hi - lo);
+                        const uint32_t fb = smem_addr(&full[s]);
+                        if (bytes > 0) {
+                            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(bytes)
+                                         : "memory");
+                            asm volatile(
+                                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                                "[%3];" ::"r"(smem_addr(ring + (size_t)s * kStreamChunk)),
+                                "l"(reinterpret_cast<const unsigned char *>(vals) + lo), "r"(bytes), "r"(fb)
+                                : "memory");
+                        } else {
+                            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(fb) : "memory");
+                        }
+                        ++issued;
+                    } else if (!*abort_flag) {
+                        *abort_flag = 1;
+                        atomicExch(err, 1);
+                    }
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+            }
+        }
+        if (lane == 0)  // the copies of the last stages may still be in flight
+            for (long long c = issued > S ? issued - S : 0; c < issued; ++c)
+                bar_wait(smem_addr(&full[c % S]), (uint32_t)((c / S) & 1), kDrainLimit, nullptr);
+        return;
+    }
+
+    // consumer warps: each waits for every chunk in order and releases every chunk below
+    // the one holding its current pair as soon as it has waited for it (a warp never holds
+    // a chunk while it waits for a later one, so the warp with the oldest chunk can always
+    // go on)
+    long long waited = 0, released = 0;  // chunks waited for / released by this warp
+    bool ok = true;                      // warp-uniform
+    auto release_below = [&](long long c) {
+        __syncwarp();
+        while (released < c && released < waited) {
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[released % S]))
+                             : "memory");
+            ++released;
+        }
+    };
+    // wait for the chunks up to c, releasing each one below `keep` once waited for
+    auto advance = [&](long long c, long long keep) {
+        while (ok && waited <= c) {
+            const int s = (int)(waited % S);
+            bool r = bar_wait(smem_addr(&full[s]), (uint32_t)((waited / S) & 1), limit, abort_flag);
+            r = __all_sync(0xffffffffu, r);
+            if (!r) {
+                ok = false;
+                if (lane == 0 && !*abort_flag) {
+                    *abort_flag = 1;
+                    atomicExch(err, 1);
+                }
+                break;
+            }
+            ++waited;
+            release_below(min(keep, waited));
+        }
+        release_below(min(keep, waited));
+    };
+
+    long long h0 = head[I0];
+    int n = count[I0];
+    int Jc = 0;
+    unsigned mc = 0;
+    long long oc = 0;
+    R xc = 0;
+    if (w < n) {
+        Jc = pair_j[h0 + w];
+        mc = masks[(h0 + w) * CS + lane];
+        oc = voff[h0 + w];
+        xc = qc[Jc * CS + lane];
+    }
+    for (int I = I0; I < I1; ++I) {
+        const long long h0n = I + 1 < I1 ? head[I + 1] : 0;
+        const int nn = I + 1 < I1 ? count[I + 1] : 0;
+        R yI = 0, yI2 = 0;  // FP32: odd slots into a second sum (half the dependent-add chain)
+        for (int k = w; k < n; k += NW) {
+            // the next pair of this warp (in this cluster or the next) while this one is summed
+            long long pn = -1;
+            if (k + NW < n)
+                pn = h0 + k + NW;
+            else if (w < nn)
+                pn = h0n + w;
+            int Jn = 0;
+            unsigned mn = 0;
+            long long on = 0;
+            R xn = 0;
+            if (pn >= 0) {
+                Jn = pair_j[pn];
+                mn = masks[pn * CS + lane];
+                on = voff[pn];
+                xn = qc[Jn * CS + lane];
+            }
+            if (ok) {
+                const long long vb = oc * E;
+                const long long c = min((vb - B0) >> kStreamShift, nch - 1);
+                advance(c, c);
+                if (ok) {
+                    const int s = (int)(c % S);
+                    unsigned m = mc;
+                    const RowGroup g = row_group(m, lane);
+                    const int rcur = RG == CS ? g.rows : (int)__reduce_max_sync(0xffffffffu, (unsigned)g.rows);
+                    const R *v = reinterpret_cast<const R *>(ring + (size_t)s * kStreamChunk + (vb - cst[s])) + g.off;
+                    for (int base = 0; base < rcur; base += U) {
+                        R t[U];
+#pragma unroll
+                        for (int u = 0; u < U; ++u) t[u] = base + u < g.rows ? v[(base + u) * RG] : (R)0;
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            const int j = top_bit(m);
+                            m = below_bit(m, j);
+                            const R xj = __shfl_sync(0xffffffffu, xc, j);
+                            if (sizeof(R) == 4 && (u & 1)) {
+                                yI2 += t[u] * xj;
+                            } else {
+                                yI += t[u] * xj;
+                            }
+                        }
+                    }
+                }
+            }
+            Jc = Jn;
+            mc = mn;
+            oc = on;
+            xc = xn;
+        }
+        if (w < n) atomicAdd(&ysum[(size_t)I * CS + lane], yI + yI2);  // this warp's part of cluster I
+        if (w >= n && w < nn) {  // no pair of this warp in cluster I: fetch its first of the next
+            Jc = pair_j[h0n + w];
+            mc = masks[(h0n + w) * CS + lane];
+            oc = voff[h0n + w];
+            xc = qc[Jc * CS + lane];
+        }
+        h0 = h0n;
+        n = nn;
+    }
+    // every chunk is waited for and released, so that the producer never waits in vain
+    advance(nch - 1, nch);
+}
+
+// out_i = Phi_body(i) - (phik_i + self q_i + y_i) (or the bare sum when phi_body is NULL)
+// from the streamed product's sums y in cluster order, which are cleared for the next one.
+template <typename R>
+__global__ void stream_finish_kernel(int nslots, const int *__restrict__ members, R *__restrict__ ysum,
+                                     const R *__restrict__ q, const R *__restrict__ phik, double selfc,
+                                     const double *__restrict__ phi_body, const uint32_t *__restrict__ body,
+                                     double *__restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nslots) return;
+    const int bi = members[k];
+    const R y = ysum[k];
+    ysum[k] = (R)0;
+    if (bi < 0) return;
+    const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)y;
+    out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+}
+
+// CTA b of G takes the clusters whose first stored value lies in [T b/G, T (b+1)/G) of the
+// T stored values (cluster boundaries), and one chunk per 8 KB window of its bytes (at
+// least one).  One block of G <= 1024 threads.
+__global__ void __launch_bounds__(1024) stream_split_kernel(int nclus, int G, const long long *__restrict__ head,
+                                    const long long *__restrict__ voff, long long total_vals, int elem,
+                                    int *__restrict__ cl0, long long *__restrict__ cbase) {
+    typedef cub::BlockScan<long long, 1024> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ int sc[1025];
+    const int b = threadIdx.x;
+    if (b < G) {
+        const long long target = total_vals * b / G;
+        int lo = 0, hi = nclus;  // first cluster whose first value is at or after target
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (voff[head[mid]] >= target)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        sc[b] = b == 0 ? 0 : lo;
+    }
+    if (b == 0) sc[G] = nclus;
+    __syncthreads();
+    long long nchunks = 0;
+    if (b < G) {
+        const int a = sc[b], e = sc[b + 1];
+        if (a < e) {
+            const long long v0 = voff[head[a]];
+            const long long v1 = e < nclus ? voff[head[e]] : total_vals;
+            const long long bytes = (v1 - v0) * elem;
+            nchunks = bytes > 0 ? ((bytes - 1) >> kStreamShift) + 1 : 1;
+        }
+        cl0[b] = sc[b];
+    }
+    if (b == 0) cl0[G] = nclus;
+    long long off = 0, tot = 0;
+    Scan(tmp).ExclusiveSum(nchunks, off, tot);
+    if (b < G) cbase[b] = off;
+    if (b == 0) cbase[G] = tot;
+}
+
+// First byte of every chunk: the first pair whose values start in the chunk's window
+// (a window without a start gets the next start, i.e. an empty chunk; windows after the
+// range's last start end at the range's end).
+__global__ void stream_chunks_kernel(long long npairs, int G, int nclus, const int *__restrict__ pair_i,
+                                     const int *__restrict__ cl0, const long long *__restrict__ cbase,
+                                     const long long *__restrict__ head, const long long *__restrict__ voff,
+                                     long long total_vals, int elem, long long *__restrict__ cstart) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const int I = pair_i[p];
+    int lo = 0, hi = G - 1;  // the last CTA whose first cluster is at or before I
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (cl0[mid] <= I)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int b = lo;
+    const long long first = head[cl0[b]];
+    const long long last = (cl0[b + 1] < nclus ? head[cl0[b + 1]] : npairs) - 1;
+    const long long B0 = voff[first] * elem;
+    const long long nch = cbase[b + 1] - cbase[b];
+    const long long k = min((voff[p] * elem - B0) >> kStreamShift, nch - 1);
+    const long long kp = p == first ? -1 : min((voff[p - 1] * elem - B0) >> kStreamShift, nch - 1);
+    for (long long kk = kp + 1; kk <= k; ++kk) cstart[cbase[b] + kk] = voff[p] * elem;
+    if (p == last) {
+        const long long B1 = (cl0[b + 1] < nclus ? voff[head[cl0[b + 1]]] : total_vals) * elem;
+        for (long long kk = k + 1; kk < nch; ++kk) cstart[cbase[b] + kk] = B1;
     }
 }
 
@@ -554,8 +953,8 @@ __global__ void __launch_bounds__(W * 32) pair_otf64_kernel(const long long *__r
         unsigned mm = m;
         for (unsigned t = 0; t < steps; ++t) {
             const bool has = mm != 0;
-            const int j = has ? __ffs(mm) - 1 : 0;
-            mm &= mm - 1;
+            const int j = top_bit(mm) & 31;
+            mm = below_bit(mm, j);
             const double xj = __shfl_sync(0xffffffffu, pjl.x, j);
             const double yj = __shfl_sync(0xffffffffu, pjl.y, j);
             const double zj = __shfl_sync(0xffffffffu, pjl.z, j);
@@ -746,6 +1145,9 @@ RSBuild rs_build(const cr_handle *h) {
     return c;
 }
 
+template <typename R> R *ysum_of(RealSpace &r);
+template <> float *ysum_of<float>(RealSpace &r) { return r.ysum32; }
+template <> double *ysum_of<double>(RealSpace &r) { return r.ysum64; }
 template <typename R> R *acc_of(RealSpace &r);
 template <> float *acc_of<float>(RealSpace &r) { return r.acc32; }
 template <> double *acc_of<double>(RealSpace &r) { return r.acc64; }
@@ -758,6 +1160,43 @@ template <> bool &valid_of<double>(RealSpace &r) { return r.valid64; }
 template <typename R> long long &cap_of(RealSpace &r);
 template <> long long &cap_of<float>(RealSpace &r) { return r.blocks32_cap; }
 template <> long long &cap_of<double>(RealSpace &r) { return r.blocks64_cap; }
+
+template <typename R> RealSpace::StreamPlan &plan_of(RealSpace &r);
+template <> RealSpace::StreamPlan &plan_of<float>(RealSpace &r) { return r.plan32; }
+template <> RealSpace::StreamPlan &plan_of<double>(RealSpace &r) { return r.plan64; }
+
+bool streamed(const cr_handle *h) { return (h->rs_onfly & CR_REALSPACE_STREAM) != 0; }
+// Cluster ranges and chunk starts of the streamed product of precision R (once per
+// geometry, after the values): kStreamCtasPerSm CTAs per multiprocessor, at most one per
+// cluster and at most 1024.
+template <typename R> int stream_plan(cr_handle *h) {
+    RealSpace &r = h->rs;
+    RealSpace::StreamPlan &P = plan_of<R>(r);
+    const int G = std::max(1, std::min(std::min(kStreamCtasPerSm * h->n_sm, r.nclus), 1024));
+    if (!P.cl0) {
+        CR_TRY(dalloc(h, &P.cl0, 1025));
+        CR_TRY(dalloc(h, &P.cbase, 1025));
+    }
+    const long long need = ((r.nnz * (long long)sizeof(R)) >> kStreamShift) + G + 1;
+    if (need > P.cap) {
+        const long long cap = need + need / 8;
+        CR_TRY(dalloc(h, &P.cstart, (size_t)cap));
+        P.cap = cap;
+    }
+    // the ring's shared memory (64 KB) is above the default limit; set once per precision,
+    // here, outside any stream capture
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        pair_stream_kernel<R, kStreamWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStreamStages * kStreamChunk);
+    CR_CUDA(h, attr);
+    stream_split_kernel<<<1, 1024, 0, h->stream>>>(r.nclus, G, r.head, r.voff, r.nnz, (int)sizeof(R), P.cl0, P.cbase);
+    CR_LAUNCH(h, "stream_split_kernel");
+    stream_chunks_kernel<<<blocks_for(r.npairs, 256), 256, 0, h->stream>>>(
+        r.npairs, G, r.nclus, r.pair_i, P.cl0, P.cbase, r.head, r.voff, r.nnz, (int)sizeof(R), P.cstart);
+    CR_LAUNCH(h, "stream_chunks_kernel");
+    P.ctas = G;
+    P.valid = true;
+    return CR_OK;
+}
 
 template <typename R> int realspace_reserve(cr_handle *h) {
     RealSpace &r = h->rs;
@@ -784,23 +1223,29 @@ template <typename R> bool onfly(const cr_handle *h) {
 
 template <typename R> int realspace_blocks(cr_handle *h) {
     RealSpace &r = h->rs;
-    if (valid_of<R>(r) || h->N == 0 || onfly<R>(h)) return CR_OK;
+    if (h->N == 0 || onfly<R>(h)) return CR_OK;
+    if (valid_of<R>(r)) return streamed(h) && !plan_of<R>(r).valid ? stream_plan<R>(h) : CR_OK;
     if (h->user.precision != CR_FP64 && !r.valid32 && !r.valid64 && !onfly<float>(h) && !onfly<double>(h)) {
         CR_TRY(realspace_reserve<float>(h));
         CR_TRY(realspace_reserve<double>(h));
         pair_values_kernel<float, double><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
             r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.voff,
-            r.nnz_pair, r.vals32, r.vals64);
+            r.vals32, r.vals64);
         CR_LAUNCH(h, "pair_values_kernel");
         r.valid32 = r.valid64 = true;
+        if (streamed(h)) {
+            CR_TRY(stream_plan<float>(h));
+            CR_TRY(stream_plan<double>(h));
+        }
         return CR_OK;
     }
     CR_TRY(realspace_reserve<R>(h));
     pair_values_kernel<R><<<blocks_for(r.npairs * 32, 256), 256, 0, h->stream>>>(
-        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.voff, r.nnz_pair,
+        r.npairs, r.pair_i, r.pair_j, r.members, h->m64.pos, h->m64.phiq, rs_build(h), r.masks, r.voff,
         blocks_of<R>(r));
     CR_LAUNCH(h, "pair_values_kernel");
     valid_of<R>(r) = true;
+    if (streamed(h)) CR_TRY(stream_plan<R>(h));
     return CR_OK;
 }
 
@@ -828,10 +1273,19 @@ void realspace_free(cr_handle *h) {
     dfree(&r.voff);
     dfree(&r.acc32);
     dfree(&r.acc64);
+    dfree(&r.ysum32);
+    dfree(&r.ysum64);
     dfree(&r.freal);
     dfree(&r.bits);
     dfree(&r.boff);
     dfree(&r.pshift);
+    dfree(&r.err);
+    for (RealSpace::StreamPlan *P : {&r.plan32, &r.plan64}) {
+        dfree(&P->cl0);
+        dfree(&P->cbase);
+        dfree(&P->cstart);
+        *P = RealSpace::StreamPlan{};
+    }
     r.pair_cap = 0;
     r.nnz = 0;
     r.blocks32_cap = r.blocks64_cap = 0;
@@ -853,9 +1307,15 @@ int realspace_alloc(cr_handle *h) {
     CR_TRY(dalloc(h, &r.sorted, (size_t)std::max(h->N, 1)));
     CR_TRY(dalloc(h, &r.acc32, nc * CS));
     CR_TRY(dalloc(h, &r.acc64, nc * CS));
+    CR_TRY(dalloc(h, &r.ysum32, nc * CS));
+    CR_TRY(dalloc(h, &r.ysum64, nc * CS));
+    CR_CUDA(h, cudaMemsetAsync(r.ysum32, 0, nc * CS * sizeof(float), h->stream));
+    CR_CUDA(h, cudaMemsetAsync(r.ysum64, 0, nc * CS * sizeof(double), h->stream));
     CR_TRY(dalloc(h, &r.freal, 3 * (size_t)std::max(h->N, 1)));
     CR_TRY(dalloc(h, &r.bits, 1));
     CR_TRY(dalloc(h, &r.boff, nc * CS));
+    CR_TRY(dalloc(h, &r.err, 1));
+    CR_CUDA(h, cudaMemsetAsync(r.err, 0, sizeof(int), h->stream));
     return CR_OK;
 }
 
@@ -865,6 +1325,7 @@ int realspace_build(cr_handle *h) {
     RealSpace &r = h->rs;
     const int N = h->N;
     r.valid32 = r.valid64 = false;
+    r.plan32.valid = r.plan64.valid = false;
     if (N == 0) return CR_OK;
     cudaStream_t s = h->stream;
     const RSBuild c = rs_build(h);
@@ -970,6 +1431,21 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
         }
         return CR_OK;
     }
+    if (streamed(h)) {
+        const RealSpace::StreamPlan &P = plan_of<R>(r);
+        constexpr int NW = kStreamWarps;
+        const size_t smem = (size_t)kStreamStages * kStreamChunk;
+        R *ysum = ysum_of<R>(r);
+        pair_stream_kernel<R, NW><<<P.ctas, (NW + 1) * 32, smem, h->stream>>>(
+            r.nclus, P.cl0, P.cbase, P.cstart, r.nnz, r.head, r.count, r.pair_j, r.masks, r.voff, blocks_of<R>(r),
+            qc, ysum, r.wait_limit, r.withhold_next, r.err);
+        r.withhold_next = 0;
+        CR_LAUNCH(h, "pair_stream_kernel");
+        stream_finish_kernel<R><<<blocks_for((long)r.nclus * CS, 256), 256, 0, h->stream>>>(
+            r.nclus * CS, r.members, ysum, m.q, m.phi, h->d.selfcoeff, phi_body, h->d_body, out);
+        CR_LAUNCH(h, "stream_finish_kernel");
+        return CR_OK;
+    }
     pair_spmv_kernel<R, W, 16><<<r.nclus, W * 32, 0, h->stream>>>(
         r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, m.phi,
         h->d.selfcoeff, phi_body, h->d_body, out);
@@ -990,6 +1466,17 @@ template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, cons
                                                                        h->field[2], r.freal, force_out);
     CR_LAUNCH(h, "force_combine_kernel");
     return CR_OK;
+}
+
+int realspace_check(cr_handle *h) {
+    RealSpace &r = h->rs;
+    if (!r.err) return CR_OK;
+    int e = 0;
+    CR_CUDA(h, cudaMemcpyAsync(&e, r.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CR_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (e == 0) return CR_OK;
+    CR_CUDA(h, cudaMemsetAsync(r.err, 0, sizeof(int), h->stream));
+    return fail(h, CR_TIMEOUT, "real-space product: a bounded device wait ran out");
 }
 
 int real_space_virial(cr_handle *h, const double *q64, double *out) {

@@ -67,8 +67,18 @@ class Handle:
 
     def set_realspace(self, flags: int):
         """CR_REALSPACE_ONFLY32 / CR_REALSPACE_ONFLY64: evaluate the real-space kernel values
-        of the FP32 / FP64 products on the fly instead of storing them per geometry."""
+        of the FP32 / FP64 products on the fly instead of storing them per geometry;
+        CR_REALSPACE_STREAM: stream the stored values through shared memory with bulk
+        copies (one producer warp per CTA) instead of reading them straight from device
+        memory."""
         self._check(_lib.lib().cr_set_realspace(self.h, int(flags)), "cr_set_realspace")
+
+    def set_wait_limit(self, cycles: int = 0, withhold_next: bool = False):
+        """Limit of each bounded device wait of the streamed real-space product (SM clock
+        cycles; <= 0 restores the default of about a second).  withhold_next: the next
+        streamed product issues none of its copies, so its waits run out (a test)."""
+        self._check(_lib.lib().cr_set_wait_limit(self.h, C.c_longlong(int(cycles)), int(bool(withhold_next))),
+                    "cr_set_wait_limit")
 
     def set_correction(self, net, weight: float = 1.0):
         """Learned preconditioner correction from `net` (a learned.Network; None removes it)."""

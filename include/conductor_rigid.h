@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define CR_ABI_VERSION 4
+#define CR_ABI_VERSION 5
 
 typedef enum {
     CR_OK = 0,
@@ -164,12 +164,22 @@ int cr_set_graphs(cr_handle *h, int enable);
  * found once (32-bead clusters, per cluster pair a 32 x 32 bit mask); the kernel values
  * T(d) of those pairs are then either stored once per geometry and streamed by every
  * product, or evaluated again in every product from the positions (the table in shared
- * memory in FP32).  flags: CR_REALSPACE_ONFLY32 evaluates the FP32 products on the fly,
- * CR_REALSPACE_ONFLY64 the FP64 products (bit-identical to the stored FP64 values'
- * product); 0 stores both.  Takes effect at the next product. */
+ * memory in FP32).  Stored values are read by one CTA per cluster straight from device
+ * memory (the default) or, with CR_REALSPACE_STREAM, streamed through shared memory by
+ * bulk copies, one producer warp per CTA.  flags: CR_REALSPACE_ONFLY32 evaluates the FP32
+ * products on the fly, CR_REALSPACE_ONFLY64 the FP64 products (bit-identical to the
+ * default stored product); 0 stores both.  Takes effect at the next product. */
 #define CR_REALSPACE_ONFLY32 1
 #define CR_REALSPACE_ONFLY64 2
+#define CR_REALSPACE_STREAM 4
 int cr_set_realspace(cr_handle *h, int flags);
+/* Limit of every bounded device wait of the streamed real-space product
+ * (CR_REALSPACE_STREAM), in SM clock
+ * cycles (<= 0: the default 2^31, about a second).  A wait that runs out ends the
+ * product early; the call that ran it (cr_compute, cr_apply_operator) then returns
+ * CR_TIMEOUT and the handle stays usable.  withhold_next != 0 (a test of the waits):
+ * the next streamed product issues none of its copies, so its waits run out. */
+int cr_set_wait_limit(cr_handle *h, long long cycles, int withhold_next);
 int cr_graph_launches(const cr_handle *h, long long *launches);
 
 /* ---- the step (gpu_ComputeForce, ConductorRigid.cu:1153-1286) ----

@@ -38,7 +38,7 @@ def test_exports_every_declared_symbol(product_lib):
 
 def test_abi_version_and_status(product_lib):
     lib = product_lib.lib()
-    assert lib.cr_abi_version() == 4
+    assert lib.cr_abi_version() == 5
     assert lib.cr_status_string(product_lib.CR_GRID_TOO_LARGE).decode() == "grid too large"
 
 

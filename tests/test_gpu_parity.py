@@ -276,14 +276,15 @@ def test_operator_matches_oracle_other_supports(cuda, product_lib, oracle_lib, s
     h.close()
 
 
-@pytest.mark.parametrize("flags", [0, 1, 2, 3])
+@pytest.mark.parametrize("flags", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("case", ["plain_small", "small_box"])
 def test_realspace_modes_match_oracle(cuda, product_lib, oracle_lib, flags, case):
-    """Stored and on-the-fly real-space values give the oracle's operator, and the FP64
-    on-the-fly product the stored one's (its real-space sum is the same arithmetic in the
-    same order; the spreading's atomic accumulation leaves summation-order differences in
-    the whole operator).  The small box (rc = 0.45 L) takes the per-separation minimum
-    image of the on-the-fly FP32 product."""
+    """Stored (read directly or streamed through shared memory) and on-the-fly real-space
+    values give the oracle's operator, and every FP64 product the directly read one's
+    (the on-the-fly sum is the same arithmetic in the same order, the streamed one adds
+    per-warp sums with atomics; the spreading's atomic accumulation leaves
+    summation-order differences in the whole operator).  The small box
+    (rc = 0.45 L) takes the per-separation minimum image of the on-the-fly FP32 product."""
     import math
 
     from conductorrigid_b200 import systems
@@ -304,7 +305,7 @@ def test_realspace_modes_match_oracle(cuda, product_lib, oracle_lib, flags, case
     assert rel(h.apply_operator(x, product_lib.CR_FP32), ref) < 2e-5
     h.set_realspace(0)
     y64s = h.apply_operator(x)
-    assert rel(y64, y64s.cpu().numpy()) < 1e-13, "FP64 on-the-fly and stored products differ"
+    assert rel(y64, y64s.cpu().numpy()) < 1e-13, "FP64 products of the two modes differ"
     h.close()
 
 
