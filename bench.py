@@ -870,7 +870,8 @@ def main() -> None:
     ap.add_argument("--coarse-cg", type=int, default=0, help="CG steps of the sparse coarse form")
     ap.add_argument("--realspace", type=int, default=0,
                     help="real-space kernel values evaluated on the fly: 1 FP32, 2 FP64, 3 both; 4: stored values "
-                         "streamed through shared memory (default 0: stored, read by one CTA per cluster)")
+                         "streamed through shared memory; 8: real-space product after the wave-space part instead of beside it "
+                         "(default 0: stored, read by one CTA per cluster, concurrent with the wave-space part)")
     ap.add_argument("--batch-threads", type=int, default=16,
                     help="replicas: host threads (one stream each) of the batched solve")
     ap.add_argument("--train-solves", type=int, default=0,

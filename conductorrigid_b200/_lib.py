@@ -32,6 +32,7 @@ PRECISIONS = {"fp64": CR_FP64, "mixed": CR_MIXED, "fp32": CR_FP32}
 CR_REALSPACE_ONFLY32 = 1
 CR_REALSPACE_ONFLY64 = 2
 CR_REALSPACE_STREAM = 4
+CR_REALSPACE_SERIAL = 8
 
 CR_PRECOND_DIAGONAL = 0
 CR_PRECOND_CONDUCTOR = 1

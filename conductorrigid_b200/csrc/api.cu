@@ -235,6 +235,9 @@ int cr_destroy(cr_handle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     else cudaDeviceSynchronize();
     free_all(h);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
@@ -365,7 +368,7 @@ int cr_correction_samples(cr_handle *h, int max_dirs, uint16_t *d_x, float *d_t,
 
 int cr_set_realspace(cr_handle *h, int flags) {
     if (!h) return CR_BAD_PARAM;
-    if (flags & ~(CR_REALSPACE_ONFLY32 | CR_REALSPACE_ONFLY64 | CR_REALSPACE_STREAM))
+    if (flags & ~(CR_REALSPACE_ONFLY32 | CR_REALSPACE_ONFLY64 | CR_REALSPACE_STREAM | CR_REALSPACE_SERIAL))
         return fail(h, CR_BAD_PARAM, "unknown real-space flags");
     if (h->stream) CR_CUDA(h, cudaStreamSynchronize(h->stream));
     h->rs_onfly = flags;

@@ -142,10 +142,32 @@ int precondition(cr_handle *h, const double *x, double *y) {
 }
 
 // MatrixVectorMultiply (ConductorRigid.cu:953-1020): y = [Phi_b - M q ; S q].
+// The wave-space part (spreading, transforms, contraction: L1-, shared-memory- and
+// issue-bound, the mesh L2-resident) and the real-space product (bound by its loads in
+// flight) are independent given the charges, so unless the profiler is on (its marks
+// time one stream) they run side by side: the wave part forks onto the handle's
+// high-priority side stream, the real-space product writes its sums, and after the join
+// rows_combine_kernel adds the wave part and the self term (the arithmetic of the fused
+// form).  In a captured Arnoldi step the fork and join become parallel graph branches.
 template <typename R> static int apply_operator_t(cr_handle *h, MeshBuffers<R> &m, const double *x, double *y) {
     CR_TRY(cast_charges(h, m, x));
-    CR_TRY(wave_potential(h, m));
-    CR_TRY(real_space_apply(h, m, x + h->N, y));
+    if (h->side && !h->prof.on && !(h->rs_onfly & CR_REALSPACE_SERIAL) && h->N > 0) {
+        cudaStream_t main = h->stream;
+        CR_CUDA(h, cudaEventRecord(h->ev_fork, main));
+        CR_CUDA(h, cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+        h->stream = h->side;
+        int st = wave_potential(h, m);
+        if (st == CR_OK) st = check_cuda(h, cudaEventRecord(h->ev_join, h->side), "cudaEventRecord");
+        h->stream = main;
+        CR_TRY(st);
+        const int rs = real_space_apply(h, m, x + h->N, y, true);
+        CR_CUDA(h, cudaStreamWaitEvent(main, h->ev_join, 0));  // joins the branch on every path
+        CR_TRY(rs);
+        CR_TRY(real_space_rows(h, m, x + h->N, y));
+    } else {
+        CR_TRY(wave_potential(h, m));
+        CR_TRY(real_space_apply(h, m, x + h->N, y));
+    }
     CR_TRY(body_sums(h, x, y));
     return CR_OK;
 }

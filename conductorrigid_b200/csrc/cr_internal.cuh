@@ -316,6 +316,10 @@ struct cr_handle {
     // real-space kernel values: CR_REALSPACE_* flags, evaluated on the fly instead of stored
     int rs_onfly = 0;
     int n_sm = 0;                     // multiprocessors of the device
+    // the wave-space part of an operator application runs on `side` (highest stream
+    // priority) while the real-space product runs on `stream`
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     long long geo_gen = 0;
     long long graph_launches = 0;
     // learned guess: caller directions for the next solve [CR_MAX_GUESS_DIRECTIONS][N+B]
@@ -394,7 +398,10 @@ template <typename R> int wave_force(cr_handle *h, MeshBuffers<R> &m);
 template <typename R> int spread_only(cr_handle *h, MeshBuffers<R> &m);
 // Real-space: out_i = Phi_b(i) - (phi_k + self q + sum T q)   (phi_body != NULL)
 //             out_i = phi_k + self q + sum T q               (phi_body == NULL)
-template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out);
+//             out_i = sum T q only (rows_only; real_space_rows then adds the rest)
+template <typename R>
+int real_space_apply(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out, bool rows_only = false);
+template <typename R> int real_space_rows(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out);
 // Forces: out = wave force (m.force) + q E0 + real-space force for FP64 charges q64.
 template <typename R> int real_space_force(cr_handle *h, MeshBuffers<R> &m, const double *q64, double *force_out);
 int realspace_alloc(cr_handle *h);

@@ -299,6 +299,30 @@ __device__ __forceinline__ unsigned below_bit(unsigned m, int j) {
     return m & k;
 }
 
+// Row i of the operator's top block from the real-space sum y_i: Phi_body(i) - (phik_i +
+// self q_i + y_i), or the bare sum when phi_body is NULL.  With phik NULL only y_i is
+// written: the wave-space part is then still being computed on another stream and
+// rows_combine_kernel adds it afterwards, with the same arithmetic.
+template <typename R>
+__device__ __forceinline__ void write_row(double *__restrict__ out, int bi, double y, const R *__restrict__ phik,
+                                          const R *__restrict__ q, double selfc, const double *__restrict__ phi_body,
+                                          const uint32_t *__restrict__ body) {
+    if (!phik) {
+        out[bi] = y;
+        return;
+    }
+    const double total = (double)phik[bi] + selfc * (double)q[bi] + y;
+    out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+}
+
+template <typename R>
+__global__ void rows_combine_kernel(int N, const R *__restrict__ phik, const R *__restrict__ q, double selfc,
+                                    const double *__restrict__ phi_body, const uint32_t *__restrict__ body,
+                                    double *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) write_row(out, i, out[i], phik, q, selfc, phi_body, body);
+}
+
 // Values T(d_ij) of the set mask bits in the operator precision, in the row-group
 // layout: the k-th set bit of row i, counted from the highest column down, in slot k of
 // the row, zeros after the row's last bit up to its group's longest row.
@@ -452,8 +476,7 @@ __global__ void __launch_bounds__(W * 32, sizeof(R) == 4 ? 6 : 1) pair_spmv_kern
         for (int v = 0; v < W; ++v) tot += part[v][lane];
         const int bi = members[I * CS + lane];
         if (bi >= 0) {
-            const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)tot;
-            out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+            write_row(out, bi, (double)tot, phik, q, selfc, phi_body, body);
         }
     }
 }
@@ -713,8 +736,7 @@ __global__ void stream_finish_kernel(int nslots, const int *__restrict__ members
     const R y = ysum[k];
     ysum[k] = (R)0;
     if (bi < 0) return;
-    const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)y;
-    out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+    write_row(out, bi, (double)y, phik, q, selfc, phi_body, body);
 }
 
 // CTA b of G takes the clusters whose first stored value lies in [T b/G, T (b+1)/G) of the
@@ -910,8 +932,7 @@ __global__ void __launch_bounds__(W * 32, 6) pair_otf32_kernel(const long long *
         for (int v = 0; v < W; ++v) tot += part[v][lane];
         const int bi = members[I * CS + lane];
         if (bi >= 0) {
-            const double total = (double)phik[bi] + selfc * (double)q[bi] + (double)tot;
-            out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+            write_row(out, bi, (double)tot, phik, q, selfc, phi_body, body);
         }
     }
 }
@@ -974,8 +995,7 @@ __global__ void __launch_bounds__(W * 32) pair_otf64_kernel(const long long *__r
         double tot = 0.0;
 #pragma unroll
         for (int v = 0; v < W; ++v) tot += part[v][lane];
-        const double total = phik[bi] + selfc * q[bi] + tot;
-        out[bi] = phi_body ? phi_body[body[bi]] - total : total;
+        write_row(out, bi, tot, phik, q, selfc, phi_body, body);
     }
 }
 
@@ -1316,6 +1336,13 @@ int realspace_alloc(cr_handle *h) {
     CR_TRY(dalloc(h, &r.boff, nc * CS));
     CR_TRY(dalloc(h, &r.err, 1));
     CR_CUDA(h, cudaMemsetAsync(r.err, 0, sizeof(int), h->stream));
+    if (!h->side) {  // the wave-space branch of the operator: highest stream priority
+        int least = 0, greatest = 0;
+        CR_CUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CR_CUDA(h, cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, greatest));
+        CR_CUDA(h, cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+        CR_CUDA(h, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    }
     return CR_OK;
 }
 
@@ -1402,7 +1429,8 @@ int realspace_build(cr_handle *h) {
     return CR_OK;
 }
 
-template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out) {
+template <typename R>
+int real_space_apply(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out, bool rows_only) {
     const int N = h->N;
     if (N == 0) return CR_OK;
     RealSpace &r = h->rs;
@@ -1411,6 +1439,7 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
         CR_TRY(realspace_blocks<R>(h));
     }
     ProfScope ps(h, PROF_REAL);
+    const R *phik = rows_only ? nullptr : m.phi;  // NULL: the real-space sums only
     R *qc = acc_of<R>(r);
     gather_cluster_kernel<R><<<blocks_for((long)r.nclus * CS, 256), 256, 0, h->stream>>>(r.nclus * CS, r.members,
                                                                                          m.q, qc);
@@ -1420,13 +1449,13 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
         if constexpr (sizeof(R) == 4) {
             pair_otf32_kernel<W><<<r.nclus, W * 32, onfly32_smem(h), h->stream>>>(
                 r.head, r.count, r.pair_j, r.members, r.masks, r.boff, r.pshift, rs_build(h), h->m32.phiq,
-                (float)(h->d.n_table / (h->d.rcut - h->d.dr)), qc, m.q, m.phi, h->d.selfcoeff, phi_body, h->d_body,
+                (float)(h->d.n_table / (h->d.rcut - h->d.dr)), qc, m.q, phik, h->d.selfcoeff, phi_body, h->d_body,
                 out);
             CR_LAUNCH(h, "pair_otf32_kernel");
         } else {
             pair_otf64_kernel<W><<<r.nclus, W * 32, 0, h->stream>>>(r.head, r.count, r.pair_j, r.members, r.masks,
                                                                     h->m64.pos, h->m64.phiq, rs_build(h), qc, m.q,
-                                                                    m.phi, h->d.selfcoeff, phi_body, h->d_body, out);
+                                                                    phik, h->d.selfcoeff, phi_body, h->d_body, out);
             CR_LAUNCH(h, "pair_otf64_kernel");
         }
         return CR_OK;
@@ -1442,14 +1471,24 @@ template <typename R> int real_space_apply(cr_handle *h, MeshBuffers<R> &m, cons
         r.withhold_next = 0;
         CR_LAUNCH(h, "pair_stream_kernel");
         stream_finish_kernel<R><<<blocks_for((long)r.nclus * CS, 256), 256, 0, h->stream>>>(
-            r.nclus * CS, r.members, ysum, m.q, m.phi, h->d.selfcoeff, phi_body, h->d_body, out);
+            r.nclus * CS, r.members, ysum, m.q, phik, h->d.selfcoeff, phi_body, h->d_body, out);
         CR_LAUNCH(h, "stream_finish_kernel");
         return CR_OK;
     }
     pair_spmv_kernel<R, W, 16><<<r.nclus, W * 32, 0, h->stream>>>(
-        r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, m.phi,
+        r.nclus, r.head, r.count, r.pair_j, r.members, r.masks, r.voff, r.nnz_pair, blocks_of<R>(r), qc, m.q, phik,
         h->d.selfcoeff, phi_body, h->d_body, out);
     CR_LAUNCH(h, "pair_spmv_kernel");
+    return CR_OK;
+}
+
+// Adds the wave-space part and the self term to rows that hold only their real-space sums
+// (real_space_apply with rows_only).
+template <typename R> int real_space_rows(cr_handle *h, MeshBuffers<R> &m, const double *phi_body, double *out) {
+    if (h->N == 0) return CR_OK;
+    rows_combine_kernel<R><<<blocks_for(h->N, 256), 256, 0, h->stream>>>(h->N, m.phi, m.q, h->d.selfcoeff, phi_body,
+                                                                        h->d_body, out);
+    CR_LAUNCH(h, "rows_combine_kernel");
     return CR_OK;
 }
 
@@ -1502,8 +1541,10 @@ int real_space_virial(cr_handle *h, const double *q64, double *out) {
     return CR_OK;
 }
 
-template int real_space_apply<float>(cr_handle *, MeshBuffers<float> &, const double *, double *);
-template int real_space_apply<double>(cr_handle *, MeshBuffers<double> &, const double *, double *);
+template int real_space_apply<float>(cr_handle *, MeshBuffers<float> &, const double *, double *, bool);
+template int real_space_apply<double>(cr_handle *, MeshBuffers<double> &, const double *, double *, bool);
+template int real_space_rows<float>(cr_handle *, MeshBuffers<float> &, const double *, double *);
+template int real_space_rows<double>(cr_handle *, MeshBuffers<double> &, const double *, double *);
 template int real_space_force<float>(cr_handle *, MeshBuffers<float> &, const double *, double *);
 template int real_space_force<double>(cr_handle *, MeshBuffers<double> &, const double *, double *);
 

@@ -166,12 +166,15 @@ int cr_set_graphs(cr_handle *h, int enable);
  * product, or evaluated again in every product from the positions (the table in shared
  * memory in FP32).  Stored values are read by one CTA per cluster straight from device
  * memory (the default) or, with CR_REALSPACE_STREAM, streamed through shared memory by
- * bulk copies, one producer warp per CTA.  flags: CR_REALSPACE_ONFLY32 evaluates the FP32
+ * bulk copies, one producer warp per CTA.  The real-space product runs concurrently with
+ * the wave-space part of the operator (a high-priority side stream of the handle) unless
+ * CR_REALSPACE_SERIAL is set or the profiler is on.  flags: CR_REALSPACE_ONFLY32 evaluates the FP32
  * products on the fly, CR_REALSPACE_ONFLY64 the FP64 products (bit-identical to the
  * default stored product); 0 stores both.  Takes effect at the next product. */
 #define CR_REALSPACE_ONFLY32 1
 #define CR_REALSPACE_ONFLY64 2
 #define CR_REALSPACE_STREAM 4
+#define CR_REALSPACE_SERIAL 8
 int cr_set_realspace(cr_handle *h, int flags);
 /* Limit of every bounded device wait of the streamed real-space product
  * (CR_REALSPACE_STREAM), in SM clock

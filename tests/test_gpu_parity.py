@@ -276,11 +276,12 @@ def test_operator_matches_oracle_other_supports(cuda, product_lib, oracle_lib, s
     h.close()
 
 
-@pytest.mark.parametrize("flags", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("flags", [0, 1, 2, 3, 4, 8])
 @pytest.mark.parametrize("case", ["plain_small", "small_box"])
 def test_realspace_modes_match_oracle(cuda, product_lib, oracle_lib, flags, case):
     """Stored (read directly or streamed through shared memory) and on-the-fly real-space
-    values give the oracle's operator, and every FP64 product the directly read one's
+    values, with the real-space product beside the wave-space part or after it (8), give
+    the oracle's operator, and every FP64 product the directly read one's
     (the on-the-fly sum is the same arithmetic in the same order, the streamed one adds
     per-warp sums with atomics; the spreading's atomic accumulation leaves
     summation-order differences in the whole operator).  The small box
