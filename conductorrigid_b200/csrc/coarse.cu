@@ -851,7 +851,7 @@ __global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__
                                     const int *__restrict__ pair_b, const long long *__restrict__ woff,
                                     const float *__restrict__ W, const float *__restrict__ u, double selfc,
                                     const double *__restrict__ y, const double *__restrict__ x,
-                                    double *__restrict__ t) {
+                                    double *__restrict__ t, int split) {
     extern __shared__ float4 dyn[];
     const int b = blockIdx.x;
     const int beg = body_start[b], nb = body_start[b + 1] - beg;
@@ -860,6 +860,7 @@ __global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__
     int4 *srow = reinterpret_cast<int4 *>(dyn);                                // [nrows] (mx, my, mz0, first mode)
     float2 *su = reinterpret_cast<float2 *>(dyn + nrows);                     // [nmodes]
     double2 *sy = reinterpret_cast<double2 *>(dyn + nrows + (nmodes + 1) / 2); // [npr][2] partner y, W offset
+    double *red = reinterpret_cast<double *>(sy + 2 * npr);                    // [split-1][P] partial sums
     for (int q = threadIdx.x; q < nrows; q += blockDim.x) srow[q] = rows[q];
     for (int q = threadIdx.x; q < nmodes; q += blockDim.x) su[q] = make_float2(u[2 * q], u[2 * q + 1]);
     for (int q = threadIdx.x; q < npr; q += blockDim.x) {
@@ -868,23 +869,28 @@ __global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__
         sy[2 * q + 1] = make_double2(y[3 * c + 2], __longlong_as_double(woff[h0 + q]));
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-        const int i = members[beg + k];
+    // `split` threads per bead (P = blockDim / split >= the body's beads when split > 1):
+    // part s takes the near pairs and the wave rows q = s, s + split, ...; the parts'
+    // sums meet in shared memory
+    const int P = blockDim.x / split, part = threadIdx.x / P, k0 = threadIdx.x % P;
+    for (int k = k0; k < nb || (split > 1 && k == k0); k += P) {
+        const bool mine = k < nb;
+        const int i = mine ? members[beg + k] : 0;
         double m0 = 0.0, m1 = 0.0;
 #pragma unroll 4
-        for (int q = 0; q < npr; ++q) {
+        for (int q = part; q < (mine ? npr : 0); q += split) {
             const double2 y01 = sy[2 * q], y2o = sy[2 * q + 1];
             const float *w = W + __double_as_longlong(y2o.y) + 3 * (size_t)k;
             const float w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
             m0 += (double)w0 * y01.x + (double)w1 * y01.y;
             m1 += (double)w2 * y2o.x;
         }
-        const double4 p = pos[i];
+        const double4 p = mine ? pos[i] : make_double4(0, 0, 0, 0);
         const float fx = (float)(p.x * Linv.x), fy = (float)(p.y * Linv.y), fz = (float)(p.z * Linv.z);
         float sz, cz;
         sincos_turns(fz, &sz, &cz);
         float wave = 0.f;
-        for (int q = 0; q < nrows; ++q) {
+        for (int q = part; q < (mine ? nrows : 0); q += split) {
             const int4 r = srow[q];
             const int end = q + 1 < nrows ? srow[q + 1].w : nmodes;
             float s, c;
@@ -898,6 +904,12 @@ __global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__
             }
         }
         double m = (double)wave + m0 + m1;
+        if (split > 1) {
+            if (part > 0 && mine) red[(part - 1) * P + k] = m;
+            __syncthreads();
+            if (part > 0 || !mine) continue;
+            for (int v = 1; v < split; ++v) m += red[(v - 1) * P + k];
+        }
         double phi = 0.0;
         if (a >= 0) {
             const double y0 = y[3 * a], y1 = y[3 * a + 1], y2 = y[3 * a + 2];
@@ -1134,10 +1146,14 @@ int coarse_prepare(cr_handle *h) {
     int max_n = 0;
     for (int b = 0; b < B; ++b) max_n = std::max(max_n, h->h_body_start[b + 1] - h->h_body_start[b]);
     const int bs = std::min(256, std::max(32, (max_n + 31) / 32 * 32));
+    // two threads per bead when one pass covers every body (more warps for the latency-
+    // bound rotation chains of the wave rows)
+    const int model_split = max_n <= bs ? 2 : 1;
     int max_pairs = 0;
     for (int a = 0; a < nbc; ++a) max_pairs = std::max(max_pairs, pcount[a]);
     const size_t model_smem =
-        ((size_t)nrows + (nmodes + 1) / 2) * sizeof(float4) + (size_t)max_pairs * 2 * sizeof(double2);
+        ((size_t)nrows + (nmodes + 1) / 2) * sizeof(float4) + (size_t)max_pairs * 2 * sizeof(double2) +
+        (size_t)(model_split - 1) * bs * sizeof(double);
     if (model_smem > 48 * 1024)
         CR_CUDA(h, cudaFuncSetAttribute(coarse_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)model_smem));
@@ -1228,6 +1244,7 @@ int coarse_prepare(cr_handle *h) {
     cs.nvec = nvec;
     cs.bs = bs;
     cs.model_smem = model_smem;
+    cs.model_split = model_split;
     cs.K2 = K2;
     cs.npairs = npairs;
     cs.kc = kc;
@@ -1285,10 +1302,11 @@ int coarse_apply(cr_handle *h, const double *x, double *z) {
                                                                                cs.kv, cs.u);
         CR_LAUNCH(h, "fcol_reduce_kernel");
     }
-    coarse_model_kernel<<<B, cs.bs, cs.model_smem, h->stream>>>(N, cs.nmodes, cs.nrows, cs.rows, cs.cidx,
+    coarse_model_kernel<<<B, cs.bs * cs.model_split, cs.model_smem, h->stream>>>(N, cs.nmodes, cs.nrows, cs.rows, cs.cidx,
                                                                  h->d_body_start, h->d_body_members, h->m64.pos,
                                                                  Linv, cs.zq, cs.zp, cs.phead, cs.pcount, cs.pair_b,
-                                                                 cs.woff, cs.W, cs.u, h->d.selfcoeff, cs.y, x, cs.t);
+                                                                 cs.woff, cs.W, cs.u, h->d.selfcoeff, cs.y, x, cs.t,
+                                                                 cs.model_split);
     CR_LAUNCH(h, "coarse_model_kernel");
     CR_TRY(conductor_apply(h, cs.t, z));
     coarse_prolong_kernel<<<cs.nbc, 128, 0, h->stream>>>(N, cs.cbody, h->d_body_start, h->d_body_members, cs.zq,

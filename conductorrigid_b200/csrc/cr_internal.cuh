@@ -206,6 +206,7 @@ struct CoarseSpace {
     int4 *rows = nullptr;               // [nrows] runs of consecutive mz: (mx, my, mz0, first mode)
     int nrows = 0, bs = 128;            // runs; threads per body CTA of the A~ Z y kernel
     size_t model_smem = 0;              // dynamic shared memory of the A~ Z y kernel
+    int model_split = 1;                // threads per bead of the A~ Z y kernel
     // sparse level (coarse problems above max_dense unknowns): near-pair blocks, PCG
     int max_dense = 12288, pcg_iters = 0;  // above max_dense: pcg_iters CG steps (0: no coarse level)
     bool sparse = false;

@@ -222,48 +222,89 @@ __device__ __forceinline__ RowGroup row_group(unsigned m, int lane) {
 // Bit masks of the in-range bead pairs of every cluster pair (row i = bead i of I,
 // bit j = bead j of J) and the stored slots of the pair (per group of RG rows, RG times
 // the group's longest row).
-// The test runs on the FP32 copies of the positions; only a pair whose FP32 squared
-// distance lies within `band` of rc^2 (or below 2 dr^2 + band) is decided again in FP64,
-// exactly as the oracle decides it.  `band` is ten times a bound on the FP32 error of
-// d^2 for |d| <= rc in a box of edge L (positions rounded to FP32: |error of dx| <= 2e-7 L),
-// so the masks equal the FP64 ones bit for bit.
+// The test runs in FP32 on the beads' offsets from their cluster centres and the centres'
+// minimum-image offset (for cluster pairs whose bead separations need no further image,
+// almost all of them), otherwise on the FP32 copies of the positions; only a pair whose
+// FP32 squared distance lies within `band` of rc^2 (or below 2 dr^2 + band) is decided
+// again in FP64, exactly as the oracle decides it.  `band` is ten times a bound on the
+// FP32 error of d^2 for |d| <= rc in a box of edge L (positions rounded to FP32: |error of
+// dx| <= 2e-7 L; the offsets, a few units long, are rounded far more finely), so the masks
+// equal the FP64 ones bit for bit.
 __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_i, const int *__restrict__ pair_j,
                                  const int *__restrict__ members, const double4 *__restrict__ pos,
                                  const float4 *__restrict__ pos32, RSBuild c, float3 L32, float3 Linv32, float rc2,
                                  float band, float low, unsigned *__restrict__ masks, int *__restrict__ nnz,
                                  unsigned long long *__restrict__ bits, const double4 *__restrict__ centre,
-                                 const double4 *__restrict__ extent, float4 *__restrict__ pshift) {
+                                 const double4 *__restrict__ extent, const float4 *__restrict__ boff,
+                                 float4 *__restrict__ pshift) {
     const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (p >= npairs) return;
     const int I = pair_i[p], J = pair_j[p];
     const int bi = members[I * CS + lane];
     const int bj = members[J * CS + lane];
-    const float4 pi = bi >= 0 ? pos32[bi] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 pjl = bj >= 0 ? pos32[bj] : make_float4(0.f, 0.f, 0.f, 0.f);
+    // offset of the cluster centres under the minimum image, and whether the bead offsets
+    // then need no further image: rc + 2 (e_I + e_J) < L/2 along every axis (a bead lies
+    // within e of its centre, so no other image of a pair within rc can be nearer)
+    const double4 cI = centre[I], cJ = centre[J], eI = extent[I], eJ = extent[J];
+    const bool direct = c.rc + 2.0 * (eI.x + eJ.x) < 0.5 * c.L[0] - 1e-3 &&
+                        c.rc + 2.0 * (eI.y + eJ.y) < 0.5 * c.L[1] - 1e-3 &&
+                        c.rc + 2.0 * (eI.z + eJ.z) < 0.5 * c.L[2] - 1e-3;
+    const float4 sh = make_float4((float)mimg(cJ.x - cI.x, c.L[0], c.Linv[0]), (float)mimg(cJ.y - cI.y, c.L[1], c.Linv[1]),
+                                  (float)mimg(cJ.z - cI.z, c.L[2], c.Linv[2]), direct ? 1.f : 0.f);
     unsigned m = 0;
-    for (int j = 0; j < CS; ++j) {
-        const int vj = __shfl_sync(0xffffffffu, bj, j);
-        const float xj = __shfl_sync(0xffffffffu, pjl.x, j);
-        const float yj = __shfl_sync(0xffffffffu, pjl.y, j);
-        const float zj = __shfl_sync(0xffffffffu, pjl.z, j);
-        if (bi >= 0 && vj >= 0) {
-            float dx = pi.x - xj, dy = pi.y - yj, dz = pi.z - zj;
-            dx -= L32.x * rintf(dx * Linv32.x);
-            dy -= L32.y * rintf(dy * Linv32.y);
-            dz -= L32.z * rintf(dz * Linv32.z);
+    if (direct) {
+        // separations from the FP32 offsets of the beads from their cluster centres: d =
+        // (o_i - shift) - o_j.  Padding beads sit at +-1e30, so every separation with one
+        // of them overflows to infinity and fails the test without a check per bead.
+        const float4 oi = boff[I * CS + lane], oj = boff[J * CS + lane];
+        const float ax = bi >= 0 ? oi.x - sh.x : 1e30f, ay = bi >= 0 ? oi.y - sh.y : 1e30f,
+                    az = bi >= 0 ? oi.z - sh.z : 1e30f;
+        const float jx = bj >= 0 ? oj.x : -1e30f, jy = bj >= 0 ? oj.y : -1e30f, jz = bj >= 0 ? oj.z : -1e30f;
+#pragma unroll 8
+        for (int j = 0; j < CS; ++j) {
+            const float dx = ax - __shfl_sync(0xffffffffu, jx, j);
+            const float dy = ay - __shfl_sync(0xffffffffu, jy, j);
+            const float dz = az - __shfl_sync(0xffffffffu, jz, j);
             const float d2 = dx * dx + dy * dy + dz * dz;
             bool in;
             if (d2 > rc2 + band) {
                 in = false;
             } else if (d2 < rc2 - band && d2 > low) {
                 in = true;
-            } else {  // near a boundary: the FP64 decision, rounded as the oracle rounds it
-                const double4 a = pos[bi], b = pos[vj];
+            } else {  // near a boundary (both beads real): the FP64 decision of the oracle
+                const double4 a = pos[bi], b = pos[members[J * CS + j]];
                 const double e2 = dist2_exact(a, b, c);
                 in = e2 < c.rc2 && e2 >= c.rmin2;
             }
             if (in) m |= 1u << j;
+        }
+    } else {
+        const float4 pi = bi >= 0 ? pos32[bi] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 pjl = bj >= 0 ? pos32[bj] : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int j = 0; j < CS; ++j) {
+            const int vj = __shfl_sync(0xffffffffu, bj, j);
+            const float xj = __shfl_sync(0xffffffffu, pjl.x, j);
+            const float yj = __shfl_sync(0xffffffffu, pjl.y, j);
+            const float zj = __shfl_sync(0xffffffffu, pjl.z, j);
+            if (bi >= 0 && vj >= 0) {
+                float dx = pi.x - xj, dy = pi.y - yj, dz = pi.z - zj;
+                dx -= L32.x * rintf(dx * Linv32.x);
+                dy -= L32.y * rintf(dy * Linv32.y);
+                dz -= L32.z * rintf(dz * Linv32.z);
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                bool in;
+                if (d2 > rc2 + band) {
+                    in = false;
+                } else if (d2 < rc2 - band && d2 > low) {
+                    in = true;
+                } else {  // near a boundary: the FP64 decision, rounded as the oracle rounds it
+                    const double4 a = pos[bi], b = pos[vj];
+                    const double e2 = dist2_exact(a, b, c);
+                    in = e2 < c.rc2 && e2 >= c.rmin2;
+                }
+                if (in) m |= 1u << j;
+            }
         }
     }
     masks[p * CS + lane] = m;
@@ -272,14 +313,7 @@ __global__ void pair_mask_kernel(long long npairs, const int *__restrict__ pair_
     if (lane == 0) {
         nnz[p] = stored;
         atomicAdd(bits, (unsigned long long)tot);
-        // offset of the cluster centres under the minimum image, and whether the bead
-        // offsets then need no further image: rc + 2 (e_I + e_J) < L/2 along every axis
-        const double4 cI = centre[I], cJ = centre[J], eI = extent[I], eJ = extent[J];
-        const bool direct = c.rc + 2.0 * (eI.x + eJ.x) < 0.5 * c.L[0] - 1e-3 &&
-                            c.rc + 2.0 * (eI.y + eJ.y) < 0.5 * c.L[1] - 1e-3 &&
-                            c.rc + 2.0 * (eI.z + eJ.z) < 0.5 * c.L[2] - 1e-3;
-        pshift[p] = make_float4((float)mimg(cJ.x - cI.x, c.L[0], c.Linv[0]), (float)mimg(cJ.y - cI.y, c.L[1], c.Linv[1]),
-                                (float)mimg(cJ.z - cI.z, c.L[2], c.Linv[2]), direct ? 1.f : 0.f);
+        pshift[p] = sh;
     }
 }
 
@@ -1410,7 +1444,7 @@ int realspace_build(cr_handle *h) {
                                             make_float3((float)(1.0 / h->L[0]), (float)(1.0 / h->L[1]),
                                                         (float)(1.0 / h->L[2])),
                                             (float)c.rc2, band, low, r.masks, r.nnz_pair, r.bits, r.centre,
-                                            r.extent, r.pshift);
+                                            r.extent, r.boff, r.pshift);
     }
     CR_LAUNCH(h, "pair_mask_kernel");
     bytes = h->sort_tmp_bytes;
