@@ -423,7 +423,7 @@ __global__ void symmetrise_kernel(int n, double *__restrict__ C, int ldc) {
 // Dinv of the pivot block (one CTA of kPivThreads threads, scalar in-place Gauss-Jordan in
 // shared memory; thread t owns entries (t/64 + kPivStride u, t%64)); a pivot that is not
 // positive and finite sets *flag and leaves Dinv untouched.
-constexpr int kPivThreads = 1024, kPivStride = kPivThreads / NB, kPivRows = NB / kPivStride;
+constexpr int kPivThreads = 256, kPivStride = kPivThreads / NB, kPivRows = NB / kPivStride;
 __global__ void __launch_bounds__(kPivThreads) gj_pivot_kernel(int k0, int np, const float *__restrict__ A,
                                                                float *__restrict__ Dinv, int *__restrict__ flag) {
     __shared__ float D[NB][NB + 1];
@@ -664,8 +664,9 @@ __global__ void block_jacobi_kernel(int nbc, const int *__restrict__ phead, cons
 
 // u = F^T v in two steps: partial column sums over chunks of kColRows rows of F (threads
 // over the columns, every load coalesced), then a reduction over the chunks in a fixed
-// order.  With kv, u[k] is also scaled by sqrt(w) of its wave vector (k / 2).
-constexpr int kColRows = 32;
+// order.  With kv, u[k] is also scaled by sqrt(w) of its wave vector (k / 2).  Chunks of 8
+// rows give ~375 CTAs for 3000 coarse unknowns (32-row chunks left most SMs idle).
+constexpr int kColRows = 8;
 __global__ void __launch_bounds__(256) fcol_partial_kernel(int nc, int K2, const float *__restrict__ F,
                                                            const double *__restrict__ v, double *__restrict__ part) {
     const int c0 = blockIdx.x * kColRows, c1 = min(nc, c0 + kColRows);

@@ -656,6 +656,26 @@ void krylov_free(cr_handle *h) {
     }
 }
 
+// The coarse level of the two-level preconditioner for this geometry, built on the
+// handle's high-priority side stream while the stored real-space values of the geometry
+// are built on the main stream: the Gauss-Jordan sweep keeps few multiprocessors busy and
+// the values pass fills the rest.  The values are queued first, before the coarse set-up's
+// host waits (which then wait on the side stream only).
+static int prepare_overlapped(cr_handle *h) {
+    const bool build = h->user.precond == CR_PRECOND_TWO_LEVEL && h->coarse.gen != h->geo_gen;
+    if (!build || !h->side || h->prof.on) return coarse_prepare(h);
+    cudaStream_t main = h->stream;
+    CR_CUDA(h, cudaEventRecord(h->ev_fork, main));
+    CR_CUDA(h, cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+    CR_TRY(realspace_prepare(h, h->user.precision == CR_FP64 ? CR_FP64 : CR_FP32));
+    h->stream = h->side;
+    int st = coarse_prepare(h);
+    if (st == CR_OK) st = check_cuda(h, cudaEventRecord(h->ev_join, h->side), "cudaEventRecord");
+    h->stream = main;
+    CR_CUDA(h, cudaStreamWaitEvent(main, h->ev_join, 0));
+    return st;
+}
+
 int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {
     Krylov &K = h->kry;
     const int n = K.n;
@@ -665,7 +685,7 @@ int solve(cr_handle *h, double *x, const double *b, cr_solve_stats *st) {
     cr_solve_stats s{};
     OpCount oc;
     double bnorm = 0, rnorm = 0;
-    CR_TRY(coarse_prepare(h));  // two-level preconditioner: coarse level of this geometry
+    CR_TRY(prepare_overlapped(h));  // two-level preconditioner: coarse level of this geometry
     CR_TRY(norm(h, b, &bnorm));
     if (!std::isfinite(bnorm)) return fail(h, CR_NUMERICAL, "non-finite right-hand side");
     const double atol = tol * bnorm;
