@@ -203,6 +203,12 @@ _SIGS = {
     "cr_guess_target": ([_P, _P, _P, C.c_double, _P], _I),
     "cr_neutral_direction": ([_P, _P, _I, C.c_double, _P], _I),
     "cr_batch_compute": ([_I, _P, _P, _P, _P, _P, _P, C.POINTER(CrSolveStats), C.POINTER(C.c_int), _I], _I),
+    "cr_batch_create": ([_I, _P, C.POINTER(_P)], _I),
+    "cr_batch_destroy": ([_P], _I),
+    "cr_batch_last_error": ([_P], C.c_char_p),
+    "cr_batch_solve": ([_P, _P, _P, _P, _P, _P, C.POINTER(CrSolveStats), C.POINTER(C.c_int), _I], _I),
+    "cr_batch_counters": ([_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], _I),
+    "cr_batch_phase_ms": ([_P, _D, _D, _D], _I),
     "cr_spread_noalloc": ([C.POINTER(CrDerived), C.c_double, _D, _I, _P, _P, _P, _P], _I),
     "cr_noalloc_last_error": ([], C.c_char_p),
     "cr_util_icosphere_count": ([_I], _I),

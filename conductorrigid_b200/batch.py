@@ -7,9 +7,11 @@ rc <= L/2; for boxes smaller than 2 rc the replica's Ewald parameter is raised t
 xi = sqrt(-ln tol)/rc with rc = L/2, which keeps the real-space truncation error at the
 tolerance and moves the rest of the sum to the mesh.
 
-solve_batched() runs all replicas through cr_batch_compute (concurrent streams, each
-Arnoldi step a captured graph); solve_looped() solves them one after another through
-cr_compute, the single-system path.  With autotune=True every replica's mesh tiling is
+solve_lockstep() runs all replicas through a lockstep batch (cr_batch_create /
+cr_batch_solve): every unconverged replica takes one Arnoldi step per round and each stage
+of the step is one kernel launch over all replicas.  solve_batched() runs them through
+cr_batch_compute (concurrent streams, each Arnoldi step a captured graph);
+solve_looped() solves them one after another through cr_compute, the single-system path.  With autotune=True every replica's mesh tiling is
 chosen by cr_autotune at construction (each system timed alone); tune_batch() instead
 chooses the tiling policy by the batch's own throughput.
 """
@@ -95,6 +97,53 @@ class Replicas:
             raise _lib.CrError(code, "cr_batch_compute", f"replicas {bad[:8]} failed")
         return [st[i].as_dict() for i in range(n)]
 
+    def _columns(self):
+        n = self.n
+        P = C.c_void_p * n
+        return [P(*[a[k].data_ptr() for a in self.arrays]) for k in range(5)]
+
+    def make_lockstep(self):
+        """The lockstep batch over these replicas' handles (8^3 register-column tiling)."""
+        if getattr(self, "_lockstep", None) is not None:
+            return self._lockstep
+        for h in self.handles:
+            h.set_tiling(8, 0)
+        n = self.n
+        hs = (C.c_void_p * n)(*[h.h.value for h in self.handles])
+        out = C.c_void_p()
+        code = _lib.lib().cr_batch_create(n, hs, C.byref(out))
+        if code != _lib.CR_OK:
+            msg = (_lib.lib().cr_batch_last_error(None) or b"").decode()
+            raise _lib.CrError(code, "cr_batch_create", msg)
+        self._lockstep = out
+        return out
+
+    def solve_lockstep(self, n_threads=16):
+        """All replicas in one lockstep batch: per-geometry set-up and forces per replica on
+        n_threads host threads, the iterations one launch per stage over every replica."""
+        bt = self.make_lockstep()
+        n = self.n
+        st = (_lib.CrSolveStats * n)()
+        status = (C.c_int * n)()
+        code = _lib.lib().cr_batch_solve(bt, *self._columns(), st, status, int(n_threads))
+        if code != _lib.CR_OK:
+            bad = [i for i in range(n) if status[i] != _lib.CR_OK]
+            msg = (_lib.lib().cr_batch_last_error(bt) or b"").decode()
+            raise _lib.CrError(code, "cr_batch_solve", f"{msg}; replicas {bad[:8]} failed")
+        return [st[i].as_dict() for i in range(n)]
+
+    def lockstep_counters(self):
+        """(batched kernel launches, batched transforms, lockstep rounds) so far."""
+        a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        _lib.lib().cr_batch_counters(self.make_lockstep(), C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
+
+    def lockstep_phases(self):
+        """Host-clock ms of the last lockstep solve: set-up, iterations, force pass."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        _lib.lib().cr_batch_phase_ms(self.make_lockstep(), C.byref(a), C.byref(b), C.byref(c))
+        return {"setup": a.value, "iterations": b.value, "forces": c.value}
+
     def set_tilings(self, tilings):
         for h, t in zip(self.handles, tilings):
             h.set_tiling(t["tile_edge"], t["spread_mode"])
@@ -136,6 +185,9 @@ class Replicas:
         return rates
 
     def close(self):
+        if getattr(self, "_lockstep", None) is not None:
+            _lib.lib().cr_batch_destroy(self._lockstep)
+            self._lockstep = None
         for h in self.handles:
             h.close()
         self.handles = []

@@ -178,4 +178,57 @@ int apply_operator(cr_handle *h, const double *x, double *y, int precision) {
     return apply_operator_t(h, h->m32, x, y);
 }
 
+// ---- lockstep batches: body rows and the diagonal preconditioner ----
+
+namespace {
+
+__global__ void body_sums_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                       const int *__restrict__ mask, int xin, int yout) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &r = reps[it.x];
+    const int b = (it.y * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (b >= r.B) return;
+    const double *x = r.vec[xin];
+    double s = 0.0;
+    for (int k = r.body_start[b] + lane; k < r.body_start[b + 1]; k += 32) s += x[r.body_members[k]];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) r.vec[yout][r.N + b] = s;
+}
+
+__global__ void diag_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                  const int *__restrict__ mask, int xin, int zout) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &r = reps[it.x];
+    const double *x = r.vec[xin];
+    double *y = r.vec[zout];
+    for (int i = it.y * blockDim.x + threadIdx.x; i < r.n; i += r.vblk * blockDim.x) {
+        if (i < r.N) {
+            y[i] = -4.0 * kPi * x[i];
+        } else {
+            const int b = i - r.N;
+            y[i] = r.rigid[b] ? x[i] / (double)r.bsize[b] : x[i] / (4.0 * kPi);
+        }
+    }
+}
+
+}  // namespace
+
+int batch_body_sums(cr_batch *bt, const int *mask, int xin, int yout, cudaStream_t s) {
+    if (bt->n_items[BL_BODYWARPS] == 0) return CR_OK;
+    body_sums_batch_kernel<<<bt->n_items[BL_BODYWARPS], 256, 0, s>>>(bt->d_reps, bt->d_items[BL_BODYWARPS], mask, xin,
+                                                                      yout);
+    ++bt->launches;
+    return batch_check(bt, cudaGetLastError(), "body_sums_batch_kernel");
+}
+
+int batch_diag(cr_batch *bt, const int *mask, int xin, int zout, cudaStream_t s) {
+    if (bt->n_items[BL_VEC] == 0) return CR_OK;
+    diag_batch_kernel<<<bt->n_items[BL_VEC], 256, 0, s>>>(bt->d_reps, bt->d_items[BL_VEC], mask, xin, zout);
+    ++bt->launches;
+    return batch_check(bt, cudaGetLastError(), "diag_batch_kernel");
+}
+
 }  // namespace cr

@@ -38,6 +38,7 @@
 // conductor response alone, on 100 bodies).
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "cr_internal.cuh"
@@ -667,22 +668,27 @@ __global__ void block_jacobi_kernel(int nbc, const int *__restrict__ phead, cons
 // order.  With kv, u[k] is also scaled by sqrt(w) of its wave vector (k / 2).  Chunks of 8
 // rows give ~375 CTAs for 3000 coarse unknowns (32-row chunks left most SMs idle).
 constexpr int kColRows = 8;
-__global__ void __launch_bounds__(256) fcol_partial_kernel(int nc, int K2, const float *__restrict__ F,
-                                                           const double *__restrict__ v, double *__restrict__ part) {
-    const int c0 = blockIdx.x * kColRows, c1 = min(nc, c0 + kColRows);
+__device__ __forceinline__ void fcol_partial_chunk(int chunk, int nc, int K2, const float *__restrict__ F,
+                                                   const double *__restrict__ v, double *__restrict__ part) {
+    const int c0 = chunk * kColRows, c1 = min(nc, c0 + kColRows);
     for (int k = threadIdx.x; k < K2; k += blockDim.x) {
         double acc = 0.0;
 #pragma unroll 8
         for (int c = c0; c < c1; ++c) acc += (double)__ldg(F + (size_t)c * K2 + k) * v[c];
-        part[(size_t)blockIdx.x * K2 + k] = acc;
+        part[(size_t)chunk * K2 + k] = acc;
     }
 }
 
+__global__ void __launch_bounds__(256) fcol_partial_kernel(int nc, int K2, const float *__restrict__ F,
+                                                           const double *__restrict__ v, double *__restrict__ part) {
+    fcol_partial_chunk(blockIdx.x, nc, K2, F, v, part);
+}
+
 template <typename T>
-__global__ void fcol_reduce_kernel(int nchunk, int K2, const double *__restrict__ part, int nmodes,
-                                   const float4 *__restrict__ kv, T *__restrict__ u) {
+__device__ __forceinline__ void fcol_reduce_block(int blk, int nchunk, int K2, const double *__restrict__ part,
+                                                  int nmodes, const float4 *__restrict__ kv, T *__restrict__ u) {
     // one warp per column: lane l sums chunks l, l+32, ..., then a fixed shuffle tree
-    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int k = (blk * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (k >= K2) return;
     double s = 0.0;
     for (int q = lane; q < nchunk; q += 32) s += part[(size_t)q * K2 + k];
@@ -690,6 +696,12 @@ __global__ void fcol_reduce_kernel(int nchunk, int K2, const double *__restrict_
     if (lane != 0) return;
     if (kv) s = k < 2 * nmodes ? s * kv[k >> 1].w : 0.0;
     u[k] = (T)s;
+}
+
+template <typename T>
+__global__ void fcol_reduce_kernel(int nchunk, int K2, const double *__restrict__ part, int nmodes,
+                                   const float4 *__restrict__ kv, T *__restrict__ u) {
+    fcol_reduce_block<T>(blockIdx.x, nchunk, K2, part, nmodes, kv, u);
 }
 
 // y = 0, r = -g, z = D r, p = z; partial r.z per block
@@ -805,12 +817,13 @@ __global__ void __launch_bounds__(kVecThreads) pcg_dir_kernel(int nbc, int nvec,
 // ---- application ----
 
 // g[3a+e] = sum_{i in a} z_ae(i) x_i + zp[a][e] x[N+a]
-__global__ void coarse_restrict_kernel(int N, const int *__restrict__ cbody, const int *__restrict__ body_start,
-                                       const int *__restrict__ members, const double *__restrict__ zq,
-                                       const double *__restrict__ zp, const double *__restrict__ x,
-                                       double *__restrict__ g) {
+__device__ __forceinline__ void coarse_restrict_body(int a, int N, const int *__restrict__ cbody,
+                                                     const int *__restrict__ body_start,
+                                                     const int *__restrict__ members, const double *__restrict__ zq,
+                                                     const double *__restrict__ zp, const double *__restrict__ x,
+                                                     double *__restrict__ g) {
     __shared__ double red[3 * 32];
-    const int a = blockIdx.x, ba = cbody[a];
+    const int ba = cbody[a];
     const int beg = body_start[ba], nb = body_start[ba + 1] - beg;
     double s[3] = {0.0, 0.0, 0.0};
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
@@ -823,13 +836,25 @@ __global__ void coarse_restrict_kernel(int N, const int *__restrict__ cbody, con
         for (int e = 0; e < 3; ++e) g[3 * a + e] = s[e] + zp[3 * ba + e] * x[N + ba];
 }
 
+__global__ void coarse_restrict_kernel(int N, const int *__restrict__ cbody, const int *__restrict__ body_start,
+                                       const int *__restrict__ members, const double *__restrict__ zq,
+                                       const double *__restrict__ zp, const double *__restrict__ x,
+                                       double *__restrict__ g) {
+    coarse_restrict_body(blockIdx.x, N, cbody, body_start, members, zq, zp, x, g);
+}
+
 // y = -Cinv g (one warp per row; rows of ld floats, g zero beyond n)
-__global__ void coarse_gemv_kernel(int n, int ld, const float *__restrict__ Ci, const double *__restrict__ g,
-                                   double *__restrict__ y) {
-    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__device__ __forceinline__ void coarse_gemv_block(int blk, int n, int ld, const float *__restrict__ Ci,
+                                                  const double *__restrict__ g, double *__restrict__ y) {
+    const int r = (blk * blockDim.x + threadIdx.x) >> 5;
     if (r >= n) return;
     const double s = warp_row_dot(Ci + (size_t)r * ld, g, ld / 4);
     if ((threadIdx.x & 31) == 0) y[r] = -s;
+}
+
+__global__ void coarse_gemv_kernel(int n, int ld, const float *__restrict__ Ci, const double *__restrict__ g,
+                                   double *__restrict__ y) {
+    coarse_gemv_block(blockIdx.x, n, ld, Ci, g, y);
 }
 
 // sin and cos of 2 pi t: t reduced to [-1/2, 1/2] first, then the fast intrinsic, whose
@@ -844,17 +869,17 @@ __device__ __forceinline__ void sincos_turns(float t, float *s, float *c) {
 // The wave vectors come in rows of consecutive m_z at fixed (m_x, m_y): one sine/cosine per
 // row, then rotation by exp(2 pi i z / L_z) along the row.  The body's near pairs (partner
 // coefficients and W offsets) are staged in shared memory first.
-__global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__restrict__ rows,
-                                    const int *__restrict__ cidx, const int *__restrict__ body_start,
-                                    const int *__restrict__ members, const double4 *__restrict__ pos, double3 Linv,
-                                    const double *__restrict__ zq, const double *__restrict__ zp,
-                                    const int *__restrict__ phead, const int *__restrict__ pcount,
-                                    const int *__restrict__ pair_b, const long long *__restrict__ woff,
-                                    const float *__restrict__ W, const float *__restrict__ u, double selfc,
-                                    const double *__restrict__ y, const double *__restrict__ x,
-                                    double *__restrict__ t, int split) {
+__device__ __forceinline__ void coarse_model_body(int b, int N, int nmodes, int nrows, const int4 *__restrict__ rows,
+                                                  const int *__restrict__ cidx, const int *__restrict__ body_start,
+                                                  const int *__restrict__ members, const double4 *__restrict__ pos,
+                                                  double3 Linv, const double *__restrict__ zq,
+                                                  const double *__restrict__ zp, const int *__restrict__ phead,
+                                                  const int *__restrict__ pcount, const int *__restrict__ pair_b,
+                                                  const long long *__restrict__ woff, const float *__restrict__ W,
+                                                  const float *__restrict__ u, double selfc,
+                                                  const double *__restrict__ y, const double *__restrict__ x,
+                                                  double *__restrict__ t, int split) {
     extern __shared__ float4 dyn[];
-    const int b = blockIdx.x;
     const int beg = body_start[b], nb = body_start[b + 1] - beg;
     const int a = cidx[b];
     const int h0 = a >= 0 ? phead[a] : 0, npr = a >= 0 ? pcount[a] : 0;
@@ -922,12 +947,26 @@ __global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__
     if (threadIdx.x == 0) t[N + b] = x[N + b];
 }
 
+__global__ void coarse_model_kernel(int N, int nmodes, int nrows, const int4 *__restrict__ rows,
+                                    const int *__restrict__ cidx, const int *__restrict__ body_start,
+                                    const int *__restrict__ members, const double4 *__restrict__ pos, double3 Linv,
+                                    const double *__restrict__ zq, const double *__restrict__ zp,
+                                    const int *__restrict__ phead, const int *__restrict__ pcount,
+                                    const int *__restrict__ pair_b, const long long *__restrict__ woff,
+                                    const float *__restrict__ W, const float *__restrict__ u, double selfc,
+                                    const double *__restrict__ y, const double *__restrict__ x,
+                                    double *__restrict__ t, int split) {
+    coarse_model_body(blockIdx.x, N, nmodes, nrows, rows, cidx, body_start, members, pos, Linv, zq, zp, phead, pcount,
+                      pair_b, woff, W, u, selfc, y, x, t, split);
+}
+
 // z += Z y
-__global__ void coarse_prolong_kernel(int N, const int *__restrict__ cbody, const int *__restrict__ body_start,
-                                      const int *__restrict__ members, const double *__restrict__ zq,
-                                      const double *__restrict__ zp, const double *__restrict__ y,
-                                      double *__restrict__ z) {
-    const int a = blockIdx.x, ba = cbody[a];
+__device__ __forceinline__ void coarse_prolong_body(int a, int N, const int *__restrict__ cbody,
+                                                    const int *__restrict__ body_start,
+                                                    const int *__restrict__ members, const double *__restrict__ zq,
+                                                    const double *__restrict__ zp, const double *__restrict__ y,
+                                                    double *__restrict__ z) {
+    const int ba = cbody[a];
     const int beg = body_start[ba], nb = body_start[ba + 1] - beg;
     const double y0 = y[3 * a], y1 = y[3 * a + 1], y2 = y[3 * a + 2];
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
@@ -935,6 +974,72 @@ __global__ void coarse_prolong_kernel(int N, const int *__restrict__ cbody, cons
         z[i] += zq[3 * i] * y0 + zq[3 * i + 1] * y1 + zq[3 * i + 2] * y2;
     }
     if (threadIdx.x == 0) z[N + ba] += zp[3 * ba] * y0 + zp[3 * ba + 1] * y1 + zp[3 * ba + 2] * y2;
+}
+
+__global__ void coarse_prolong_kernel(int N, const int *__restrict__ cbody, const int *__restrict__ body_start,
+                                      const int *__restrict__ members, const double *__restrict__ zq,
+                                      const double *__restrict__ zp, const double *__restrict__ y,
+                                      double *__restrict__ z) {
+    coarse_prolong_body(blockIdx.x, N, cbody, body_start, members, zq, zp, y, z);
+}
+
+// ---- lockstep batches: the same bodies, one CTA per (replica, item) of the replicas
+// whose coarse level is active ----
+__global__ void restrict_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                      const int *__restrict__ mask, int xin) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &r = reps[it.x];
+    if (!r.coarse) return;
+    coarse_restrict_body(it.y, r.N, r.cbody, r.body_start, r.body_members, r.zq, r.zpv, r.vec[xin], r.cg);
+}
+
+__global__ void gemv_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                  const int *__restrict__ mask) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &r = reps[it.x];
+    if (!r.coarse) return;
+    coarse_gemv_block(it.y, r.nc, r.np, r.Ci, r.cg, r.cy);
+}
+
+__global__ void __launch_bounds__(256) fpart_batch_kernel(const BatchRep *__restrict__ reps,
+                                                          const int2 *__restrict__ items,
+                                                          const int *__restrict__ mask) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &r = reps[it.x];
+    if (!r.coarse || r.nmodes == 0) return;
+    fcol_partial_chunk(it.y, r.nc, r.K2, r.F, r.cy, r.fpart);
+}
+
+__global__ void freduce_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                     const int *__restrict__ mask) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &r = reps[it.x];
+    if (!r.coarse || r.nmodes == 0) return;
+    fcol_reduce_block<float>(it.y, (r.nc + kColRows - 1) / kColRows, r.K2, r.fpart, r.nmodes, r.kv, r.cu);
+}
+
+__global__ void model_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                   const int *__restrict__ mask, int xin, int split) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &r = reps[it.x];
+    if (!r.coarse) return;
+    coarse_model_body(it.y, r.N, r.nmodes, r.nrows, r.rows, r.cidx, r.body_start, r.body_members, r.pos64,
+                      make_double3(r.Linv[0], r.Linv[1], r.Linv[2]), r.zq, r.zpv, r.phead, r.pcount, r.pair_b, r.woff,
+                      r.W, r.cu, r.selfc, r.cy, r.vec[xin], r.ct, split);
+}
+
+__global__ void prolong_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                     const int *__restrict__ mask, int zout) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &r = reps[it.x];
+    if (!r.coarse) return;
+    coarse_prolong_body(it.y, r.N, r.cbody, r.body_start, r.body_members, r.zq, r.zpv, r.cy, r.vec[zout]);
 }
 
 template <typename T> int grow(cr_handle *h, T **p, size_t &cap, size_t need, bool &moved) {
@@ -1251,6 +1356,59 @@ int coarse_prepare(cr_handle *h) {
     cs.kc = kc;
     cs.failed = bad != 0;
     cs.active = !cs.failed;
+    return CR_OK;
+}
+
+// The two-level preconditioner of a lockstep batch: the stages of coarse_apply, each one
+// launch over the replicas (a replica without an active coarse level only takes the
+// conductor response of its input).  Replicas share the model kernel's launch shape
+// (the largest body rounded to whole warps, two threads per bead), so the batch requires
+// it to be the same for all of them.
+int batch_coarse_attrs(cr_batch *bt) {
+    static size_t set = 0;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (bt->model_smem > 48 * 1024 && bt->model_smem > set) {
+        CR_TRY(batch_check(bt, cudaFuncSetAttribute(model_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)bt->model_smem),
+                           "model_batch_kernel attribute"));
+        set = bt->model_smem;
+    }
+    return CR_OK;
+}
+
+int batch_coarse(cr_batch *bt, const int *mask, int xin, int zout, cudaStream_t s) {
+    const int split = bt->model_threads > 0 ? bt->model_split : 1;
+    if (bt->n_items[BL_CBODIES] > 0) {
+        restrict_batch_kernel<<<bt->n_items[BL_CBODIES], 128, 0, s>>>(bt->d_reps, bt->d_items[BL_CBODIES], mask, xin);
+        ++bt->launches;
+        CR_TRY(batch_check(bt, cudaGetLastError(), "restrict_batch_kernel"));
+    }
+    if (bt->n_items[BL_GEMV] > 0) {
+        gemv_batch_kernel<<<bt->n_items[BL_GEMV], 256, 0, s>>>(bt->d_reps, bt->d_items[BL_GEMV], mask);
+        ++bt->launches;
+        CR_TRY(batch_check(bt, cudaGetLastError(), "gemv_batch_kernel"));
+    }
+    if (bt->n_items[BL_FCHUNK] > 0) {
+        fpart_batch_kernel<<<bt->n_items[BL_FCHUNK], 256, 0, s>>>(bt->d_reps, bt->d_items[BL_FCHUNK], mask);
+        ++bt->launches;
+        CR_TRY(batch_check(bt, cudaGetLastError(), "fpart_batch_kernel"));
+        freduce_batch_kernel<<<bt->n_items[BL_FCOL], 256, 0, s>>>(bt->d_reps, bt->d_items[BL_FCOL], mask);
+        ++bt->launches;
+        CR_TRY(batch_check(bt, cudaGetLastError(), "freduce_batch_kernel"));
+    }
+    if (bt->n_items[BL_BODIES] > 0 && bt->n_items[BL_CBODIES] > 0) {
+        model_batch_kernel<<<bt->n_items[BL_BODIES], bt->model_threads, bt->model_smem, s>>>(
+            bt->d_reps, bt->d_items[BL_BODIES], mask, xin, split);
+        ++bt->launches;
+        CR_TRY(batch_check(bt, cudaGetLastError(), "model_batch_kernel"));
+    }
+    CR_TRY(batch_conductor(bt, mask, xin, true, zout, s));
+    if (bt->n_items[BL_CBODIES] > 0) {
+        prolong_batch_kernel<<<bt->n_items[BL_CBODIES], 128, 0, s>>>(bt->d_reps, bt->d_items[BL_CBODIES], mask, zout);
+        ++bt->launches;
+        CR_TRY(batch_check(bt, cudaGetLastError(), "prolong_batch_kernel"));
+    }
     return CR_OK;
 }
 

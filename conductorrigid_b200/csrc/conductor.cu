@@ -63,16 +63,19 @@ void chol_solve(const std::vector<double> &l, int n, double *x) {
     }
 }
 
-__global__ void conductor_apply_kernel(int N, int B, const int *__restrict__ body_start,
-                                       const int *__restrict__ members, const int *__restrict__ body_shape,
-                                       const int *__restrict__ shape_n, const long long *__restrict__ shape_mat,
-                                       const int *__restrict__ shape_vec, const double *__restrict__ kinv,
-                                       const double *__restrict__ uvec, const double *__restrict__ inv_s,
-                                       const double *__restrict__ v, double *__restrict__ z) {
+// (body b: the body of conductor_apply_kernel and of its lockstep-batch form)
+__device__ __forceinline__ void conductor_apply_body(int b, int N, const int *__restrict__ body_start,
+                                                     const int *__restrict__ members,
+                                                     const int *__restrict__ body_shape,
+                                                     const int *__restrict__ shape_n,
+                                                     const long long *__restrict__ shape_mat,
+                                                     const int *__restrict__ shape_vec,
+                                                     const double *__restrict__ kinv,
+                                                     const double *__restrict__ uvec,
+                                                     const double *__restrict__ inv_s, const double *__restrict__ v,
+                                                     double *__restrict__ z) {
     extern __shared__ double sh[];
     __shared__ double red[32];
-    const int b = blockIdx.x;
-    if (b >= B) return;
     const int s = body_shape[b];
     const int n = shape_n[s];
     const int beg = body_start[b];
@@ -103,7 +106,38 @@ __global__ void conductor_apply_kernel(int N, int B, const int *__restrict__ bod
     if (threadIdx.x == 0) z[N + b] = phi;
 }
 
+__global__ void conductor_apply_kernel(int N, int B, const int *__restrict__ body_start,
+                                       const int *__restrict__ members, const int *__restrict__ body_shape,
+                                       const int *__restrict__ shape_n, const long long *__restrict__ shape_mat,
+                                       const int *__restrict__ shape_vec, const double *__restrict__ kinv,
+                                       const double *__restrict__ uvec, const double *__restrict__ inv_s,
+                                       const double *__restrict__ v, double *__restrict__ z) {
+    if ((int)blockIdx.x >= B) return;
+    conductor_apply_body(blockIdx.x, N, body_start, members, body_shape, shape_n, shape_mat, shape_vec, kinv, uvec,
+                         inv_s, v, z);
+}
+
+// lockstep batch: one CTA per (replica, body); the input is the coarse level's t for
+// replicas whose coarse level is active when from_coarse is set
+__global__ void conductor_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                       const int *__restrict__ mask, int xin, int from_coarse, int zout) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &r = reps[it.x];
+    const double *v = from_coarse && r.coarse ? r.ct : r.vec[xin];
+    conductor_apply_body(it.y, r.N, r.body_start, r.body_members, r.body_shape, r.shape_n, r.shape_mat, r.shape_vec,
+                         r.kinv, r.uvec, r.inv_s, v, r.vec[zout]);
+}
+
 }  // namespace
+
+int batch_conductor(cr_batch *bt, const int *mask, int xin, bool from_coarse, int zout, cudaStream_t s) {
+    if (bt->n_items[BL_BODIES] == 0) return CR_OK;
+    conductor_batch_kernel<<<bt->n_items[BL_BODIES], bt->cond_threads, bt->cond_smem, s>>>(
+        bt->d_reps, bt->d_items[BL_BODIES], mask, xin, from_coarse ? 1 : 0, zout);
+    ++bt->launches;
+    return batch_check(bt, cudaGetLastError(), "conductor_batch_kernel");
+}
 
 void conductor_free(cr_handle *h) {
     dfree(&h->cond.d_body_shape);

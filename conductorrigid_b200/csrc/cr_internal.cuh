@@ -232,6 +232,104 @@ struct CoarseSpace {
            cap_u = 0, cap_t = 0, cap_rows = 0;
 };
 
+// ---- lockstep batches (batchsolve.cu) ----------------------------------------------
+// One replica of a lockstep batch: the addresses and constants every batched kernel reads
+// for it, copied from its handle after the replica's set-up.  A batched kernel runs one
+// CTA per work item (replica, local block) and calls the same per-block body as the
+// single-system kernel with this replica's arguments.
+enum BatchVec { BV_V = 0, BV_Z, BV_W, BV_R, BV_B, BV_X, BV_RR, BV_SIN, BV_SZ, BV_COUNT };
+
+struct BatchRep {
+    int N, B, n, vblk;               // beads, bodies, unknowns, blocks of the vector kernels
+    int ntiles, nclus, m, pad0;      // mesh tiles, 32-bead clusters, restart length
+    int Ng[3], ntd[3], zp32, zp64;   // mesh nodes and tiles per dimension, contraction pitches
+    int coarse, nbc, nc, np;         // two-level coarse level (coarse = 1: active, dense)
+    int nmodes, K2, nrows, pad1;
+    long long goff, soff;            // the replica's mesh and half spectrum in the batch buffers
+    double hm[3], halfL[3], inv_eta[3];
+    double xiterm, prefac, coeff_phi, selfc;
+    double Linv[3];
+    // geometry
+    const float4 *pos32;
+    const double4 *pos64;
+    const int4 *wstart;
+    const int *tile_start, *tile_beads;
+    float *q32, *phi32;
+    double *q64, *phi64;
+    // real space (stored values)
+    const long long *head, *voff;
+    const int *count, *pair_j, *members, *slots;
+    const unsigned *masks;
+    const float *vals32;
+    const double *vals64;
+    float *acc32;
+    double *acc64;
+    const uint32_t *body;
+    // bodies and preconditioners
+    const int *body_start, *body_members, *bsize;
+    const uint8_t *rigid;
+    const int *body_shape, *shape_n, *shape_vec;
+    const long long *shape_mat;
+    const double *kinv, *uvec, *inv_s;
+    const int *cbody, *cidx, *phead, *pcount, *pair_b;
+    const long long *woff;
+    const double *zq, *zpv;
+    const float *W, *Ci, *F;
+    const float4 *kv;
+    const int4 *rows;
+    double *cg, *cy, *fpart, *ct;
+    float *cu;
+    // Krylov workspace of the replica's handle
+    double *vec[BV_COUNT];
+    double *partial, *hcol, *yvec, *H, *cs, *sn, *g;
+};
+
+// The precision-dependent arrays of a batch replica.
+template <typename R> __device__ __forceinline__ const typename Prec<R>::R4 *brep_pos(const BatchRep &b) {
+    if constexpr (sizeof(R) == 4) return b.pos32;
+    else return b.pos64;
+}
+template <typename R> __device__ __forceinline__ R *brep_q(const BatchRep &b) {
+    if constexpr (sizeof(R) == 4) return b.q32;
+    else return b.q64;
+}
+template <typename R> __device__ __forceinline__ R *brep_phi(const BatchRep &b) {
+    if constexpr (sizeof(R) == 4) return b.phi32;
+    else return b.phi64;
+}
+template <typename R> __device__ __forceinline__ const R *brep_vals(const BatchRep &b) {
+    if constexpr (sizeof(R) == 4) return b.vals32;
+    else return b.vals64;
+}
+template <typename R> __device__ __forceinline__ R *brep_acc(const BatchRep &b) {
+    if constexpr (sizeof(R) == 4) return b.acc32;
+    else return b.acc64;
+}
+
+// Work lists of the batched kernels: item k = (replica, local block) of CTA k.
+enum BatchList {
+    BL_TILES = 0,   // mesh tiles
+    BL_CLUSTERS,    // 32-bead clusters
+    BL_CLELEMS,     // cluster slots, 256 per block
+    BL_VEC,         // vector blocks (vblk per replica, grid-stride over the replica's rows)
+    BL_BODYWARPS,   // bodies, 8 per block (one warp each)
+    BL_BODIES,      // bodies, one per block
+    BL_CBODIES,     // coarse bodies, one per block
+    BL_GEMV,        // coarse rows, 8 per block (one warp each)
+    BL_FCHUNK,      // 8-row chunks of the structure factors
+    BL_FCOL,        // structure-factor columns, 8 per block (one warp each)
+    BL_COUNT
+};
+
+// Replicas of one mesh size: consecutive in the batch mesh buffers, transformed by one
+// batched cuFFT plan per direction and precision ([0] FP64, [1] FP32).
+struct BatchFftGroup {
+    int grid[3] = {0, 0, 0};
+    long long goff = 0, soff = 0;
+    std::vector<int> reps;
+    cufftHandle fwd[2] = {0, 0}, inv[2] = {0, 0};
+};
+
 // Kernel classes timed by the built-in profiler (CUDA events on the handle's stream).
 enum ProfId {
     PROF_SPREAD = 0,
@@ -257,6 +355,48 @@ struct Profiler {
 };
 
 }  // namespace cr
+
+// A lockstep batch over existing handles (batchsolve.cu).
+struct cr_batch {
+    int n = 0;
+    std::vector<cr_handle *> handles;
+    std::string last_error;
+    int support = 0, m = 0, precision = 0, precond = 0;
+    cudaStream_t stream = nullptr, side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev0 = nullptr, ev1 = nullptr;
+    // per-replica descriptors
+    std::vector<cr::BatchRep> reps;
+    cr::BatchRep *d_reps = nullptr;
+    // work lists
+    int2 *d_items[cr::BL_COUNT] = {};
+    int n_items[cr::BL_COUNT] = {};
+    size_t cap_items[cr::BL_COUNT] = {};
+    std::vector<int2> h_items;
+    // stage masks: [0] Arnoldi step, [1] cycle end, [2] cycle start, [3] all
+    int *d_mask = nullptr;
+    int *h_mask = nullptr;           // pinned [4 n]
+    // batch mesh buffers (every replica's mesh and half spectrum, grouped by size)
+    long long G = 0, S = 0;
+    float *grid32 = nullptr, *scale32 = nullptr;
+    double *grid64 = nullptr, *scale64 = nullptr;
+    cufftComplex *spec32 = nullptr;
+    cufftDoubleComplex *spec64 = nullptr;
+    std::vector<cr::BatchFftGroup> groups;
+    std::vector<int> rep_group;      // group of each replica
+    int contract_threads = 256;
+    size_t contract_smem32 = 0, contract_smem64 = 0;
+    int cond_threads = 64;
+    size_t cond_smem = 0;
+    int model_threads = 128, model_split = 1;
+    size_t model_smem = 0;
+    // solver state (device, contiguous over replicas) and its pinned mirrors
+    void *d_state = nullptr, *h_state = nullptr;  // [n] Arnoldi states
+    double *d_norm2 = nullptr, *h_norm2 = nullptr; // [n] squared norms
+    double *d_scal = nullptr, *h_scal = nullptr;   // [2 n] per-replica scalars of a stage
+    long long launches = 0, fft_execs = 0, steps = 0;
+    double phase_ms[3] = {0, 0, 0};  // last solve: per-replica set-up, lockstep loop, force pass (host clock)
+    std::vector<double> h_grid_check;  // derived grid and box of each replica at creation
+};
 
 struct cr_handle {
     cr_params user{};
@@ -455,5 +595,27 @@ int brownian_step(cr_handle *h, const cr_brownian_params *bp, long long step, co
                   const double *force, double *pos, double *bpos);
 int krylov_alloc(cr_handle *h);
 void krylov_free(cr_handle *h);
+
+// ---- lockstep batch stages: one launch per stage over the replicas whose entry in the
+// mask (device, [n]) is nonzero; xin / yout select vectors of the Krylov workspace ----
+int batch_fail(cr_batch *bt, int status, const std::string &msg);
+int batch_check(cr_batch *bt, cudaError_t e, const char *what);
+// charges of the input vector into the operator precision (mesh.cu)
+template <typename R> int batch_cast(cr_batch *bt, const int *mask, int xin, cudaStream_t s);
+// wave-space potential: spread, transforms by size group, influence function, contract
+// (mesh.cu); group_live[g] = 0 skips a size group whose replicas are all masked out
+template <typename R> int batch_wave(cr_batch *bt, const int *mask, const std::vector<char> &group_live, cudaStream_t s);
+// real-space sums into the rows of yout (realspace.cu), then the full rows
+template <typename R> int batch_real(cr_batch *bt, const int *mask, int yout, cudaStream_t s);
+template <typename R> int batch_rows(cr_batch *bt, const int *mask, int xin, int yout, cudaStream_t s);
+// body rows yout[N + b] = sum of xin over body b (body.cu)
+int batch_body_sums(cr_batch *bt, const int *mask, int xin, int yout, cudaStream_t s);
+// the batch's preconditioner zout = P xin (body.cu, conductor.cu, coarse.cu)
+int batch_diag(cr_batch *bt, const int *mask, int xin, int zout, cudaStream_t s);
+int batch_conductor(cr_batch *bt, const int *mask, int xin, bool from_coarse, int zout, cudaStream_t s);
+int batch_coarse(cr_batch *bt, const int *mask, int xin, int zout, cudaStream_t s);
+// dynamic shared memory of the batched kernels (process-wide attributes, only grown)
+int batch_mesh_attrs(cr_batch *bt);
+int batch_coarse_attrs(cr_batch *bt);
 
 }  // namespace cr

@@ -148,9 +148,10 @@ __global__ void __launch_bounds__(256) spread_tiles_kernel(
 // already shifted to the column's x index and scaled by prefac q), then every thread adds
 // the beads whose window covers its column.  No shared-memory atomics; within a tile the
 // summation order is fixed.  The columns are added to the mesh once at the end.
+// (one tile: the body of spread_columns_kernel and of its lockstep-batch form)
 template <typename R, int PT>
-__global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32) spread_columns_kernel(
-    const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
+__device__ __forceinline__ void spread_columns_tile(
+    int tile, const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
     const int *__restrict__ tile_start, const int *__restrict__ tile_beads, MeshShape ms, WindowConst<R> wc,
     R prefac, R *__restrict__ grid) {
     constexpr int P = PT, T = 8, BD = T + PT - 1;
@@ -159,7 +160,6 @@ __global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32) 
     __shared__ R sp[32][3], sc[32];
     __shared__ int4 sst[32];
     __shared__ int sox[32], soy[32], soz[32];
-    const int tile = blockIdx.x;
     const int b0 = tile_start[tile], b1 = tile_start[tile + 1];
     if (b0 == b1) return;
     const int t = threadIdx.x;
@@ -236,9 +236,18 @@ __global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32) 
     }
 }
 
-template <typename R, bool FORCE, int PT>
-__global__ void __launch_bounds__(256) contract_tiles_kernel(
+template <typename R, int PT>
+__global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32) spread_columns_kernel(
     const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
+    const int *__restrict__ tile_start, const int *__restrict__ tile_beads, MeshShape ms, WindowConst<R> wc,
+    R prefac, R *__restrict__ grid) {
+    spread_columns_tile<R, PT>(blockIdx.x, pos, q, wstart, tile_start, tile_beads, ms, wc, prefac, grid);
+}
+
+// (one tile: the body of contract_tiles_kernel and of its lockstep-batch form)
+template <typename R, bool FORCE, int PT>
+__device__ __forceinline__ void contract_tile(
+    int tile, const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
     const int *__restrict__ tile_start, const int *__restrict__ tile_beads, MeshShape ms, WindowConst<R> wc,
     R coeff, const R *__restrict__ grid, R *__restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -252,7 +261,6 @@ __global__ void __launch_bounds__(256) contract_tiles_kernel(
     const int zp = ms.zp;
     const int plane = Bd * zp;
     const int nbuf = Bd * plane;
-    const int tile = blockIdx.x;
     const int b0 = tile_start[tile], b1 = tile_start[tile + 1];
     if (b0 == b1) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -320,6 +328,14 @@ __global__ void __launch_bounds__(256) contract_tiles_kernel(
         }
         __syncwarp();
     }
+}
+
+template <typename R, bool FORCE, int PT>
+__global__ void __launch_bounds__(256) contract_tiles_kernel(
+    const typename Prec<R>::R4 *__restrict__ pos, const R *__restrict__ q, const int4 *__restrict__ wstart,
+    const int *__restrict__ tile_start, const int *__restrict__ tile_beads, MeshShape ms, WindowConst<R> wc,
+    R coeff, const R *__restrict__ grid, R *__restrict__ out) {
+    contract_tile<R, FORCE, PT>(blockIdx.x, pos, q, wstart, tile_start, tile_beads, ms, wc, coeff, grid, out);
 }
 
 template <typename R, typename C>
@@ -688,6 +704,193 @@ int mesh_set_tile(cr_handle *h, int T) {
     if (h->have_topology) CR_TRY(geometry_alloc(h));
     return CR_OK;
 }
+
+// ---- lockstep batches ----------------------------------------------------------------
+// The mesh stages of a batched operator application: the same per-tile bodies as the
+// single-system kernels, one CTA per (replica, tile) item, each replica's mesh and half
+// spectrum in the batch buffers (replicas of one size consecutive, so that one batched
+// cuFFT plan per size transforms them all).
+
+namespace {
+
+template <typename R> __device__ __forceinline__ MeshShape batch_shape(const BatchRep &b, int P) {
+    MeshShape ms;
+    for (int d = 0; d < 3; ++d) {
+        ms.Ng[d] = b.Ng[d];
+        ms.ntd[d] = b.ntd[d];
+    }
+    ms.T = 8;
+    ms.P = P;
+    ms.Bd = 8 + P - 1;
+    ms.zp = sizeof(R) == 4 ? b.zp32 : b.zp64;
+    return ms;
+}
+
+template <typename R> __device__ __forceinline__ WindowConst<R> batch_window(const BatchRep &b) {
+    WindowConst<R> wc;
+    for (int d = 0; d < 3; ++d) {
+        wc.h[d] = (R)b.hm[d];
+        wc.halfL[d] = (R)b.halfL[d];
+        wc.inv_eta[d] = (R)b.inv_eta[d];
+    }
+    wc.xiterm = (R)b.xiterm;
+    return wc;
+}
+
+template <typename R>
+__global__ void cast_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                  const int *__restrict__ mask, int xin) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &b = reps[it.x];
+    const double *in = b.vec[xin];
+    R *out = brep_q<R>(b);
+    for (int i = it.y * blockDim.x + threadIdx.x; i < b.N; i += b.vblk * blockDim.x) out[i] = (R)in[i];
+}
+
+template <typename R, int PT>
+__global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32)
+    spread_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items, const int *__restrict__ mask,
+                        R *__restrict__ grid) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &b = reps[it.x];
+    spread_columns_tile<R, PT>(it.y, brep_pos<R>(b), brep_q<R>(b), b.wstart, b.tile_start, b.tile_beads,
+                               batch_shape<R>(b, PT), batch_window<R>(b), (R)b.prefac, grid + b.goff);
+}
+
+template <typename R, int PT>
+__global__ void __launch_bounds__(256) contract_batch_kernel(const BatchRep *__restrict__ reps,
+                                                             const int2 *__restrict__ items,
+                                                             const int *__restrict__ mask, const R *__restrict__ grid) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &b = reps[it.x];
+    contract_tile<R, false, PT>(it.y, brep_pos<R>(b), brep_q<R>(b), b.wstart, b.tile_start, b.tile_beads,
+                                batch_shape<R>(b, PT), batch_window<R>(b), (R)b.coeff_phi, grid + b.goff,
+                                brep_phi<R>(b));
+}
+
+// launch helpers: the batch's support selects the compiled kernels
+template <typename R, typename F> int batch_with_support(cr_batch *bt, F f) {
+    if (bt->support == 9) return f(std::integral_constant<int, 9>());
+    if (bt->support == 11) return f(std::integral_constant<int, 11>());
+    return batch_fail(bt, CR_BAD_PARAM, "lockstep batch: support must be 9 or 11");
+}
+
+// A failed batched transform: the cuFFT status, the group, and the stream's own state (an
+// earlier asynchronous error shows there).
+int batch_fft_fail(cr_batch *bt, cufftResult fr, const char *dir, size_t g, cudaStream_t s) {
+    const cudaError_t q = cudaStreamQuery(s);
+    const BatchFftGroup &G = bt->groups[g];
+    return batch_fail(bt, CR_CUDA_ERROR,
+                      std::string("batched ") + dir + " transform failed: cufftResult " + std::to_string((int)fr) +
+                          ", size group " + std::to_string(g) + " (" + std::to_string(G.grid[0]) + "x" +
+                          std::to_string(G.grid[1]) + "x" + std::to_string(G.grid[2]) + ", " +
+                          std::to_string(G.reps.size()) + " replicas), stream: " + cudaGetErrorString(q));
+}
+
+template <typename R> R *batch_grid(cr_batch *bt);
+template <> float *batch_grid<float>(cr_batch *bt) { return bt->grid32; }
+template <> double *batch_grid<double>(cr_batch *bt) { return bt->grid64; }
+template <typename R> typename Prec<R>::C *batch_spec(cr_batch *bt);
+template <> cufftComplex *batch_spec<float>(cr_batch *bt) { return bt->spec32; }
+template <> cufftDoubleComplex *batch_spec<double>(cr_batch *bt) { return bt->spec64; }
+template <typename R> R *batch_scale(cr_batch *bt);
+template <> float *batch_scale<float>(cr_batch *bt) { return bt->scale32; }
+template <> double *batch_scale<double>(cr_batch *bt) { return bt->scale64; }
+
+}  // namespace
+
+// Contraction buffers of the batch (the same tile and support for every replica).
+int batch_mesh_attrs(cr_batch *bt) {
+    static size_t set32[2] = {0, 0}, set64[2] = {0, 0};
+    std::lock_guard<std::mutex> lk(g_smem_mu);
+    const int P = bt->support, Bd = 8 + P - 1;
+    bt->contract_smem32 = ((size_t)Bd * Bd * contract_pitch(8, P, 4) + 8 * 6 * (size_t)P) * 4;
+    bt->contract_smem64 = ((size_t)Bd * Bd * contract_pitch(8, P, 8) + 8 * 6 * (size_t)P) * 8;
+    const int k = P == 9 ? 0 : 1;
+    if (bt->contract_smem32 > set32[k]) {
+        CR_TRY(batch_check(bt,
+                           cudaFuncSetAttribute(P == 9 ? contract_batch_kernel<float, 9> : contract_batch_kernel<float, 11>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bt->contract_smem32),
+                           "contract_batch_kernel attribute"));
+        set32[k] = bt->contract_smem32;
+    }
+    if (bt->contract_smem64 > set64[k]) {
+        CR_TRY(batch_check(bt,
+                           cudaFuncSetAttribute(P == 9 ? contract_batch_kernel<double, 9>
+                                                       : contract_batch_kernel<double, 11>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bt->contract_smem64),
+                           "contract_batch_kernel attribute"));
+        set64[k] = bt->contract_smem64;
+    }
+    return CR_OK;
+}
+
+template <typename R> int batch_cast(cr_batch *bt, const int *mask, int xin, cudaStream_t s) {
+    if (bt->n_items[BL_VEC] == 0) return CR_OK;
+    cast_batch_kernel<R><<<bt->n_items[BL_VEC], 256, 0, s>>>(bt->d_reps, bt->d_items[BL_VEC], mask, xin);
+    ++bt->launches;
+    return batch_check(bt, cudaGetLastError(), "cast_batch_kernel");
+}
+
+template <typename R>
+int batch_wave(cr_batch *bt, const int *mask, const std::vector<char> &group_live, cudaStream_t s) {
+    const int slot = sizeof(R) == 4 ? 1 : 0;
+    R *grid = batch_grid<R>(bt);
+    typename Prec<R>::C *spec = batch_spec<R>(bt);
+    CR_TRY(batch_check(bt, cudaMemsetAsync(grid, 0, (size_t)bt->G * sizeof(R), s), "batch mesh clear"));
+    const int nt = bt->n_items[BL_TILES];
+    CR_TRY(batch_with_support<R>(bt, [&](auto pt) -> int {
+        constexpr int PT = decltype(pt)::value;
+        constexpr int BD = 8 + PT - 1;
+        if (nt > 0) {
+            spread_batch_kernel<R, PT><<<nt, (BD * BD + 31) / 32 * 32, 0, s>>>(bt->d_reps, bt->d_items[BL_TILES], mask,
+                                                                              grid);
+            ++bt->launches;
+            CR_TRY(batch_check(bt, cudaGetLastError(), "spread_batch_kernel"));
+        }
+        return CR_OK;
+    }));
+    for (size_t g = 0; g < bt->groups.size(); ++g) {
+        if (!group_live[g]) continue;
+        BatchFftGroup &G = bt->groups[g];
+        cufftResult fr = cufftSetStream(G.fwd[slot], s);
+        if (fr == CUFFT_SUCCESS) fr = fft_forward(G.fwd[slot], grid + G.goff, spec + G.soff);
+        if (fr != CUFFT_SUCCESS) return batch_fft_fail(bt, fr, "forward", g, s);
+        ++bt->fft_execs;
+    }
+    const long long S = bt->S;
+    if (S > 0) {
+        scale_kernel<R, typename Prec<R>::C><<<blocks_for(S, 256), 256, 0, s>>>(spec, batch_scale<R>(bt), (int)S);
+        ++bt->launches;
+        CR_TRY(batch_check(bt, cudaGetLastError(), "scale_kernel (batch)"));
+    }
+    for (size_t g = 0; g < bt->groups.size(); ++g) {
+        if (!group_live[g]) continue;
+        BatchFftGroup &G = bt->groups[g];
+        cufftResult fr = cufftSetStream(G.inv[slot], s);
+        if (fr == CUFFT_SUCCESS) fr = fft_inverse(G.inv[slot], spec + G.soff, grid + G.goff);
+        if (fr != CUFFT_SUCCESS) return batch_fft_fail(bt, fr, "inverse", g, s);
+        ++bt->fft_execs;
+    }
+    return batch_with_support<R>(bt, [&](auto pt) -> int {
+        constexpr int PT = decltype(pt)::value;
+        if (nt > 0) {
+            contract_batch_kernel<R, PT><<<nt, 256, sizeof(R) == 4 ? bt->contract_smem32 : bt->contract_smem64, s>>>(
+                bt->d_reps, bt->d_items[BL_TILES], mask, grid);
+            ++bt->launches;
+            CR_TRY(batch_check(bt, cudaGetLastError(), "contract_batch_kernel"));
+        }
+        return CR_OK;
+    });
+}
+
+template int batch_cast<float>(cr_batch *, const int *, int, cudaStream_t);
+template int batch_cast<double>(cr_batch *, const int *, int, cudaStream_t);
+template int batch_wave<float>(cr_batch *, const int *, const std::vector<char> &, cudaStream_t);
+template int batch_wave<double>(cr_batch *, const int *, const std::vector<char> &, cudaStream_t);
 
 template int mesh_init<float>(cr_handle *, MeshBuffers<float> &);
 template int mesh_init<double>(cr_handle *, MeshBuffers<double> &);

@@ -426,22 +426,18 @@ __global__ void gather_cluster_kernel(int n, const int *__restrict__ members, co
 // added in warp order, so the result does not depend on scheduling.
 // FP32: six CTAs per SM (at most 40 registers; 48 warps of loads in flight, 0.864 ->
 // 0.835 ms per application at 162k charges; 32 registers spill and lose it again).
+// (cluster I: the body of pair_spmv_kernel and of its lockstep-batch form)
 template <typename R, int W, int U>
-__global__ void __launch_bounds__(W * 32, sizeof(R) == 4 ? 6 : 1) pair_spmv_kernel(int nclus, const long long *__restrict__ head,
-                                                           const int *__restrict__ count,
-                                                           const int *__restrict__ pair_j,
-                                                           const int *__restrict__ members,
-                                                           const unsigned *__restrict__ masks,
-                                                           const long long *__restrict__ voff,
-                                                           const int *__restrict__ slots,
-                                                           const R *__restrict__ vals, const R *__restrict__ qc,
-                                                           const R *__restrict__ q, const R *__restrict__ phik,
-                                                           double selfc, const double *__restrict__ phi_body,
-                                                           const uint32_t *__restrict__ body,
-                                                           double *__restrict__ out) {
+__device__ __forceinline__ void pair_spmv_cluster(int I, const long long *__restrict__ head,
+                                                  const int *__restrict__ count, const int *__restrict__ pair_j,
+                                                  const int *__restrict__ members, const unsigned *__restrict__ masks,
+                                                  const long long *__restrict__ voff, const int *__restrict__ slots,
+                                                  const R *__restrict__ vals, const R *__restrict__ qc,
+                                                  const R *__restrict__ q, const R *__restrict__ phik, double selfc,
+                                                  const double *__restrict__ phi_body,
+                                                  const uint32_t *__restrict__ body, double *__restrict__ out) {
     __shared__ R part[W][CS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int I = blockIdx.x;
     R yI = 0, yI2 = 0;  // FP32: odd slots into a second sum (half the dependent-add chain)
     const long long h0 = head[I];
     const int n = count[I];
@@ -513,6 +509,23 @@ __global__ void __launch_bounds__(W * 32, sizeof(R) == 4 ? 6 : 1) pair_spmv_kern
             write_row(out, bi, (double)tot, phik, q, selfc, phi_body, body);
         }
     }
+}
+
+template <typename R, int W, int U>
+__global__ void __launch_bounds__(W * 32, sizeof(R) == 4 ? 6 : 1) pair_spmv_kernel(int nclus, const long long *__restrict__ head,
+                                                           const int *__restrict__ count,
+                                                           const int *__restrict__ pair_j,
+                                                           const int *__restrict__ members,
+                                                           const unsigned *__restrict__ masks,
+                                                           const long long *__restrict__ voff,
+                                                           const int *__restrict__ slots,
+                                                           const R *__restrict__ vals, const R *__restrict__ qc,
+                                                           const R *__restrict__ q, const R *__restrict__ phik,
+                                                           double selfc, const double *__restrict__ phi_body,
+                                                           const uint32_t *__restrict__ body,
+                                                           double *__restrict__ out) {
+    pair_spmv_cluster<R, W, U>(blockIdx.x, head, count, pair_j, members, masks, voff, slots, vals, qc, q, phik, selfc,
+                               phi_body, body, out);
 }
 
 // ---- streamed product: a bulk-copy producer warp per CTA ------------------------------
@@ -1574,6 +1587,80 @@ int real_space_virial(cr_handle *h, const double *q64, double *out) {
         for (int e = 0; e < 6; ++e) out[e] += part[(size_t)I * 6 + e];
     return CR_OK;
 }
+
+// ---- lockstep batches ----------------------------------------------------------------
+// The real-space stages of a batched operator application: charges in cluster order, the
+// stored-value product (the same per-cluster body as pair_spmv_kernel) writing the bare
+// sums into the rows of the output vector, then the rows combined with the wave-space
+// part and the self term.
+
+namespace {
+
+template <typename R>
+__global__ void gather_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                    const int *__restrict__ mask) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &b = reps[it.x];
+    const int k = it.y * blockDim.x + threadIdx.x;
+    if (k >= b.nclus * CS) return;
+    const int i = b.members[k];
+    brep_acc<R>(b)[k] = i >= 0 ? brep_q<R>(b)[i] : (R)0;
+}
+
+template <typename R, int W, int U>
+__global__ void __launch_bounds__(W * 32, sizeof(R) == 4 ? 6 : 1)
+    spmv_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items, const int *__restrict__ mask,
+                      int yout) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &b = reps[it.x];
+    pair_spmv_cluster<R, W, U>(it.y, b.head, b.count, b.pair_j, b.members, b.masks, b.voff, b.slots, brep_vals<R>(b),
+                               brep_acc<R>(b), brep_q<R>(b), nullptr, b.selfc, nullptr, b.body, b.vec[yout]);
+}
+
+template <typename R>
+__global__ void rows_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+                                  const int *__restrict__ mask, int xin, int yout) {
+    const int2 it = items[blockIdx.x];
+    if (!mask[it.x]) return;
+    const BatchRep &b = reps[it.x];
+    double *out = b.vec[yout];
+    const double *phi_body = b.vec[xin] + b.N;
+    const R *phik = brep_phi<R>(b), *q = brep_q<R>(b);
+    for (int i = it.y * blockDim.x + threadIdx.x; i < b.N; i += b.vblk * blockDim.x)
+        write_row(out, i, out[i], phik, q, b.selfc, phi_body, b.body);
+}
+
+}  // namespace
+
+template <typename R> int batch_real(cr_batch *bt, const int *mask, int yout, cudaStream_t s) {
+    if (bt->n_items[BL_CLELEMS] > 0) {
+        gather_batch_kernel<R><<<bt->n_items[BL_CLELEMS], 256, 0, s>>>(bt->d_reps, bt->d_items[BL_CLELEMS], mask);
+        ++bt->launches;
+        CR_TRY(batch_check(bt, cudaGetLastError(), "gather_batch_kernel"));
+    }
+    if (bt->n_items[BL_CLUSTERS] > 0) {
+        constexpr int W = kSpmvWarps;
+        spmv_batch_kernel<R, W, 16><<<bt->n_items[BL_CLUSTERS], W * 32, 0, s>>>(bt->d_reps, bt->d_items[BL_CLUSTERS],
+                                                                                mask, yout);
+        ++bt->launches;
+        CR_TRY(batch_check(bt, cudaGetLastError(), "spmv_batch_kernel"));
+    }
+    return CR_OK;
+}
+
+template <typename R> int batch_rows(cr_batch *bt, const int *mask, int xin, int yout, cudaStream_t s) {
+    if (bt->n_items[BL_VEC] == 0) return CR_OK;
+    rows_batch_kernel<R><<<bt->n_items[BL_VEC], 256, 0, s>>>(bt->d_reps, bt->d_items[BL_VEC], mask, xin, yout);
+    ++bt->launches;
+    return batch_check(bt, cudaGetLastError(), "rows_batch_kernel");
+}
+
+template int batch_real<float>(cr_batch *, const int *, int, cudaStream_t);
+template int batch_real<double>(cr_batch *, const int *, int, cudaStream_t);
+template int batch_rows<float>(cr_batch *, const int *, int, int, cudaStream_t);
+template int batch_rows<double>(cr_batch *, const int *, int, int, cudaStream_t);
 
 template int real_space_apply<float>(cr_handle *, MeshBuffers<float> &, const double *, double *, bool);
 template int real_space_apply<double>(cr_handle *, MeshBuffers<double> &, const double *, double *, bool);

@@ -408,6 +408,45 @@ int cr_batch_compute(int n, cr_handle *const *handles, const double *const *d_po
                      double *const *d_q, double *const *d_phi, double *const *d_force, cr_solve_stats *stats,
                      int *status, int n_threads);
 
+/* ---- lockstep batches: all replicas advanced together, one launch per stage ----
+ * No single counterpart in the reference, which solves one system per computeForces
+ * (ConductorRigid.cu:1153-1286); each replica is solved by that path
+ * (MatrixVectorSolve, ConductorRigid.cu:1051-1151, with the operator of
+ * ConductorRigid.cu:862-1020).
+ *
+ * cr_batch_create groups n existing handles (each with its topology set) into a batch
+ * whose solves advance every unconverged replica by one Arnoldi step per round, each
+ * stage of the step (preconditioner, charge cast, spreading, the transforms of each mesh
+ * size, influence function, contraction, real-space product, rows, body sums,
+ * Gram-Schmidt, Givens rotations) one kernel launch over all replicas.  The members must
+ * share the precision (CR_MIXED or CR_FP64), preconditioner, restart length and support
+ * (9 or 11), use 8^3 mesh tiles with register-column spreading (the default tiling),
+ * stored real-space values with the direct product, and no learned start or correction;
+ * cr_batch_create returns CR_BAD_PARAM otherwise (message from cr_batch_last_error(NULL)
+ * on the calling thread).  The batch keeps each replica's mesh size, box and influence
+ * function as they were at creation: after cr_set_params on a member, make a new batch.
+ * The handles stay owned by the caller and must outlive the batch; do not use them
+ * concurrently with cr_batch_solve. */
+typedef struct cr_batch cr_batch;
+int cr_batch_create(int n, cr_handle *const *handles, cr_batch **out);
+int cr_batch_destroy(cr_batch *batch);
+const char *cr_batch_last_error(const cr_batch *batch);
+/* Solve every replica (arguments as cr_batch_compute: per-replica device arrays; d_q and
+ * d_phi hold the start and receive the solution, d_force the forces).  Per-geometry work
+ * (geometry, stored values, coarse level) and the FP64 force pass run per replica on
+ * n_threads host threads (<= 0: 16) with one stream each; the iterations run in lockstep
+ * on the batch's own streams.  status[i] receives each replica's status, stats (may be
+ * NULL) its statistics (solve_ms: the lockstep loop, the same for all replicas); the
+ * return value is the worst status. */
+int cr_batch_solve(cr_batch *batch, const double *const *d_pos, const double *const *d_body_pos,
+                   double *const *d_q, double *const *d_phi, double *const *d_force, cr_solve_stats *stats,
+                   int *status, int n_threads);
+/* Batched kernel launches, batched transforms and lockstep rounds since creation. */
+int cr_batch_counters(const cr_batch *batch, long long *kernel_launches, long long *fft_execs, long long *steps);
+/* Host-clock durations of the last cr_batch_solve: per-replica set-up, the lockstep
+ * iterations, the per-replica force pass (each phase ends with the device idle). */
+int cr_batch_phase_ms(const cr_batch *batch, double *setup_ms, double *loop_ms, double *force_ms);
+
 /* ---- spreading without device allocation ----
  * No counterpart in the reference.  For callers that cannot allocate device memory
  * where they need the charge mesh: a host engine that owns all device memory through
