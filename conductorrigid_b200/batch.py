@@ -139,10 +139,11 @@ class Replicas:
         return a.value, b.value, c.value
 
     def lockstep_phases(self):
-        """Host-clock ms of the last lockstep solve: set-up, iterations, force pass."""
+        """Last lockstep solve: ms until the first replica joined the rounds, ms of the
+        rounds from then on (device), ms of the whole call (host)."""
         a, b, c = C.c_double(), C.c_double(), C.c_double()
         _lib.lib().cr_batch_phase_ms(self.make_lockstep(), C.byref(a), C.byref(b), C.byref(c))
-        return {"setup": a.value, "iterations": b.value, "forces": c.value}
+        return {"first_join": a.value, "rounds": b.value, "total": c.value}
 
     def set_tilings(self, tilings):
         for h, t in zip(self.handles, tilings):

@@ -32,8 +32,12 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <functional>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -329,90 +333,60 @@ enum Phase { kIdle = 0, kStart, kArnoldi, kEnd, kDone };
 struct Run {
     int phase = kIdle;
     int status = CR_OK;
-    double bnorm = 0, atol = 0, rnorm = 0;
+    double tol = 0, bnorm = 0, atol = 0, rnorm = 0;
+    int maxit = 0;
+    bool force_queued = false;
     int outer = 0;
     cr_solve_stats s{};
 };
 
-// The per-replica work that runs once per solve, on `threads` host threads with one
-// stream each, largest replicas first.
-template <typename F> int for_replicas(cr_batch *bt, int n_threads, const std::vector<int> &which, F f) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        cudaGetLastError();
-        return batch_fail(bt, CR_CUDA_ERROR, "cudaGetDevice failed");
-    }
-    const int T = std::max(1, std::min((int)which.size(), n_threads > 0 ? n_threads : 16));
-    std::vector<cudaStream_t> streams(T, nullptr);
-    for (int t = 0; t < T; ++t)
-        if (cudaStreamCreateWithFlags(&streams[t], cudaStreamNonBlocking) != cudaSuccess) {
-            cudaGetLastError();
-            for (int u = 0; u < t; ++u) cudaStreamDestroy(streams[u]);
-            return batch_fail(bt, CR_CUDA_ERROR, "stream creation failed");
-        }
-    std::vector<int> order(which);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        return bt->handles[a]->N + bt->handles[a]->B > bt->handles[b]->N + bt->handles[b]->B;
-    });
-    std::atomic<int> next(0);
-    auto worker = [&](int t) {
-        cudaSetDevice(dev);
-        for (int k = next++; k < (int)order.size(); k = next++) {
-            const int i = order[k];
-            cr_handle *h = bt->handles[i];
-            cudaStream_t saved = h->stream;
-            h->stream = streams[t];
-            f(i, h);
-            cudaStreamSynchronize(streams[t]);
-            h->stream = saved;
-        }
-    };
-    std::vector<std::thread> pool;
-    pool.reserve(T - 1);
-    for (int t = 1; t < T; ++t) pool.emplace_back(worker, t);
-    worker(0);
-    for (auto &th : pool) th.join();
-    for (int t = 0; t < T; ++t) cudaStreamDestroy(streams[t]);
-    return CR_OK;
-}
-
-int upload_items(cr_batch *bt, const std::vector<std::vector<int2>> &lists) {
-    size_t total = 0;
-    for (int k = 0; k < BL_COUNT; ++k) total += lists[k].size();
+// Upload the work lists of the replicas in `set` (their ranges of h_full) into device slot
+// `slot` (the buffer only grows, by half again, so that a growing batch reallocates rarely).
+int upload_slot(cr_batch *bt, int slot, const std::vector<int> &set) {
     bt->h_items.clear();
-    bt->h_items.reserve(total);
     size_t off[BL_COUNT];
     for (int k = 0; k < BL_COUNT; ++k) {
         off[k] = bt->h_items.size();
-        bt->h_items.insert(bt->h_items.end(), lists[k].begin(), lists[k].end());
-        bt->n_items[k] = (int)lists[k].size();
+        for (int i : set) {
+            const long long b = bt->rep_range[k][2 * i], e = bt->rep_range[k][2 * i + 1];
+            bt->h_items.insert(bt->h_items.end(), bt->h_full[k].begin() + b, bt->h_full[k].begin() + e);
+        }
+        bt->slot_n[slot][k] = (int)(bt->h_items.size() - off[k]);
     }
-    if (total > bt->cap_items[0]) {
-        if (bt->d_items[0]) cudaFree(bt->d_items[0]);
-        bt->d_items[0] = nullptr;
-        bt->cap_items[0] = 0;
-        CR_TRY(batch_check(bt, cudaMalloc((void **)&bt->d_items[0], std::max<size_t>(total, 1) * sizeof(int2)),
-                           "work lists"));
-        bt->cap_items[0] = std::max<size_t>(total, 1);
+    const size_t total = bt->h_items.size();
+    if (total > bt->slot_cap[slot]) {
+        if (bt->slot_base[slot]) cudaFree(bt->slot_base[slot]);
+        bt->slot_base[slot] = nullptr;
+        bt->slot_cap[slot] = 0;
+        const size_t cap = std::max<size_t>(total + total / 2, 1024);
+        CR_TRY(batch_check(bt, cudaMalloc((void **)&bt->slot_base[slot], cap * sizeof(int2)), "work lists"));
+        bt->slot_cap[slot] = cap;
     }
-    int2 *base = bt->d_items[0];
-    for (int k = 0; k < BL_COUNT; ++k) bt->d_items[k] = base + off[k];
+    for (int k = 0; k < BL_COUNT; ++k) bt->slot_items[slot][k] = bt->slot_base[slot] + off[k];
     if (total)
-        CR_TRY(batch_check(bt, cudaMemcpyAsync(base, bt->h_items.data(), total * sizeof(int2), cudaMemcpyHostToDevice,
-                                               bt->stream),
+        CR_TRY(batch_check(bt, cudaMemcpyAsync(bt->slot_base[slot], bt->h_items.data(), total * sizeof(int2),
+                                               cudaMemcpyHostToDevice, bt->stream),
                            "work lists upload"));
     return CR_OK;
 }
 
-// Descriptors and work lists of the replicas after their set-up.
-int describe(cr_batch *bt, const std::vector<int> &live) {
-    const int n = bt->n;
-    std::vector<std::vector<int2>> lists(BL_COUNT);
-    bt->cond_threads = 64;
-    bt->cond_smem = 0;
+// The lists the launchers read: slot 0 (the replicas of a join or of cycle ends) or slot 1
+// (the replicas of the current Arnoldi step).
+void use_slot(cr_batch *bt, int slot) {
+    for (int k = 0; k < BL_COUNT; ++k) {
+        bt->d_items[k] = bt->slot_items[slot][k];
+        bt->n_items[k] = bt->slot_n[slot][k];
+    }
+}
+
+// Launch shapes shared by the replicas (reset at the start of every solve).
+struct Shapes {
     int model_bs = -1, model_split = -1;
-    bt->model_smem = 0;
-    for (int i = 0; i < n; ++i) {
+};
+
+// Descriptor of replica i after its set-up; the launch shapes grow to cover it.
+int describe_rep(cr_batch *bt, int i, Shapes &sh) {
+    {
         cr_handle *h = bt->handles[i];
         BatchRep &r = bt->reps[i];
         std::memset(&r, 0, sizeof(BatchRep));
@@ -490,10 +464,10 @@ int describe(cr_batch *bt, const std::vector<int> &live) {
             if (cs.sparse)
                 return batch_fail(bt, CR_BAD_PARAM,
                                   "lockstep batch: a replica's coarse level uses the sparse form (too many bodies)");
-            if (model_bs < 0) {
-                model_bs = cs.bs;
-                model_split = cs.model_split;
-            } else if (cs.bs != model_bs || cs.model_split != model_split) {
+            if (sh.model_bs < 0) {
+                sh.model_bs = cs.bs;
+                sh.model_split = cs.model_split;
+            } else if (cs.bs != sh.model_bs || cs.model_split != sh.model_split) {
                 return batch_fail(bt, CR_BAD_PARAM,
                                   "lockstep batch: replicas' largest bodies differ in warps (coarse model launch shape)");
             }
@@ -541,12 +515,25 @@ int describe(cr_batch *bt, const std::vector<int> &live) {
         r.sn = K.sn;
         r.g = K.g;
     }
-    bt->model_threads = model_bs > 0 ? model_bs * model_split : 128;
-    bt->model_split = model_split > 0 ? model_split : 1;
-    for (int i : live) {
+    bt->model_threads = sh.model_bs > 0 ? sh.model_bs * sh.model_split : 128;
+    bt->model_split = sh.model_split > 0 ? sh.model_split : 1;
+    return CR_OK;
+}
+
+// Work items of the replicas that just joined (kept on the host; each phase uploads the
+// ranges of the replicas taking part) and the descriptor table, uploaded on the batch
+// stream (between rounds: the stream is idle then).
+int publish(cr_batch *bt, const std::vector<int> &joined) {
+    const int n = bt->n;
+    for (int k = 0; k < BL_COUNT; ++k)
+        if (bt->rep_range[k].size() != 2 * (size_t)n) bt->rep_range[k].assign(2 * (size_t)n, 0);
+    for (int i : joined) {
         const BatchRep &r = bt->reps[i];
         auto add = [&](int list, long long count) {
-            for (long long k = 0; k < count; ++k) lists[list].push_back(make_int2(i, (int)k));
+            std::vector<int2> &L = bt->h_full[list];
+            bt->rep_range[list][2 * i] = (long long)L.size();
+            for (long long k = 0; k < count; ++k) L.push_back(make_int2(i, (int)k));
+            bt->rep_range[list][2 * i + 1] = (long long)L.size();
         };
         add(BL_TILES, r.ntiles);
         add(BL_CLUSTERS, r.nclus);
@@ -554,17 +541,12 @@ int describe(cr_batch *bt, const std::vector<int> &live) {
         add(BL_VEC, r.vblk);
         add(BL_BODYWARPS, ((long long)r.B * 32 + kThreads - 1) / kThreads);
         add(BL_BODIES, r.B);
-        if (r.coarse) {
-            add(BL_CBODIES, r.nbc);
-            add(BL_GEMV, ((long long)r.nc * 32 + kThreads - 1) / kThreads);
-            if (r.nmodes > 0) {
-                add(BL_FCHUNK, (r.nc + 7) / 8);
-                add(BL_FCOL, ((long long)r.K2 * 32 + kThreads - 1) / kThreads);
-            }
-        }
+        add(BL_CBODIES, r.coarse ? r.nbc : 0);
+        add(BL_GEMV, r.coarse ? ((long long)r.nc * 32 + kThreads - 1) / kThreads : 0);
+        add(BL_FCHUNK, r.coarse && r.nmodes > 0 ? (r.nc + 7) / 8 : 0);
+        add(BL_FCOL, r.coarse && r.nmodes > 0 ? ((long long)r.K2 * 32 + kThreads - 1) / kThreads : 0);
     }
     CR_TRY(batch_coarse_attrs(bt));
-    CR_TRY(upload_items(bt, lists));
     return batch_check(bt,
                        cudaMemcpyAsync(bt->d_reps, bt->reps.data(), (size_t)n * sizeof(BatchRep),
                                        cudaMemcpyHostToDevice, bt->stream),
@@ -737,38 +719,36 @@ void next_cycle(cr_batch *bt, int i, Run &u, int maxit) {
     u.phase = kStart;
 }
 
-int solve_lockstep(cr_batch *bt, std::vector<Run> &run, const std::vector<int> &live, double *loop_ms) {
+// Initial residuals of the replicas in `newr` (just set up): ||b||, ||x0||, r0 = b - A64 x0
+// (or b from a zero start: A 0 = 0 exactly), CR_MIXED's refinement residual rr = r0, and
+// each replica's first cycle.  Uses the all-replica mask slot for the set.
+int init_replicas(cr_batch *bt, std::vector<Run> &run, const std::vector<int> &newr) {
     const int n = bt->n;
-    const cr_handle *h0 = bt->handles[live.front()];
-    const double tol = h0->user.gmres_tol > 0 ? h0->user.gmres_tol : h0->user.errortol;
-    const int maxit = h0->user.maxiter > 0 ? h0->user.maxiter : 100;
-    const int inner = bt->precision == CR_MIXED ? CR_FP32 : CR_FP64;
     int *hm = bt->h_mask;
     std::memset(hm, 0, (size_t)4 * n * sizeof(int));
-    for (int i : live) hm[kMaskAll * n + i] = 1;
+    for (int i : newr) hm[kMaskAll * n + i] = 1;
     CR_TRY(upload_masks(bt));
-    CR_TRY(batch_check(bt, cudaEventRecord(bt->ev0, bt->stream), "event"));
-    // ||b||, ||x0||
+    CR_TRY(upload_slot(bt, 0, newr));
+    use_slot(bt, 0);
     CR_TRY(batch_norms(bt, kMaskAll, BV_B));
     CR_TRY(batch_check(bt, cudaMemcpyAsync(bt->h_norm2, bt->d_norm2, n * sizeof(double), cudaMemcpyDeviceToHost,
                                            bt->stream),
                        "norm read-back"));
     CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "norms"));
-    for (int i : live) {
+    for (int i : newr) {
         run[i].bnorm = std::sqrt(std::max(0.0, bt->h_norm2[i]));
-        run[i].atol = tol * run[i].bnorm;
+        run[i].atol = run[i].tol * run[i].bnorm;
     }
     CR_TRY(batch_norms(bt, kMaskAll, BV_X));
     CR_TRY(batch_check(bt, cudaMemcpyAsync(bt->h_norm2, bt->d_norm2, n * sizeof(double), cudaMemcpyDeviceToHost,
                                            bt->stream),
                        "norm read-back"));
     CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "norms"));
-    // r0 = b - A64 x0, or b from a zero start (A 0 = 0 exactly)
     bool any_x = false;
-    for (int i : live) {
+    for (int i : newr) {
         const bool nz = std::sqrt(std::max(0.0, bt->h_norm2[i])) != 0.0;
-        hm[kMaskEnd * n + i] = nz ? 1 : 0;        // nonzero starts
-        hm[kMaskStart * n + i] = nz ? 0 : 1;      // zero starts
+        hm[kMaskEnd * n + i] = nz ? 1 : 0;    // nonzero starts
+        hm[kMaskStart * n + i] = nz ? 0 : 1;  // zero starts
         if (nz) ++run[i].s.matvecs_fp64;
         any_x = any_x || nz;
     }
@@ -792,7 +772,7 @@ int solve_lockstep(cr_batch *bt, std::vector<Run> &run, const std::vector<int> &
                                            bt->stream),
                        "norm read-back"));
     CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "initial residual"));
-    for (int i : live) {
+    for (int i : newr) {
         Run &u = run[i];
         u.rnorm = std::sqrt(std::max(0.0, bt->h_norm2[i]));
         u.s.initial_residual = u.bnorm > 0 ? u.rnorm / u.bnorm : u.rnorm;
@@ -801,69 +781,177 @@ int solve_lockstep(cr_batch *bt, std::vector<Run> &run, const std::vector<int> &
             u.phase = kDone;
             continue;
         }
-        next_cycle(bt, i, u, maxit);
-    }
-    // rounds: start the new cycles and take one Arnoldi step; then end the finished cycles
-    for (;;) {
-        bool any_step = false;
-        for (int i = 0; i < n; ++i) {
-            hm[kMaskStart * n + i] = run[i].phase == kStart;
-            if (run[i].phase == kStart) run[i].phase = kArnoldi;
-            hm[kMaskStep * n + i] = run[i].phase == kArnoldi;
-            hm[kMaskEnd * n + i] = 0;
-            any_step = any_step || run[i].phase == kArnoldi;
-        }
-        if (!any_step) break;
-        CR_TRY(upload_masks(bt));
-        CR_TRY(upload_scal(bt));
-        CR_TRY(batch_step(bt, inner));
-        CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "Arnoldi step"));
-        const BState *hs = reinterpret_cast<const BState *>(bt->h_state);
-        bool any_end = false;
-        for (int i = 0; i < n; ++i) {
-            Run &u = run[i];
-            if (u.phase != kArnoldi) continue;
-            if (inner == CR_FP32) ++u.s.matvecs_fp32;
-            else ++u.s.matvecs_fp64;
-            if (hs[i].stop == 2) {
-                u.status = CR_NUMERICAL;
-                u.phase = kDone;
-                continue;
-            }
-            if (hs[i].frozen || u.s.iterations + hs[i].j >= maxit) {
-                u.phase = kEnd;
-                hm[kMaskEnd * n + i] = 1;
-                any_end = true;
-            }
-        }
-        if (!any_end) continue;
-        for (int i = 0; i < n; ++i) hm[kMaskStep * n + i] = hm[kMaskStart * n + i] = 0;
-        CR_TRY(upload_masks(bt));
-        CR_TRY(batch_cycle_end(bt));
-        for (int i = 0; i < n; ++i) {
-            Run &u = run[i];
-            if (u.phase != kEnd) continue;
-            u.s.iterations += hs[i].j;
-            ++u.s.restarts;
-            ++u.s.matvecs_fp64;
-            ++u.outer;
-            u.rnorm = std::sqrt(std::max(0.0, bt->h_norm2[i]));
-            next_cycle(bt, i, u, maxit);
-        }
-    }
-    CR_TRY(batch_check(bt, cudaEventRecord(bt->ev1, bt->stream), "event"));
-    CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "batch solve"));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, bt->ev0, bt->ev1);
-    *loop_ms = ms;
-    for (int i : live) {
-        Run &u = run[i];
-        u.s.final_residual = u.bnorm > 0 ? u.rnorm / u.bnorm : u.rnorm;
-        u.s.converged = u.rnorm <= u.atol ? 1 : 0;
-        if (u.status == CR_OK && !u.s.converged) u.status = CR_NOT_CONVERGED;
+        next_cycle(bt, i, u, u.maxit);
     }
     return CR_OK;
 }
+
+// One lockstep round: start the new cycles, one Arnoldi step of every replica in a cycle,
+// then the ends of the cycles that finished.  Returns false in *any when no replica took
+// part.
+int round_once(cr_batch *bt, std::vector<Run> &run, bool *any) {
+    const int n = bt->n;
+    const int inner = bt->precision == CR_MIXED ? CR_FP32 : CR_FP64;
+    int *hm = bt->h_mask;
+    bool any_step = false;
+    for (int i = 0; i < n; ++i) {
+        hm[kMaskStart * n + i] = run[i].phase == kStart;
+        if (run[i].phase == kStart) run[i].phase = kArnoldi;
+        hm[kMaskStep * n + i] = run[i].phase == kArnoldi;
+        hm[kMaskEnd * n + i] = 0;
+        hm[kMaskAll * n + i] = 0;
+        any_step = any_step || run[i].phase == kArnoldi;
+    }
+    *any = any_step;
+    if (!any_step) return CR_OK;
+    CR_TRY(upload_masks(bt));
+    CR_TRY(upload_scal(bt));
+    // the step's work lists hold only the replicas that take the step
+    std::vector<int> set;
+    for (int i = 0; i < n; ++i)
+        if (hm[kMaskStep * n + i]) set.push_back(i);
+    if (set != bt->step_set) {
+        CR_TRY(upload_slot(bt, 1, set));
+        bt->step_set = set;
+    }
+    use_slot(bt, 1);
+    CR_TRY(batch_step(bt, inner));
+    CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "Arnoldi step"));
+    const BState *hs = reinterpret_cast<const BState *>(bt->h_state);
+    bool any_end = false;
+    for (int i = 0; i < n; ++i) {
+        Run &u = run[i];
+        if (u.phase != kArnoldi) continue;
+        if (inner == CR_FP32) ++u.s.matvecs_fp32;
+        else ++u.s.matvecs_fp64;
+        if (hs[i].stop == 2) {
+            u.status = CR_NUMERICAL;
+            u.phase = kDone;
+            continue;
+        }
+        if (hs[i].frozen || u.s.iterations + hs[i].j >= u.maxit) {
+            u.phase = kEnd;
+            hm[kMaskEnd * n + i] = 1;
+            any_end = true;
+        }
+    }
+    if (!any_end) return CR_OK;
+    std::vector<int> ends;
+    for (int i = 0; i < n; ++i) {
+        hm[kMaskStep * n + i] = hm[kMaskStart * n + i] = 0;
+        if (hm[kMaskEnd * n + i]) ends.push_back(i);
+    }
+    CR_TRY(upload_masks(bt));
+    CR_TRY(upload_slot(bt, 0, ends));
+    use_slot(bt, 0);
+    CR_TRY(batch_cycle_end(bt));
+    for (int i = 0; i < n; ++i) {
+        Run &u = run[i];
+        if (u.phase != kEnd) continue;
+        u.s.iterations += hs[i].j;
+        ++u.s.restarts;
+        ++u.s.matvecs_fp64;
+        ++u.outer;
+        u.rnorm = std::sqrt(std::max(0.0, bt->h_norm2[i]));
+        next_cycle(bt, i, u, u.maxit);
+    }
+    return CR_OK;
+}
+
+// Host threads with one stream each, running per-replica tasks (set-up, force pass) from
+// a queue while the calling thread runs the lockstep rounds.
+class TaskPool {
+public:
+    typedef std::function<void(int, cr_handle *)> Fn;
+    TaskPool(cr_batch *bt, int threads) : bt_(bt) {
+        cudaGetDevice(&dev_);
+        for (int t = 0; t < threads; ++t) {
+            cudaStream_t s = nullptr;
+            if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+                cudaGetLastError();
+                break;
+            }
+            streams_.push_back(s);
+        }
+        for (size_t t = 0; t < streams_.size(); ++t) threads_.emplace_back([this, t] { work(t); });
+    }
+    ~TaskPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &th : threads_) th.join();
+        for (cudaStream_t s : streams_) cudaStreamDestroy(s);
+    }
+    bool ok() const { return !streams_.empty(); }
+    void push(int i, Fn f) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            q_.push_back({i, std::move(f)});
+            ++pending_;
+        }
+        cv_.notify_one();
+    }
+    // Replicas whose tasks finished since the last call (waits up to `wait_ms` for one when
+    // `block` is set and none is there yet).
+    std::vector<int> finished(bool block) {
+        std::unique_lock<std::mutex> lk(mu_);
+        if (block && done_.empty() && pending_ > 0) done_cv_.wait(lk, [this] { return !done_.empty() || pending_ == 0; });
+        std::vector<int> out;
+        out.swap(done_);
+        return out;
+    }
+    int pending() {
+        std::lock_guard<std::mutex> lk(mu_);
+        return pending_;
+    }
+    void drain() {
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [this] { return pending_ == 0; });
+    }
+
+private:
+    struct Task {
+        int i;
+        Fn f;
+    };
+    void work(size_t t) {
+        cudaSetDevice(dev_);
+        for (;;) {
+            Task task;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [this] { return stop_ || !q_.empty(); });
+                if (q_.empty()) return;
+                task = std::move(q_.front());
+                q_.pop_front();
+            }
+            cr_handle *h = bt_->handles[task.i];
+            cudaStream_t saved = h->stream;
+            h->stream = streams_[t];
+            task.f(task.i, h);
+            cudaStreamSynchronize(streams_[t]);
+            h->stream = saved;
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                done_.push_back(task.i);
+                --pending_;
+            }
+            done_cv_.notify_all();
+        }
+    }
+    cr_batch *bt_;
+    int dev_ = 0;
+    std::vector<cudaStream_t> streams_;
+    std::vector<std::thread> threads_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    std::deque<Task> q_;
+    std::vector<int> done_;
+    int pending_ = 0;
+    bool stop_ = false;
+};
 
 // Requirements every member handle meets for the batched kernels (checked at creation
 // and before every solve).
@@ -894,7 +982,8 @@ void destroy_batch(cr_batch *bt) {
             if (G.fwd[p]) cufftDestroy(G.fwd[p]);
             if (G.inv[p]) cufftDestroy(G.inv[p]);
         }
-    for (void *p : {(void *)bt->d_reps, (void *)bt->d_items[0], (void *)bt->d_mask, (void *)bt->grid32,
+    for (void *p : {(void *)bt->d_reps, (void *)bt->slot_base[0], (void *)bt->slot_base[1], (void *)bt->d_mask,
+                    (void *)bt->grid32,
                     (void *)bt->scale32, (void *)bt->grid64, (void *)bt->scale64, (void *)bt->spec32,
                     (void *)bt->spec64, bt->d_state, (void *)bt->d_norm2, (void *)bt->d_scal})
         if (p) cudaFree(p);
@@ -1082,6 +1171,7 @@ int cr_batch_solve(cr_batch *bt, const double *const *d_pos, const double *const
         if (h->B > 0 && (!d_phi[i] || !d_body_pos[i]))
             return batch_fail(bt, CR_BAD_PARAM, "lockstep batch: null body array of replica " + std::to_string(i));
     }
+    bt->last_error.clear();
     using clock = std::chrono::steady_clock;
     auto ms_since = [](clock::time_point t) {
         return std::chrono::duration<double, std::milli>(clock::now() - t).count();
@@ -1089,13 +1179,26 @@ int cr_batch_solve(cr_batch *bt, const double *const *d_pos, const double *const
     const clock::time_point t0 = clock::now();
     bt->phase_ms[0] = bt->phase_ms[1] = bt->phase_ms[2] = 0.0;
     std::vector<Run> run(n);
-    std::vector<int> all(n);
-    std::iota(all.begin(), all.end(), 0);
-    for (int i = 0; i < n; ++i) status[i] = CR_OK;
-    // 1. per-replica set-up: geometry, right-hand side, start, stored values, coarse level
+    for (int i = 0; i < n; ++i) {
+        const cr_handle *h = bt->handles[i];
+        run[i].tol = h->user.gmres_tol > 0 ? h->user.gmres_tol : h->user.errortol;
+        run[i].maxit = h->user.maxiter > 0 ? h->user.maxiter : 100;
+        status[i] = CR_OK;
+    }
+    bt->cond_threads = 64;
+    bt->cond_smem = 0;
+    bt->model_smem = 0;
+    for (int k = 0; k < BL_COUNT; ++k) {
+        bt->h_full[k].clear();
+        bt->rep_range[k].assign(2 * (size_t)n, 0);
+        bt->n_items[k] = 0;
+    }
+    bt->step_set.clear();
+    Shapes shapes;
     const bool mixed = bt->precision == CR_MIXED;
-    CR_TRY(for_replicas(bt, n_threads, all, [&](int i, cr_handle *h) {
-        if (h->N == 0) return;
+    // Per-replica tasks: the set-up of every replica (largest first) and, once it has
+    // converged, its force pass.  status[i] is written by the task's thread only.
+    auto setup = [&](int i, cr_handle *h) {
         int st = geometry_update(h, d_pos[i], d_body_pos[i]);
         Krylov &K = h->kry;
         if (st == CR_OK) st = objective(h, K.b);
@@ -1112,55 +1215,127 @@ int cr_batch_solve(cr_batch *bt, const double *const *d_pos, const double *const
         if (st == CR_OK && bt->precond != CR_PRECOND_DIAGONAL && h->B > 0 && !h->cond.ready)
             st = fail(h, CR_NOT_READY, "conductor preconditioner not set up");
         status[i] = st;
-    }));
-    bt->phase_ms[0] = ms_since(t0);
-    const clock::time_point t1 = clock::now();
-    std::vector<int> live;
+    };
+    auto forces = [&](int i, cr_handle *h) {
+        int st = check_cuda(h, cudaMemcpyAsync(d_q[i], h->kry.x, h->N * sizeof(double), cudaMemcpyDeviceToDevice,
+                                               h->stream),
+                            "solution copy");
+        if (st == CR_OK && h->B)
+            st = check_cuda(h, cudaMemcpyAsync(d_phi[i], h->kry.x + h->N, h->B * sizeof(double),
+                                               cudaMemcpyDeviceToDevice, h->stream),
+                            "solution copy");
+        if (st == CR_OK) st = cast_charges(h, h->m64, h->kry.x);
+        if (st == CR_OK) st = wave_force(h, h->m64);
+        if (st == CR_OK) st = real_space_force(h, h->m64, h->kry.x, d_force[i]);
+        status[i] = st;
+    };
+    std::vector<int> order;
     for (int i = 0; i < n; ++i) {
-        if (status[i] != CR_OK) {
-            run[i].status = status[i];
-            run[i].phase = kDone;
-        } else if (bt->handles[i]->N == 0) {
+        if (bt->handles[i]->N == 0) {
             run[i].phase = kDone;
             run[i].s.converged = 1;
         } else {
-            live.push_back(i);
+            order.push_back(i);
         }
     }
-    double loop_ms = 0.0;
-    if (!live.empty()) {
-        CR_TRY(describe(bt, live));
-        CR_TRY(solve_lockstep(bt, run, live, &loop_ms));
-        // solutions out, then the FP64 force pass per replica
-        for (int i : live) {
-            cr_handle *h = bt->handles[i];
-            CR_TRY(batch_check(bt, cudaMemcpyAsync(d_q[i], h->kry.x, h->N * sizeof(double), cudaMemcpyDeviceToDevice,
-                                                   bt->stream),
-                               "solution copy"));
-            if (h->B)
-                CR_TRY(batch_check(bt, cudaMemcpyAsync(d_phi[i], h->kry.x + h->N, h->B * sizeof(double),
-                                                       cudaMemcpyDeviceToDevice, bt->stream),
-                                   "solution copy"));
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return bt->handles[a]->N + bt->handles[a]->B > bt->handles[b]->N + bt->handles[b]->B;
+    });
+    int err = CR_OK;
+    std::vector<char> in_setup(n, 0), in_force(n, 0);
+    {
+        TaskPool pool(bt, std::max(1, std::min((int)std::max<size_t>(order.size(), 1), n_threads > 0 ? n_threads : 16)));
+        if (!pool.ok()) return batch_fail(bt, CR_CUDA_ERROR, "lockstep batch: no worker stream");
+        for (int i : order) {
+            in_setup[i] = 1;
+            pool.push(i, setup);
         }
-        CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "solution copy"));
-        bt->phase_ms[1] = ms_since(t1);
-        const clock::time_point t2 = clock::now();
-        std::vector<int> ok;
-        for (int i : live)
-            if (run[i].status == CR_OK || run[i].status == CR_NOT_CONVERGED) ok.push_back(i);
-        CR_TRY(for_replicas(bt, n_threads, ok, [&](int i, cr_handle *h) {
-            int st = cast_charges(h, h->m64, h->kry.x);
-            if (st == CR_OK) st = wave_force(h, h->m64);
-            if (st == CR_OK) st = real_space_force(h, h->m64, h->kry.x, d_force[i]);
-            if (st != CR_OK) run[i].status = st;
-        }));
-        bt->phase_ms[2] = ms_since(t2);
+        std::vector<int> live;
+        bool started = false;
+        double first_join_ms = -1.0;
+        // rounds: replicas join once set up, leave for their force pass once converged
+        for (;;) {
+            bool active = false;
+            for (int i = 0; i < n; ++i) active = active || (run[i].phase >= kStart && run[i].phase <= kEnd);
+            std::vector<int> fin = pool.finished(!active);
+            std::vector<int> joined;
+            for (int i : fin) {
+                if (in_setup[i]) {
+                    in_setup[i] = 0;
+                    if (status[i] != CR_OK) {
+                        run[i].status = status[i];
+                        run[i].phase = kDone;
+                    } else if (err == CR_OK) {
+                        err = describe_rep(bt, i, shapes);
+                        if (err == CR_OK) joined.push_back(i);
+                    }
+                } else if (in_force[i]) {
+                    in_force[i] = 0;
+                }
+            }
+            if (err != CR_OK) break;
+            if (!joined.empty()) {
+                if (!started) {
+                    started = true;
+                    first_join_ms = ms_since(t0);
+                    err = batch_check(bt, cudaEventRecord(bt->ev0, bt->stream), "event");
+                    if (err != CR_OK) break;
+                }
+                live.insert(live.end(), joined.begin(), joined.end());
+                err = publish(bt, joined);
+                if (err == CR_OK) err = init_replicas(bt, run, joined);
+                if (err != CR_OK) break;
+            }
+            bool any = false;
+            err = round_once(bt, run, &any);
+            if (err != CR_OK) break;
+            // finished replicas leave for their force pass (also when not converged, as
+            // cr_compute does; not after a numerical failure)
+            for (int i : live)
+                if (run[i].phase == kDone && !run[i].force_queued) {
+                    run[i].force_queued = true;
+                    if (run[i].status == CR_OK) {
+                        in_force[i] = 1;
+                        pool.push(i, forces);
+                    }
+                }
+            if (!any && pool.pending() == 0) {
+                bool waiting = false;
+                for (int i = 0; i < n; ++i) waiting = waiting || in_setup[i] || in_force[i];
+                if (!waiting) break;
+            }
+        }
+        pool.drain();
+        for (int i : pool.finished(false))
+            if (in_force[i]) in_force[i] = 0;
+        bt->phase_ms[0] = first_join_ms;
     }
+    if (err != CR_OK) return err;
+    float loop_ms = 0.f;
+    bool any_live = false;
+    for (int i = 0; i < n; ++i) any_live = any_live || bt->handles[i]->N > 0;
+    if (any_live && bt->phase_ms[0] >= 0.0) {
+        CR_TRY(batch_check(bt, cudaEventRecord(bt->ev1, bt->stream), "event"));
+        CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "batch solve"));
+        if (cudaEventElapsedTime(&loop_ms, bt->ev0, bt->ev1) != cudaSuccess) {
+            cudaGetLastError();
+            loop_ms = 0.f;
+        }
+    }
+    bt->phase_ms[1] = loop_ms;
+    bt->phase_ms[2] = ms_since(t0);
     int worst = CR_OK;
     for (int i = 0; i < n; ++i) {
-        run[i].s.solve_ms = loop_ms;
-        if (stats) stats[i] = run[i].s;
-        status[i] = run[i].status;
+        Run &u = run[i];
+        if (u.force_queued && u.status == CR_OK && status[i] != CR_OK) u.status = status[i];  // force pass failed
+        if (bt->handles[i]->N > 0 && u.status == CR_OK) {
+            u.s.final_residual = u.bnorm > 0 ? u.rnorm / u.bnorm : u.rnorm;
+            u.s.converged = u.rnorm <= u.atol ? 1 : 0;
+            if (!u.s.converged) u.status = CR_NOT_CONVERGED;
+        }
+        u.s.solve_ms = loop_ms;
+        if (stats) stats[i] = u.s;
+        status[i] = u.status;
         if (status[i] != CR_OK && (worst == CR_OK || worst == CR_NOT_CONVERGED)) worst = status[i];
     }
     if (worst != CR_OK && bt->last_error.empty()) bt->last_error = "lockstep batch: a replica failed (see status)";

@@ -367,11 +367,18 @@ struct cr_batch {
     // per-replica descriptors
     std::vector<cr::BatchRep> reps;
     cr::BatchRep *d_reps = nullptr;
-    // work lists
+    // work lists: the lists the launchers read (d_items, n_items) point into one of two
+    // device slots, [0] every live replica, [1] the replicas of the current Arnoldi step
     int2 *d_items[cr::BL_COUNT] = {};
     int n_items[cr::BL_COUNT] = {};
-    size_t cap_items[cr::BL_COUNT] = {};
-    std::vector<int2> h_items;
+    int2 *slot_base[2] = {nullptr, nullptr};
+    size_t slot_cap[2] = {0, 0};
+    int2 *slot_items[2][cr::BL_COUNT] = {};
+    int slot_n[2][cr::BL_COUNT] = {};
+    std::vector<int2> h_items;                     // staging of a slot's upload
+    std::vector<int2> h_full[cr::BL_COUNT];        // items of the live replicas, replica after replica
+    std::vector<long long> rep_range[cr::BL_COUNT];  // [2 n] first and end item of each replica
+    std::vector<int> step_set;                     // replicas of the lists in slot 1
     // stage masks: [0] Arnoldi step, [1] cycle end, [2] cycle start, [3] all
     int *d_mask = nullptr;
     int *h_mask = nullptr;           // pinned [4 n]

@@ -433,9 +433,11 @@ int cr_batch_destroy(cr_batch *batch);
 const char *cr_batch_last_error(const cr_batch *batch);
 /* Solve every replica (arguments as cr_batch_compute: per-replica device arrays; d_q and
  * d_phi hold the start and receive the solution, d_force the forces).  Per-geometry work
- * (geometry, stored values, coarse level) and the FP64 force pass run per replica on
- * n_threads host threads (<= 0: 16) with one stream each; the iterations run in lockstep
- * on the batch's own streams.  status[i] receives each replica's status, stats (may be
+ * (geometry, stored values, coarse level) and the FP64 force pass run per replica as tasks
+ * of n_threads host threads (<= 0: 16) with one stream each, largest replicas first; a
+ * replica joins the lockstep rounds (on the batch's own streams) as soon as its set-up is
+ * done and leaves for its force pass as soon as it has converged, so set-up, iterations
+ * and forces of different replicas overlap on the GPU.  status[i] receives each replica's status, stats (may be
  * NULL) its statistics (solve_ms: the lockstep loop, the same for all replicas); the
  * return value is the worst status. */
 int cr_batch_solve(cr_batch *batch, const double *const *d_pos, const double *const *d_body_pos,
@@ -443,8 +445,9 @@ int cr_batch_solve(cr_batch *batch, const double *const *d_pos, const double *co
                    int *status, int n_threads);
 /* Batched kernel launches, batched transforms and lockstep rounds since creation. */
 int cr_batch_counters(const cr_batch *batch, long long *kernel_launches, long long *fft_execs, long long *steps);
-/* Host-clock durations of the last cr_batch_solve: per-replica set-up, the lockstep
- * iterations, the per-replica force pass (each phase ends with the device idle). */
+/* Timings of the last cr_batch_solve: host-clock ms until the first replica finished its
+ * set-up and joined the rounds, device ms from then to the end (CUDA events on the
+ * batch's stream), host-clock ms of the whole call. */
 int cr_batch_phase_ms(const cr_batch *batch, double *setup_ms, double *loop_ms, double *force_ms);
 
 /* ---- spreading without device allocation ----
