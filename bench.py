@@ -208,12 +208,17 @@ def run_replicas(args) -> None:
         e1.synchronize()
         return e0.elapsed_time(e1), st
 
+    # --arms lockstep: the lockstep arm alone (a launch list of its rounds under ncu)
+    only_lockstep = set(args.arms.split(",")) == {"lockstep"}
     # the looped single-system solve: reference solutions and the looped rate
     for h in R.handles:
         h.set_tiling(8, 0)
-    R.warm()
-    ms_loop, st_loop = timed(R.solve_looped)
-    ref = [tuple(a.clone() for a in arr[2:]) for arr in R.arrays]
+    if only_lockstep:
+        ms_loop, st_loop, ref = None, None, None
+    else:
+        R.warm()
+        ms_loop, st_loop = timed(R.solve_looped)
+        ref = [tuple(a.clone() for a in arr[2:]) for arr in R.arrays]
     # lockstep batch (8^3 register-column tiling, the default)
     for _ in range(args.warmup):
         timed(lambda: R.solve_lockstep(nt))
@@ -222,37 +227,42 @@ def run_replicas(args) -> None:
     l1, f1, r1 = R.lockstep_counters()
     phases = R.lockstep_phases()
     st = ms_lock[-1][1]
-    err = {"q": 0.0, "phi": 0.0, "force": 0.0}
-    for arr, want in zip(R.arrays, ref):
-        for key, a, b in zip(("q", "phi", "force"), arr[2:], want):
-            err[key] = max(err[key], float((a - b).abs().max() / b.abs().max().clamp_min(1e-300)))
+    err = None
+    if ref is not None:
+        err = {"q": 0.0, "phi": 0.0, "force": 0.0}
+        for arr, want in zip(R.arrays, ref):
+            for key, a, b in zip(("q", "phi", "force"), arr[2:], want):
+                err[key] = max(err[key], float((a - b).abs().max() / b.abs().max().clamp_min(1e-300)))
+        err = {k: float(f"{v:.3g}") for k, v in err.items()}
     rounds = (r1 - r0) / args.steps
     t_lock = statistics.median(m for m, _ in ms_lock)
-    # stream batch, tiling policy chosen by its own throughput
-    policy_rates = R.tune_batch(nt)  # untimed set-up
-    for _ in range(args.warmup):
-        timed(lambda: R.solve_batched(nt))
-    ms = [timed(lambda: R.solve_batched(nt)) for _ in range(args.steps)]
-    t_batch = statistics.median(m for m, _ in ms)
-    st_b = ms[-1][1]
+    t_batch, st_b, policy_rates = None, None, {}
+    if not only_lockstep:
+        # stream batch, tiling policy chosen by its own throughput
+        policy_rates = R.tune_batch(nt)  # untimed set-up
+        for _ in range(args.warmup):
+            timed(lambda: R.solve_batched(nt))
+        ms = [timed(lambda: R.solve_batched(nt)) for _ in range(args.steps)]
+        t_batch = statistics.median(m for m, _ in ms)
+        st_b = ms[-1][1]
     groups = len({tuple(h.derived().grid) for h in R.handles})
     line = {
         "metric": "replica solves/s at 1e-6 residual, 256 uneven replicas in one batch",
         "value": round(R.n / (t_lock / 1e3), 2), "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_lock, 2), "higher_is_better": True,
-        "stream_batch_solves_per_s": round(R.n / (t_batch / 1e3), 2),
-        "looped_solves_per_s": round(R.n / (ms_loop / 1e3), 2), "preconditioner": args.precond,
+        "stream_batch_solves_per_s": round(R.n / (t_batch / 1e3), 2) if t_batch else None,
+        "looped_solves_per_s": round(R.n / (ms_loop / 1e3), 2) if ms_loop else None, "preconditioner": args.precond,
         "iterations_mean": round(float(np.mean([s["iterations"] for s in st])), 1),
         "iterations_max": int(max(s["iterations"] for s in st)),
-        "iterations_mean_looped": round(float(np.mean([s["iterations"] for s in st_loop])), 1),
+        "iterations_mean_looped": round(float(np.mean([s["iterations"] for s in st_loop])), 1) if st_loop else None,
         "converged": int(sum(s["converged"] for s in st)),
-        "converged_stream_batch": int(sum(s["converged"] for s in st_b)),
+        "converged_stream_batch": int(sum(s["converged"] for s in st_b)) if st_b else None,
         "max_final_residual": max(s["final_residual"] for s in st),
-        "error_vs_looped": {k: float(f"{v:.3g}") for k, v in err.items()},
+        "error_vs_looped": err,
         "lockstep": {"phase_ms": {k: round(v, 2) for k, v in phases.items()}, "rounds_per_solve": rounds, "kernel_launches_per_round": round((l1 - l0) / args.steps / rounds, 1),
                      "batched_transforms_per_solve": (f1 - f0) / args.steps, "mesh_size_groups": groups},
         "replicas": R.n, "charges": R.n_charges,
-        "host_threads": nt, "tiling_policy_stream_batch": R.best_policy,
+        "host_threads": nt, "tiling_policy_stream_batch": getattr(R, "best_policy", None),
         "tiling_policy_rates": {k: round(v, 1) for k, v in policy_rates.items()},
         "dtype": "f32 operator, f64 Krylov", "data": "synthetic (seeded replica generator)",
         "config": {"workload": "replicas_256: N_body~U[20,400], phi~U[0.05,0.35], |E0|=1, 2 nodes/unit, P=9",
@@ -884,7 +894,8 @@ def main() -> None:
                          "applications in FP32 (small enough for a full ncu capture)")
     ap.add_argument("--arms", default="fast,f64t,f64c,plain",
                     help="arms to run besides the headline one: fast (FP32 operator), f64t (FP64, same "
-                         "preconditioner), f64c (FP64, conductor response), plain (FP64, reference preconditioner)")
+                         "preconditioner), f64c (FP64, conductor response), plain (FP64, reference preconditioner); "
+                         "replicas_256: 'lockstep' runs the lockstep arm alone (no looped or stream-batch arm)")
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=[WORKLOAD, "plain_small", "replicas_256", "dynamics_420k", "mlp", "polydisperse_204k"],
                     help="headline solve (default), the small plain-method system, 256 batched replicas, Brownian "

@@ -600,15 +600,15 @@ int launch_check(cr_batch *bt, const char *what) {
     return batch_check(bt, cudaGetLastError(), what);
 }
 
-// Squared norms of vector v of the replicas of mask `which` into d_norm2.
-int batch_norms(cr_batch *bt, int which, int v) {
+// Squared norms of vector v of the replicas of mask `which` into d_norm2[off + replica].
+int batch_norms(cr_batch *bt, int which, int v, int off = 0) {
     const int *mask = mask_ptr(bt, which);
     BState *st = reinterpret_cast<BState *>(bt->d_state);
     if (bt->n_items[BL_VEC] == 0) return CR_OK;
     dots_kernel<<<bt->n_items[BL_VEC], kThreads, 0, bt->stream>>>(bt->d_reps, bt->d_items[BL_VEC], mask, st, 0, 1, v,
                                                                    v);
     CR_TRY(launch_check(bt, "dots_kernel"));
-    reduce_kernel<<<bt->n, 32, 0, bt->stream>>>(bt->d_reps, bt->n, mask, st, 0, 1, 1, 0, bt->d_norm2);
+    reduce_kernel<<<bt->n, 32, 0, bt->stream>>>(bt->d_reps, bt->n, mask, st, 0, 1, 1, 0, bt->d_norm2 + off);
     return launch_check(bt, "reduce_kernel");
 }
 
@@ -730,8 +730,9 @@ int init_replicas(cr_batch *bt, std::vector<Run> &run, const std::vector<int> &n
     CR_TRY(upload_masks(bt));
     CR_TRY(upload_slot(bt, 0, newr));
     use_slot(bt, 0);
-    CR_TRY(batch_norms(bt, kMaskAll, BV_B));
-    CR_TRY(batch_check(bt, cudaMemcpyAsync(bt->h_norm2, bt->d_norm2, n * sizeof(double), cudaMemcpyDeviceToHost,
+    CR_TRY(batch_norms(bt, kMaskAll, BV_B, 0));
+    CR_TRY(batch_norms(bt, kMaskAll, BV_X, n));
+    CR_TRY(batch_check(bt, cudaMemcpyAsync(bt->h_norm2, bt->d_norm2, 2 * n * sizeof(double), cudaMemcpyDeviceToHost,
                                            bt->stream),
                        "norm read-back"));
     CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "norms"));
@@ -739,14 +740,9 @@ int init_replicas(cr_batch *bt, std::vector<Run> &run, const std::vector<int> &n
         run[i].bnorm = std::sqrt(std::max(0.0, bt->h_norm2[i]));
         run[i].atol = run[i].tol * run[i].bnorm;
     }
-    CR_TRY(batch_norms(bt, kMaskAll, BV_X));
-    CR_TRY(batch_check(bt, cudaMemcpyAsync(bt->h_norm2, bt->d_norm2, n * sizeof(double), cudaMemcpyDeviceToHost,
-                                           bt->stream),
-                       "norm read-back"));
-    CR_TRY(batch_check(bt, cudaStreamSynchronize(bt->stream), "norms"));
     bool any_x = false;
     for (int i : newr) {
-        const bool nz = std::sqrt(std::max(0.0, bt->h_norm2[i])) != 0.0;
+        const bool nz = std::sqrt(std::max(0.0, bt->h_norm2[n + i])) != 0.0;
         hm[kMaskEnd * n + i] = nz ? 1 : 0;    // nonzero starts
         hm[kMaskStart * n + i] = nz ? 0 : 1;  // zero starts
         if (nz) ++run[i].s.matvecs_fp64;
@@ -863,11 +859,16 @@ int round_once(cr_batch *bt, std::vector<Run> &run, bool *any) {
 class TaskPool {
 public:
     typedef std::function<void(int, cr_handle *)> Fn;
+    // The task streams take the highest priority: a set-up is a latency-bound chain of
+    // small kernels that the rounds' full-GPU kernels would otherwise hold back, delaying
+    // the replica's join; the rounds fill the multiprocessors the chains leave free.
     TaskPool(cr_batch *bt, int threads) : bt_(bt) {
         cudaGetDevice(&dev_);
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
         for (int t = 0; t < threads; ++t) {
             cudaStream_t s = nullptr;
-            if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+            if (cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest) != cudaSuccess) {
                 cudaGetLastError();
                 break;
             }
@@ -1051,10 +1052,13 @@ int create_batch(cr_batch *bt, int n, cr_handle *const *handles) {
         return batch_fail(bt, CR_BAD_PARAM, "lockstep batch: the replicas' meshes exceed 2^31 nodes");
     bt->G = G;
     bt->S = S;
-    CR_TRY(batch_check(bt, cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking), "stream"));
+    // rounds at the lowest priority (the per-replica tasks take the highest); the wave part
+    // one level above the real-space product beside it, where the device has the levels
     int lo = 0, hi = 0;
     cudaDeviceGetStreamPriorityRange(&lo, &hi);
-    CR_TRY(batch_check(bt, cudaStreamCreateWithPriority(&bt->side, cudaStreamNonBlocking, hi), "stream"));
+    CR_TRY(batch_check(bt, cudaStreamCreateWithPriority(&bt->stream, cudaStreamNonBlocking, lo), "stream"));
+    CR_TRY(batch_check(bt, cudaStreamCreateWithPriority(&bt->side, cudaStreamNonBlocking, lo > hi ? lo - 1 : lo),
+                       "stream"));
     for (cudaEvent_t *e : {&bt->ev_fork, &bt->ev_join})
         CR_TRY(batch_check(bt, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event"));
     for (cudaEvent_t *e : {&bt->ev0, &bt->ev1}) CR_TRY(batch_check(bt, cudaEventCreate(e), "event"));
@@ -1095,8 +1099,8 @@ int create_batch(cr_batch *bt, int n, cr_handle *const *handles) {
     CR_TRY(batch_check(bt, cudaMallocHost((void **)&bt->h_mask, (size_t)4 * n * sizeof(int)), "masks"));
     CR_TRY(batch_check(bt, cudaMalloc(&bt->d_state, (size_t)n * sizeof(BState)), "states"));
     CR_TRY(batch_check(bt, cudaMallocHost(&bt->h_state, (size_t)n * sizeof(BState)), "states"));
-    CR_TRY(batch_check(bt, cudaMalloc((void **)&bt->d_norm2, (size_t)n * sizeof(double)), "norms"));
-    CR_TRY(batch_check(bt, cudaMallocHost((void **)&bt->h_norm2, (size_t)n * sizeof(double)), "norms"));
+    CR_TRY(batch_check(bt, cudaMalloc((void **)&bt->d_norm2, (size_t)2 * n * sizeof(double)), "norms"));
+    CR_TRY(batch_check(bt, cudaMallocHost((void **)&bt->h_norm2, (size_t)2 * n * sizeof(double)), "norms"));
     CR_TRY(batch_check(bt, cudaMalloc((void **)&bt->d_scal, (size_t)3 * n * sizeof(double)), "scalars"));
     CR_TRY(batch_check(bt, cudaMallocHost((void **)&bt->h_scal, (size_t)3 * n * sizeof(double)), "scalars"));
     std::memset(bt->h_scal, 0, (size_t)3 * n * sizeof(double));

@@ -1022,7 +1022,7 @@ __global__ void freduce_batch_kernel(const BatchRep *__restrict__ reps, const in
     fcol_reduce_block<float>(it.y, (r.nc + kColRows - 1) / kColRows, r.K2, r.fpart, r.nmodes, r.kv, r.cu);
 }
 
-__global__ void model_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
+__global__ void __launch_bounds__(128, 10) model_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items,
                                    const int *__restrict__ mask, int xin, int split) {
     const int2 it = items[blockIdx.x];
     if (!mask[it.x]) return;

@@ -398,7 +398,7 @@ struct cr_batch {
     size_t model_smem = 0;
     // solver state (device, contiguous over replicas) and its pinned mirrors
     void *d_state = nullptr, *h_state = nullptr;  // [n] Arnoldi states
-    double *d_norm2 = nullptr, *h_norm2 = nullptr; // [n] squared norms
+    double *d_norm2 = nullptr, *h_norm2 = nullptr; // [2 n] squared norms
     double *d_scal = nullptr, *h_scal = nullptr;   // [2 n] per-replica scalars of a stage
     long long launches = 0, fft_execs = 0, steps = 0;
     double phase_ms[3] = {0, 0, 0};  // last solve: per-replica set-up, lockstep loop, force pass (host clock)

@@ -748,8 +748,9 @@ __global__ void cast_batch_kernel(const BatchRep *__restrict__ reps, const int2 
     for (int i = it.y * blockDim.x + threadIdx.x; i < b.N; i += b.vblk * blockDim.x) out[i] = (R)in[i];
 }
 
+// (the descriptor's addresses cost registers: bounded to the single kernel's four CTAs per SM)
 template <typename R, int PT>
-__global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32)
+__global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32, sizeof(R) == 4 ? (PT == 9 ? 4 : 2) : 2)
     spread_batch_kernel(const BatchRep *__restrict__ reps, const int2 *__restrict__ items, const int *__restrict__ mask,
                         R *__restrict__ grid) {
     const int2 it = items[blockIdx.x];
@@ -760,7 +761,7 @@ __global__ void __launch_bounds__(((8 + PT - 1) * (8 + PT - 1) + 31) / 32 * 32)
 }
 
 template <typename R, int PT>
-__global__ void __launch_bounds__(256) contract_batch_kernel(const BatchRep *__restrict__ reps,
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) contract_batch_kernel(const BatchRep *__restrict__ reps,
                                                              const int2 *__restrict__ items,
                                                              const int *__restrict__ mask, const R *__restrict__ grid) {
     const int2 it = items[blockIdx.x];
