@@ -107,3 +107,25 @@ def test_compute_requires_topology(product_lib):
     d = C.c_void_p()
     assert lib.cr_destroy(None) == product_lib.CR_BAD_PARAM
     assert lib.cr_create(None, None, C.byref(d)) == product_lib.CR_BAD_PARAM
+
+
+def test_lockstep_batch_argument_checks(product_lib):
+    """The lockstep batch's host-side refusals (no device work): no handles, a null
+    handle, a null batch; the creation message is readable with a NULL batch."""
+    lib = product_lib.lib()
+    out = C.c_void_p(1)
+    assert lib.cr_batch_create(0, None, C.byref(out)) == product_lib.CR_BAD_PARAM
+    assert not out.value
+    assert b"no handles" in lib.cr_batch_last_error(None)
+    assert lib.cr_batch_create(1, None, C.byref(out)) == product_lib.CR_BAD_PARAM
+    assert lib.cr_batch_create(1, (C.c_void_p * 1)(None), None) == product_lib.CR_BAD_PARAM
+    assert lib.cr_batch_create(1, (C.c_void_p * 1)(None), C.byref(out)) == product_lib.CR_BAD_PARAM
+    assert not out.value and b"null handle" in lib.cr_batch_last_error(None)
+    assert lib.cr_batch_destroy(None) == product_lib.CR_BAD_PARAM
+    st = (product_lib.CrSolveStats * 1)()
+    status = (C.c_int * 1)()
+    assert lib.cr_batch_solve(None, None, None, None, None, None, st, status, 1) == product_lib.CR_BAD_PARAM
+    a = C.c_longlong()
+    assert lib.cr_batch_counters(None, C.byref(a), None, None) == product_lib.CR_BAD_PARAM
+    x = C.c_double()
+    assert lib.cr_batch_phase_ms(None, C.byref(x), None, None) == product_lib.CR_BAD_PARAM
