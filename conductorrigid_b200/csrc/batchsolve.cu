@@ -24,10 +24,14 @@
 // whose cycle ends leaves the Arnoldi mask for one round (update, FP64 residual, norm)
 // and re-enters with its next cycle; converged replicas drop out of every mask.
 //
-// Work that runs once per solve stays per replica, on a pool of host threads with one
-// stream each (as in cr_batch_compute): the geometry (tiles, clusters, masks, stored
-// values), the right-hand side, the coarse level of the two-level preconditioner, and
-// the FP64 force pass after the solve.
+// Work that runs once per solve stays per replica, as tasks of a pool of host threads
+// with one stream each: the geometry (tiles, clusters, masks, stored values), the
+// right-hand side, the coarse level of the two-level preconditioner, and the FP64 force
+// pass after the solve.  A replica joins the rounds as soon as its set-up is done and
+// leaves for its force pass as soon as it has converged, so the three overlap on the GPU;
+// the task streams take the highest priority (a set-up is a latency-bound chain of small
+// kernels) and the rounds the lowest.  Each round's work lists hold only the replicas
+// taking part in it.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -1145,11 +1149,11 @@ int cr_batch_destroy(cr_batch *bt) {
 
 const char *cr_batch_last_error(const cr_batch *bt) { return bt ? bt->last_error.c_str() : g_create_error.c_str(); }
 
-int cr_batch_phase_ms(const cr_batch *bt, double *setup_ms, double *loop_ms, double *force_ms) {
+int cr_batch_phase_ms(const cr_batch *bt, double *first_join_ms, double *rounds_ms, double *total_ms) {
     if (!bt) return CR_BAD_PARAM;
-    if (setup_ms) *setup_ms = bt->phase_ms[0];
-    if (loop_ms) *loop_ms = bt->phase_ms[1];
-    if (force_ms) *force_ms = bt->phase_ms[2];
+    if (first_join_ms) *first_join_ms = bt->phase_ms[0];
+    if (rounds_ms) *rounds_ms = bt->phase_ms[1];
+    if (total_ms) *total_ms = bt->phase_ms[2];
     return CR_OK;
 }
 

@@ -401,7 +401,7 @@ struct cr_batch {
     double *d_norm2 = nullptr, *h_norm2 = nullptr; // [2 n] squared norms
     double *d_scal = nullptr, *h_scal = nullptr;   // [2 n] per-replica scalars of a stage
     long long launches = 0, fft_execs = 0, steps = 0;
-    double phase_ms[3] = {0, 0, 0};  // last solve: per-replica set-up, lockstep loop, force pass (host clock)
+    double phase_ms[3] = {0, 0, 0};  // last solve: first join (host), rounds (device), whole call (host)
     std::vector<double> h_grid_check;  // derived grid and box of each replica at creation
 };
 

@@ -448,7 +448,7 @@ int cr_batch_counters(const cr_batch *batch, long long *kernel_launches, long lo
 /* Timings of the last cr_batch_solve: host-clock ms until the first replica finished its
  * set-up and joined the rounds, device ms from then to the end (CUDA events on the
  * batch's stream), host-clock ms of the whole call. */
-int cr_batch_phase_ms(const cr_batch *batch, double *setup_ms, double *loop_ms, double *force_ms);
+int cr_batch_phase_ms(const cr_batch *batch, double *first_join_ms, double *rounds_ms, double *total_ms);
 
 /* ---- spreading without device allocation ----
  * No counterpart in the reference.  For callers that cannot allocate device memory
