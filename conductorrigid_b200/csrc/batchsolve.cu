@@ -347,17 +347,30 @@ struct Run {
 // Upload the work lists of the replicas in `set` (their ranges of h_full) into device slot
 // `slot` (the buffer only grows, by half again, so that a growing batch reallocates rarely).
 int upload_slot(cr_batch *bt, int slot, const std::vector<int> &set) {
-    bt->h_items.clear();
-    size_t off[BL_COUNT];
+    size_t total = 0;
+    for (int k = 0; k < BL_COUNT; ++k)
+        for (int i : set) total += (size_t)(bt->rep_range[k][2 * i + 1] - bt->rep_range[k][2 * i]);
+    // pinned staging (one buffer per slot: the next upload into a slot comes after the
+    // stream synchronisation that ends the phase reading it)
+    if (total > bt->pin_cap[slot]) {
+        if (bt->pin_items[slot]) cudaFreeHost(bt->pin_items[slot]);
+        bt->pin_items[slot] = nullptr;
+        bt->pin_cap[slot] = 0;
+        const size_t cap = std::max<size_t>(total + total / 2, 1024);
+        CR_TRY(batch_check(bt, cudaMallocHost((void **)&bt->pin_items[slot], cap * sizeof(int2)), "work lists"));
+        bt->pin_cap[slot] = cap;
+    }
+    int2 *h = bt->pin_items[slot];
+    size_t off[BL_COUNT], pos = 0;
     for (int k = 0; k < BL_COUNT; ++k) {
-        off[k] = bt->h_items.size();
+        off[k] = pos;
         for (int i : set) {
             const long long b = bt->rep_range[k][2 * i], e = bt->rep_range[k][2 * i + 1];
-            bt->h_items.insert(bt->h_items.end(), bt->h_full[k].begin() + b, bt->h_full[k].begin() + e);
+            if (e > b) std::memcpy(h + pos, bt->h_full[k].data() + b, (size_t)(e - b) * sizeof(int2));
+            pos += (size_t)(e - b);
         }
-        bt->slot_n[slot][k] = (int)(bt->h_items.size() - off[k]);
+        bt->slot_n[slot][k] = (int)(pos - off[k]);
     }
-    const size_t total = bt->h_items.size();
     if (total > bt->slot_cap[slot]) {
         if (bt->slot_base[slot]) cudaFree(bt->slot_base[slot]);
         bt->slot_base[slot] = nullptr;
@@ -368,8 +381,8 @@ int upload_slot(cr_batch *bt, int slot, const std::vector<int> &set) {
     }
     for (int k = 0; k < BL_COUNT; ++k) bt->slot_items[slot][k] = bt->slot_base[slot] + off[k];
     if (total)
-        CR_TRY(batch_check(bt, cudaMemcpyAsync(bt->slot_base[slot], bt->h_items.data(), total * sizeof(int2),
-                                               cudaMemcpyHostToDevice, bt->stream),
+        CR_TRY(batch_check(bt, cudaMemcpyAsync(bt->slot_base[slot], h, total * sizeof(int2), cudaMemcpyHostToDevice,
+                                               bt->stream),
                            "work lists upload"));
     return CR_OK;
 }
@@ -992,7 +1005,8 @@ void destroy_batch(cr_batch *bt) {
                     (void *)bt->scale32, (void *)bt->grid64, (void *)bt->scale64, (void *)bt->spec32,
                     (void *)bt->spec64, bt->d_state, (void *)bt->d_norm2, (void *)bt->d_scal})
         if (p) cudaFree(p);
-    for (void *p : {(void *)bt->h_mask, bt->h_state, (void *)bt->h_norm2, (void *)bt->h_scal})
+    for (void *p : {(void *)bt->h_mask, bt->h_state, (void *)bt->h_norm2, (void *)bt->h_scal,
+                    (void *)bt->pin_items[0], (void *)bt->pin_items[1]})
         if (p) cudaFreeHost(p);
     for (cudaEvent_t e : {bt->ev_fork, bt->ev_join, bt->ev0, bt->ev1})
         if (e) cudaEventDestroy(e);

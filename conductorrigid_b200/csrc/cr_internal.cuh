@@ -375,7 +375,8 @@ struct cr_batch {
     size_t slot_cap[2] = {0, 0};
     int2 *slot_items[2][cr::BL_COUNT] = {};
     int slot_n[2][cr::BL_COUNT] = {};
-    std::vector<int2> h_items;                     // staging of a slot's upload
+    int2 *pin_items[2] = {nullptr, nullptr};       // pinned staging of each slot's upload
+    size_t pin_cap[2] = {0, 0};
     std::vector<int2> h_full[cr::BL_COUNT];        // items of the live replicas, replica after replica
     std::vector<long long> rep_range[cr::BL_COUNT];  // [2 n] first and end item of each replica
     std::vector<int> step_set;                     // replicas of the lists in slot 1
