@@ -102,12 +102,19 @@ class Replicas:
         P = C.c_void_p * n
         return [P(*[a[k].data_ptr() for a in self.arrays]) for k in range(5)]
 
+    def _lockstep_tiling(self):
+        """The lockstep batch's tiling (8^3 tiles, register-column spreading) on every handle,
+        set again only after tune_batch or set_tilings changed it."""
+        if not getattr(self, "_default_tiling", False):
+            for h in self.handles:
+                h.set_tiling(8, 0)
+            self._default_tiling = True
+
     def make_lockstep(self):
         """The lockstep batch over these replicas' handles (8^3 register-column tiling)."""
+        self._lockstep_tiling()
         if getattr(self, "_lockstep", None) is not None:
             return self._lockstep
-        for h in self.handles:
-            h.set_tiling(8, 0)
         n = self.n
         hs = (C.c_void_p * n)(*[h.h.value for h in self.handles])
         out = C.c_void_p()
@@ -146,6 +153,7 @@ class Replicas:
         return {"first_join": a.value, "rounds": b.value, "total": c.value}
 
     def set_tilings(self, tilings):
+        self._default_tiling = False
         for h, t in zip(self.handles, tilings):
             h.set_tiling(t["tile_edge"], t["spread_mode"])
 
@@ -160,6 +168,7 @@ class Replicas:
         if "isolated" in policies and not self.tilings:
             self.tilings = [h.autotune(a[0], a[1], reps=3) for h, a in zip(self.handles, self.arrays)]
         rates = {}
+        self._default_tiling = False
         for pol in policies:
             if pol == "isolated":
                 self.set_tilings(self.tilings)
